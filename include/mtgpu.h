@@ -1,0 +1,355 @@
+/*
+ * mtgpu.h - C ABI of the B200 (sm_100a) renderer core for marmel-trace.
+ *
+ * The library renders marmel-trace scenes on the GPU behind the same entry
+ * points the reference exposes to its CLI:
+ *
+ *   mt_pathtrace_render   <- pathtrace_render   (src/pathtrace.h:78-80)
+ *   mt_render_image_ex    <- render_image_ex    (src/render.h:65, src/render.c:1627)
+ *   mt_render_image       <- render_image       (src/render.h:29, src/render.c:1522)
+ *   mt_pathtrace_radiance <- pathtrace_radiance (src/pathtrace.h:48), batched
+ *   mt_intersect          <- scene_intersect    (src/scene.c:767), batched
+ *   mt_occluded           <- scene_occluded     (src/scene.c:804), batched
+ *   mt_camera_create      <- camera_create      (src/camera.c:24-66)
+ *
+ * Every signature uses plain C types, pointers and sizes. The reference's
+ * own `Scene` / `Camera` structs are converted to the flat descriptors below
+ * by a small binding on the reference side (see the integration notes);
+ * nothing here depends on the reference headers.
+ *
+ * Return codes follow the reference exactly for argument errors
+ * (src/pathtrace.c:1260-1268, src/render.c:1630-1641):
+ *   0 ok, 1 NULL pointer, 2 non-positive dimensions, 3 bad spp / depth,
+ * and add codes >= 10 for device-side failures. Unsupported scene content
+ * (CSG, SDF, fog, textures, bump maps, volumetric clouds, starfield) is
+ * rejected with MT_ERR_UNSUPPORTED; there is no CPU fallback.
+ *
+ * Threading: a scene handle may be used from one host thread at a time.
+ * All calls are synchronous unless they take a `stream` argument.
+ */
+#ifndef MTGPU_H
+#define MTGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Status codes                                                        */
+/* ------------------------------------------------------------------ */
+#define MT_OK               0
+#define MT_ERR_NULL         1   /* NULL pointer (reference code 1)          */
+#define MT_ERR_DIMS         2   /* width/height <= 0 (reference code 2)     */
+#define MT_ERR_COUNTS       3   /* spp < 1 or depth < 0 (reference code 3)  */
+#define MT_ERR_NO_DEVICE    10  /* no usable CUDA device                    */
+#define MT_ERR_OOM          11  /* device or host allocation failed         */
+#define MT_ERR_LAUNCH       12  /* kernel launch / execution error          */
+#define MT_ERR_WATCHDOG     13  /* a bounded device loop hit its cap        */
+#define MT_ERR_UNSUPPORTED  14  /* scene feature outside the GPU path       */
+#define MT_ERR_INVALID      15  /* malformed descriptor / option            */
+#define MT_ERR_OVERFLOW     16  /* a device queue or stack ran out of room  */
+
+/* ------------------------------------------------------------------ */
+/* Scene descriptor (mirrors the renderer-visible parts of `Scene`)     */
+/* ------------------------------------------------------------------ */
+
+/* Primitive kinds, numbered as the reference's PrimKind (src/geometry.h:32-40). */
+#define MT_PRIM_SPHERE   0
+#define MT_PRIM_PLANE    1
+#define MT_PRIM_BOX      2
+#define MT_PRIM_TRIANGLE 3
+#define MT_PRIM_CYLINDER 4
+
+/*
+ * One primitive, in the reference's `Primitive` order (src/geometry.h:42-66).
+ * The array index is the reference `prim_index` used for the equal-t
+ * tie-break (src/bvh.c:641-646), so the caller must keep file order.
+ *   SPHERE   : v[0..2] center, v[3] radius
+ *   PLANE    : v[0..2] point,  v[3..5] unit normal
+ *   BOX      : v[0..2] center, v[3..5] half extents
+ *   TRIANGLE : v[0..2] a, v[3..5] b, v[6..8] c; when `smooth` is set,
+ *              n[0..8] are the vertex normals na, nb, nc (the reference's
+ *              prim_triangle_smooth, radius > 0.5 gate, src/geometry.c:506)
+ *   CYLINDER : v[0..2] base, v[3..5] top, v[6] r_bottom, v[7] r_top
+ */
+typedef struct {
+    int32_t kind;
+    int32_t material;
+    int32_t smooth;
+    int32_t reserved;
+    double  v[9];
+    double  n[9];
+} mt_prim;
+
+/* Surface material: the `Material` fields the hot path reads (src/material.h). */
+typedef struct {
+    double  albedo[3];
+    double  specular[3];
+    double  shininess;
+    double  reflectivity;
+    double  transparency;
+    double  ior;
+    double  absorption[3];
+    double  deep_color[3];
+    double  metallic;
+    double  roughness;
+    double  emissive[3];
+    double  atmosphere_glow[3];
+    double  bump_strength;   /* must be <= 1e-6 (bump maps are not on the GPU path) */
+    int32_t is_water;
+    int32_t beer_lambert;
+    int32_t pbr;
+    int32_t texture_kind;    /* must be 0 (TEXTURE_NONE)                           */
+} mt_material;
+
+/* Sky / sun parameters (SkyParams, src/material.h). */
+typedef struct {
+    double   sun_dir[3];
+    double   sun_color[3];
+    double   horizon_color[3];
+    double   zenith_color[3];
+    double   gradient_gamma;
+    double   sun_glow_exponent;
+    double   sun_glow_strength;
+    double   cloud_height;
+    double   cloud_scale;
+    double   cloud_coverage;
+    double   cloud_softness;
+    double   cloud_sharpness;
+    double   cloud_thickness;   /* must be <= 1e-4 (planar clouds only)  */
+    double   sun_radius;        /* degrees; 0 = hard sun                 */
+    double   star_intensity;    /* must be 0                             */
+    double   nebula_intensity;  /* must be 0                             */
+    double   galaxy_intensity;  /* must be 0                             */
+    int32_t  cloud_octaves;
+    uint32_t seed;
+} mt_sky;
+
+/* Procedural Gerstner ocean height parameters (SceneOceanParams, src/scene.h:67-77). */
+typedef struct {
+    int32_t  enabled;
+    uint32_t seed;
+    double   center[3];
+    double   amplitude;
+    double   wavelength;
+    double   direction[3];
+    double   chop;
+    double   chop_wavelength;
+} mt_ocean;
+
+typedef struct {
+    const mt_prim     *prims;
+    int32_t            prim_count;
+    int32_t            material_count;
+    const mt_material *materials;
+    mt_sky             sky;
+    double             fog_density;     /* must be 0: fog is not on the GPU path */
+    double             water_level;     /* Scene.water_level                     */
+    int32_t            water_material;  /* Scene.water_material, -1 = none      */
+    int32_t            fog_shadow_steps;/* FogParams.shadow_steps: must be 0     */
+    mt_ocean           ocean;           /* Scene.has_ocean / ocean_params        */
+} mt_scene_desc;
+
+/* Pinhole / thin-lens camera (Camera, src/camera.h). */
+typedef struct {
+    double position[3];
+    double lower_left[3];
+    double horizontal[3];
+    double vertical[3];
+    double aperture;
+    double focus_distance;
+    double dome_radius;
+    double anamorphic_squeeze;
+} mt_camera;
+
+/* Fixed / adaptive Whitted parameters (RenderParams, src/render.h:49-55). */
+typedef struct {
+    int32_t samples_per_pixel;
+    int32_t max_depth;
+    int32_t adaptive;          /* 1 = adaptive refinement (src/render.c:1128-1500) */
+    int32_t adaptive_max_spp;
+    double  adaptive_tau;
+} mt_render_params;
+
+/* ------------------------------------------------------------------ */
+/* Build / render options                                              */
+/* ------------------------------------------------------------------ */
+
+/* Arithmetic of the device path. FP32 is the production path; FP64 follows
+ * the reference's double-precision expression order operation by operation
+ * and is the exact-parity mode. */
+#define MT_PRECISION_FP32 0
+#define MT_PRECISION_FP64 1
+
+/* Integrator for the path tracer. */
+#define MT_INTEGRATOR_MEGAKERNEL 0   /* one thread per pixel, full bounce loop    */
+#define MT_INTEGRATOR_WAVEFRONT  1   /* per-bounce stage kernels + queues         */
+
+typedef struct {
+    int32_t precision;       /* MT_PRECISION_*                                  */
+    int32_t integrator;      /* MT_INTEGRATOR_*                                 */
+    int32_t block_size;      /* threads per block, 0 = library default          */
+    int32_t queue_capacity;  /* wavefront paths in flight, 0 = library default  */
+    int32_t bvh_width;       /* 2, 4 or 8; 0 = library default                  */
+    int32_t sort_threshold;  /* wavefront: sort by material above this many paths (0 = never) */
+    int32_t use_graph;       /* wavefront: capture the spp loop in a CUDA graph */
+    int32_t device;          /* CUDA device ordinal                             */
+} mt_options;
+
+/* Fill `o` with the library defaults (FP32, megakernel, BVH2, device 0). */
+void mt_options_default(mt_options *o);
+
+/* ------------------------------------------------------------------ */
+/* Scene lifetime                                                      */
+/* ------------------------------------------------------------------ */
+
+typedef struct mt_scene mt_scene;
+
+/*
+ * Build the acceleration structure on the host (binned SAH, 12 bins, leaf
+ * size 4, planes kept out of the tree: src/bvh.c:40-48,180-422), flatten it
+ * into the device node layout and upload everything to device memory.
+ * `opts` may be NULL (defaults). On success *out owns the device copy and
+ * must be released with mt_scene_release.
+ */
+int  mt_scene_create(const mt_scene_desc *desc, const mt_options *opts, mt_scene **out);
+void mt_scene_release(mt_scene *scene);
+
+/* Introspection: tree node count, depth, emissive-light count, device bytes. */
+typedef struct {
+    int32_t prim_count;
+    int32_t plane_count;
+    int32_t node_count;       /* binary tree nodes, as bvh_node_count()     */
+    int32_t depth;            /* leaf depth, root = 1, as bvh_depth()       */
+    int32_t light_count;      /* emissive sphere lights (<= 8)              */
+    int32_t light_prims[8];   /* their prim indices, file order             */
+    int64_t device_bytes;     /* device memory held by the scene            */
+} mt_scene_info;
+int mt_scene_get_info(const mt_scene *scene, mt_scene_info *info);
+
+/* Export the host BVH (for parity checks against the reference builder):
+ * nodes as {min xyz, max xyz} doubles plus {left, right, first, count} ints
+ * in the reference's node order, and the prim permutation `order`. Arrays
+ * may be NULL to query sizes only. */
+int mt_scene_export_bvh(const mt_scene *scene, double *bounds6, int32_t *links4,
+                        int32_t *order, int32_t *node_count, int32_t *order_count);
+
+/* Host-only build of the same BVH (no device needed): nodes, permutation and
+ * leaf depth exactly as mt_scene_export_bvh reports them. Call once with NULL
+ * arrays to query the sizes. */
+int mt_bvh_build_host(const mt_prim *prims, int32_t prim_count, double *bounds6, int32_t *links4,
+                      int32_t *order, int32_t *node_count, int32_t *order_count, int32_t *depth);
+
+/* ------------------------------------------------------------------ */
+/* Camera                                                              */
+/* ------------------------------------------------------------------ */
+
+/* Restates camera_create (src/camera.c:24-66): look-at basis and viewport. */
+void mt_camera_create(const double from[3], const double at[3], const double up[3],
+                      double vfov_deg, double aspect, mt_camera *out);
+
+/* ------------------------------------------------------------------ */
+/* Renderers (drop-in entry points)                                     */
+/* ------------------------------------------------------------------ */
+
+/*
+ * Path-traced image into a top-down row-major RGB8 buffer of w*h*3 bytes
+ * (src/pathtrace.h:62-80). Per-pixel jitter, lens samples and seeds follow
+ * pt_render_pixel (src/pathtrace.c:1047-1096).
+ */
+int mt_pathtrace_render(mt_scene *scene, const mt_camera *cam, int width, int height,
+                        int samples_per_pixel, int max_depth, unsigned char *rgb_out);
+
+/* Whitted renderer, fixed spp (render_image, src/render.c:1522-1625). */
+int mt_render_image(mt_scene *scene, const mt_camera *cam, int width, int height,
+                    int samples_per_pixel, int max_depth, unsigned char *rgb_out);
+
+/* render_image_ex (src/render.c:1627-1665): fixed or adaptive Whitted. */
+int mt_render_image_ex(mt_scene *scene, const mt_camera *cam, int width, int height,
+                       const mt_render_params *params, unsigned char *rgb_out);
+
+/*
+ * Linear (pre-gamma) per-pixel mean radiance, w*h*3 floats, top-down.
+ * mode 0 = path tracer, 1 = Whitted. `out` is host memory. This is the
+ * FP32 image the progressive / RMSE measurements read.
+ */
+#define MT_MODE_PATHTRACE 0
+#define MT_MODE_WHITTED   1
+int mt_render_linear(mt_scene *scene, const mt_camera *cam, int width, int height,
+                     int samples_per_pixel, int max_depth, int mode, float *out);
+
+/*
+ * Same as mt_render_linear but for a sample window [spp_begin, spp_end) and
+ * with DEVICE output: `accum_dev` (w*h*3 floats) receives the SUM of the
+ * window's samples (added to its contents when `accumulate` is 1), so a
+ * progressive render is a sequence of windows. Asynchronous on `stream`
+ * (a cudaStream_t, NULL = legacy default stream). Used by the benchmark.
+ */
+int mt_render_accumulate_device(mt_scene *scene, const mt_camera *cam, int width, int height,
+                                int spp_begin, int spp_end, int max_depth, int mode,
+                                float *accum_dev, int accumulate, void *stream);
+
+/* Per-launch statistics of the last render on this scene. */
+typedef struct {
+    double  kernel_ms;        /* device time of the render kernels (CUDA events) */
+    int64_t primary_rays;     /* camera rays                                     */
+    int64_t extension_rays;   /* nearest-hit rays incl. primary                  */
+    int64_t shadow_rays;      /* NEE / any-hit rays                              */
+    int64_t node_visits;      /* inner nodes whose two child boxes were tested   */
+    int64_t prim_tests;       /* primitive intersection tests                    */
+    int32_t launches;         /* kernels launched                                */
+    int32_t error_flags;      /* device error word (0 = clean)                   */
+} mt_stats;
+int mt_get_stats(const mt_scene *scene, mt_stats *out);
+/* Enable (1) or disable (0) the ray / node counters (off by default: they
+ * cost atomics). */
+int mt_set_counting(mt_scene *scene, int enable);
+
+/* ------------------------------------------------------------------ */
+/* Batched queries (parity harness entry points)                        */
+/* ------------------------------------------------------------------ */
+
+/*
+ * Batched pathtrace_radiance (src/pathtrace.c:800-1028): n rays (origins and
+ * directions as xyz doubles), one seed key each, linear RGB out (doubles).
+ */
+int mt_pathtrace_radiance(mt_scene *scene, int n, const double *origins, const double *dirs,
+                          int max_depth, const uint32_t *seed_keys, double *radiance_out);
+
+/* Batched Whitted trace() at depth 0 (src/render.c:842-863), time 0: n rays
+ * (xyz doubles) and seed keys in, linear RGB colour out (doubles). */
+int mt_whitted_trace(mt_scene *scene, int n, const double *origins, const double *dirs,
+                     int max_depth, const uint32_t *seed_keys, double *color_out);
+
+/*
+ * Batched scene_intersect (src/scene.c:767-775 -> src/bvh.c:557-712).
+ * Outputs per ray: prim index (-1 = miss), t, u, v, front_face, the unit
+ * normal facing the ray (xyz) and the material index. Output pointers may
+ * be NULL except prim_out.
+ */
+int mt_intersect(mt_scene *scene, int n, const double *origins, const double *dirs,
+                 double tmin, double tmax, int32_t *prim_out, double *t_out,
+                 double *normal_out, int32_t *front_out, int32_t *material_out);
+
+/* Batched any-hit test (scene_occluded, src/scene.c:777-811): 1 = blocked. */
+int mt_occluded(mt_scene *scene, int n, const double *origins, const double *dirs,
+                double tmin, double tmax, int32_t *occluded_out);
+
+/* Primary rays exactly as pt_render_pixel draws them (src/pathtrace.c:1057-1082):
+ * for every (x, y, s), origin + direction (doubles, 6 per ray) in
+ * ((y*w + x)*spp + s) order. Computed on the device. */
+int mt_primary_rays(mt_scene *scene, const mt_camera *cam, int width, int height, int spp,
+                    int mode, double *rays_out);
+
+/* Library version and last error text (thread-local, never NULL). */
+const char *mt_version(void);
+const char *mt_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MTGPU_H */

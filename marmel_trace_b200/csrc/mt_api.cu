@@ -1,0 +1,829 @@
+// mt_api.cu - implementation of the C ABI declared in include/mtgpu.h.
+//
+// Host side: validates the scene descriptor, builds the BVH with the
+// restated reference builder (mt_bvh.cpp), flattens it, uploads the scene in
+// the arithmetic type the options select and dispatches the kernels. Every
+// CUDA call is checked and mapped to an MT_ERR_* code; there is no CPU
+// fallback anywhere on this path.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/mtgpu.h"
+#include "mt_bvh.h"
+#include "mt_launch.h"
+#include "mt_layout.h"
+#include "mt_wavefront.h"
+
+using namespace mt;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    int code = (e == cudaErrorMemoryAllocation) ? MT_ERR_OOM
+               : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? MT_ERR_NO_DEVICE
+                                                                               : MT_ERR_LAUNCH;
+    return fail(code, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                          \
+    do {                                        \
+        cudaError_t e_ = (call);                \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+// vec3_normalize in host double arithmetic (src/vec3.c:29-37)
+void normalize3(const double *a, double *o)
+{
+    double len_sq = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+    if (len_sq <= 1e-12) {
+        o[0] = o[1] = o[2] = 0.0;
+        return;
+    }
+    double inv = 1.0 / sqrt(len_sq);
+    o[0] = a[0] * inv;
+    o[1] = a[1] * inv;
+    o[2] = a[2] * inv;
+}
+
+}  // namespace
+
+struct mt_scene {
+    mt_options opts;
+    HostBvh bvh;
+    FlatBvh flat;
+    int prim_count = 0;
+    int light_count = 0;
+    int light_prims[kMaxLights] = {0};
+    std::vector<void *> allocs;
+    int64_t device_bytes = 0;
+    DevScene<float> sf;
+    DevScene<double> sd;
+    unsigned *d_err = nullptr;
+    DevCounters *d_counters = nullptr;
+    bool counting = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    mt_stats stats;
+    WavefrontState *wf = nullptr;
+
+    template <typename T> int upload(const std::vector<T> &v, const T **dst)
+    {
+        *dst = nullptr;
+        if (v.empty()) return 0;
+        void *p = nullptr;
+        size_t bytes = v.size() * sizeof(T);
+        CK(cudaMalloc(&p, bytes), "cudaMalloc(scene)");
+        allocs.push_back(p);
+        device_bytes += (int64_t)bytes;
+        CK(cudaMemcpy(p, v.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(scene)");
+        *dst = (const T *)p;
+        return 0;
+    }
+};
+
+namespace {
+
+int validate(const mt_scene_desc *d)
+{
+    if (d->prim_count < 0 || d->material_count < 0) return fail(MT_ERR_INVALID, "negative counts");
+    if (d->prim_count > 0 && !d->prims) return fail(MT_ERR_NULL, "prims is NULL");
+    if (d->material_count > 0 && !d->materials) return fail(MT_ERR_NULL, "materials is NULL");
+    if (d->prim_count >= (1 << 28)) return fail(MT_ERR_UNSUPPORTED, "more than 2^28 primitives");
+    if (d->fog_density > 0.0) return fail(MT_ERR_UNSUPPORTED, "fog is not on the GPU path");
+    if (d->fog_shadow_steps > 0) return fail(MT_ERR_UNSUPPORTED, "volumetric fog/water marching is not on the GPU path");
+    const mt_sky &s = d->sky;
+    if (s.cloud_thickness > 1e-4) return fail(MT_ERR_UNSUPPORTED, "volumetric clouds are not on the GPU path");
+    if (s.star_intensity > 0.0 || s.nebula_intensity > 0.0 || s.galaxy_intensity > 0.0)
+        return fail(MT_ERR_UNSUPPORTED, "starfield / nebula / galaxy sky terms are not on the GPU path");
+    for (int i = 0; i < d->material_count; ++i) {
+        const mt_material &m = d->materials[i];
+        if (m.texture_kind != 0) return fail(MT_ERR_UNSUPPORTED, "material %d: textures are not on the GPU path", i);
+        if (m.bump_strength > 1e-6) return fail(MT_ERR_UNSUPPORTED, "material %d: bump maps are not on the GPU path", i);
+    }
+    for (int i = 0; i < d->prim_count; ++i) {
+        int k = d->prims[i].kind;
+        if (k < MT_PRIM_SPHERE || k > MT_PRIM_CYLINDER)
+            return fail(MT_ERR_UNSUPPORTED, "prim %d: kind %d (CSG / SDF) is not on the GPU path", i, k);
+    }
+    return 0;
+}
+
+template <typename R> void fill_material(const mt_material &m, DevMaterial<R> *o)
+{
+    memset(o, 0, sizeof *o);
+    for (int k = 0; k < 3; ++k) {
+        o->albedo[k] = (R)m.albedo[k];
+        o->specular[k] = (R)m.specular[k];
+        o->absorption[k] = (R)m.absorption[k];
+        o->deep_color[k] = (R)m.deep_color[k];
+        o->emissive[k] = (R)m.emissive[k];
+        o->atmosphere_glow[k] = (R)m.atmosphere_glow[k];
+    }
+    o->shininess = (R)m.shininess;
+    o->reflectivity = (R)m.reflectivity;
+    o->transparency = (R)m.transparency;
+    o->ior = (R)m.ior;
+    o->metallic = (R)m.metallic;
+    o->roughness = (R)m.roughness;
+    o->is_water = m.is_water;
+    o->beer_lambert = m.beer_lambert;
+    o->pbr = m.pbr;
+}
+
+template <typename R> void fill_sky(const mt_sky &s, DevSky<R> *o)
+{
+    for (int k = 0; k < 3; ++k) {
+        o->sun_dir[k] = (R)s.sun_dir[k];
+        o->sun_color[k] = (R)s.sun_color[k];
+        o->horizon_color[k] = (R)s.horizon_color[k];
+        o->zenith_color[k] = (R)s.zenith_color[k];
+    }
+    o->gradient_gamma = (R)s.gradient_gamma;
+    o->sun_glow_exponent = (R)s.sun_glow_exponent;
+    o->sun_glow_strength = (R)s.sun_glow_strength;
+    o->cloud_height = (R)s.cloud_height;
+    o->cloud_scale = (R)s.cloud_scale;
+    o->cloud_coverage = (R)s.cloud_coverage;
+    o->cloud_softness = (R)s.cloud_softness;
+    o->cloud_sharpness = (R)s.cloud_sharpness;
+    o->sun_radius = (R)s.sun_radius;
+    o->cloud_octaves = s.cloud_octaves;
+    o->seed = s.seed;
+}
+
+// Upload every array of the scene in arithmetic type R.
+template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, DevScene<R> *S)
+{
+    const int n = d->prim_count;
+    const FlatBvh &fb = sc->flat;
+    memset(S, 0, sizeof *S);
+
+    // Slots per kind in leaf order (tree prims), planes in file order.
+    std::vector<int2> prim_info(n > 0 ? n : 1, make_int2(0, -1));
+    std::vector<int2> refs(fb.ref_prim.size());
+    std::vector<float4> tri4;
+    std::vector<R> tris, tri_normals, spheres, boxes, cyls, planes;
+    std::vector<int> tri_smooth, plane_prims;
+    bool any_smooth = false;
+    for (int i = 0; i < n; ++i)
+        if (d->prims[i].kind == MT_PRIM_TRIANGLE && d->prims[i].smooth) any_smooth = true;
+
+    int ntri = 0, nsph = 0, nbox = 0, ncyl = 0;
+    for (size_t k = 0; k < fb.ref_prim.size(); ++k) {
+        int pi = fb.ref_prim[k];
+        const mt_prim &p = d->prims[pi];
+        int code = 0;
+        switch (p.kind) {
+        case MT_PRIM_SPHERE:
+            code = (KIND_SPHERE << 28) | nsph++;
+            for (int j = 0; j < 4; ++j) spheres.push_back((R)p.v[j]);
+            break;
+        case MT_PRIM_BOX:
+            code = (KIND_BOX << 28) | nbox++;
+            for (int j = 0; j < 6; ++j) boxes.push_back((R)p.v[j]);
+            break;
+        case MT_PRIM_CYLINDER:
+            code = (KIND_CYLINDER << 28) | ncyl++;
+            for (int j = 0; j < 8; ++j) cyls.push_back((R)p.v[j]);
+            break;
+        case MT_PRIM_TRIANGLE: {
+            code = (KIND_TRIANGLE << 28) | ntri++;
+            if (sizeof(R) == 8) {
+                // a, e1 = b - a, e2 = c - a in double (src/geometry.c:229-241)
+                for (int j = 0; j < 3; ++j) tris.push_back((R)p.v[j]);
+                for (int j = 0; j < 3; ++j) tris.push_back((R)(p.v[3 + j] - p.v[j]));
+                for (int j = 0; j < 3; ++j) tris.push_back((R)(p.v[6 + j] - p.v[j]));
+                tri_smooth.push_back(p.smooth ? 1 : 0);
+            } else {
+                float4 a = make_float4((float)p.v[0], (float)p.v[1], (float)p.v[2], 0.0f);
+                float4 b = make_float4((float)p.v[3], (float)p.v[4], (float)p.v[5], 0.0f);
+                float4 c = make_float4((float)p.v[6], (float)p.v[7], (float)p.v[8], 0.0f);
+                int pid = pi, sm = p.smooth ? 1 : 0;
+                memcpy(&a.w, &pid, 4);
+                memcpy(&b.w, &sm, 4);
+                tri4.push_back(a);
+                tri4.push_back(b);
+                tri4.push_back(c);
+            }
+            if (any_smooth)
+                for (int j = 0; j < 9; ++j) tri_normals.push_back((R)p.n[j]);
+            break;
+        }
+        default:
+            break;
+        }
+        refs[k] = make_int2(pi, code);
+        prim_info[pi] = make_int2(code, p.material);
+    }
+    for (size_t k = 0; k < sc->bvh.planes.size(); ++k) {
+        int pi = sc->bvh.planes[k];
+        const mt_prim &p = d->prims[pi];
+        double nrm[3];
+        normalize3(p.v + 3, nrm);  // intersect_plane re-normalises the axis (src/geometry.c:375)
+        for (int j = 0; j < 3; ++j) planes.push_back((R)p.v[j]);
+        for (int j = 0; j < 3; ++j) planes.push_back((R)nrm[j]);
+        plane_prims.push_back(pi);
+        prim_info[pi] = make_int2((KIND_PLANE << 28) | (int)k, p.material);
+    }
+
+    std::vector<DevMaterial<R>> mats(d->material_count);
+    for (int i = 0; i < d->material_count; ++i) fill_material(d->materials[i], &mats[i]);
+
+    std::vector<float4> nodes(fb.nodes.size() / 4);
+    if (!fb.nodes.empty()) memcpy(nodes.data(), fb.nodes.data(), fb.nodes.size() * sizeof(float));
+
+    int rc = 0;
+    if ((rc = sc->upload(nodes, &S->nodes))) return rc;
+    if ((rc = sc->upload(refs, &S->refs))) return rc;
+    if ((rc = sc->upload(tri4, &S->tri4))) return rc;
+    if ((rc = sc->upload(tris, &S->tris))) return rc;
+    if ((rc = sc->upload(tri_normals, &S->tri_normals))) return rc;
+    if ((rc = sc->upload(tri_smooth, &S->tri_smooth))) return rc;
+    if ((rc = sc->upload(spheres, &S->spheres))) return rc;
+    if ((rc = sc->upload(boxes, &S->boxes))) return rc;
+    if ((rc = sc->upload(cyls, &S->cyls))) return rc;
+    if ((rc = sc->upload(planes, &S->planes))) return rc;
+    if ((rc = sc->upload(plane_prims, &S->plane_prims))) return rc;
+    if ((rc = sc->upload(prim_info, &S->prim_info))) return rc;
+    if ((rc = sc->upload(mats, &S->materials))) return rc;
+
+    S->node_count = fb.node_count;
+    S->plane_count = (int)plane_prims.size();
+    S->prim_count = n;
+    S->material_count = d->material_count;
+    S->water_material = d->water_material;
+    S->water_level = (R)d->water_level;
+    S->ocean.enabled = d->ocean.enabled;
+    S->ocean.seed = d->ocean.seed;
+    for (int k = 0; k < 3; ++k) {
+        S->ocean.center[k] = (R)d->ocean.center[k];
+        S->ocean.direction[k] = (R)d->ocean.direction[k];
+    }
+    S->ocean.amplitude = (R)d->ocean.amplitude;
+    S->ocean.wavelength = (R)d->ocean.wavelength;
+    S->ocean.chop = (R)d->ocean.chop;
+    S->ocean.chop_wavelength = (R)d->ocean.chop_wavelength;
+    fill_sky(d->sky, &S->sky);
+
+    // scene_collect_emissive_lights (src/scene.c:1384-1426): the first 8
+    // emissive PBR spheres with radius > 0, in file order.
+    S->light_count = 0;
+    for (int i = 0; i < n && S->light_count < kMaxLights; ++i) {
+        const mt_prim &p = d->prims[i];
+        if (p.kind != MT_PRIM_SPHERE) continue;
+        if (p.material < 0 || p.material >= d->material_count) continue;
+        const mt_material &m = d->materials[p.material];
+        if (!m.pbr) continue;
+        if (m.emissive[0] == 0.0 && m.emissive[1] == 0.0 && m.emissive[2] == 0.0) continue;
+        if (!(p.v[3] > 0.0)) continue;
+        DevLight<R> &L = S->lights[S->light_count];
+        for (int k = 0; k < 3; ++k) {
+            L.center[k] = (R)p.v[k];
+            L.emissive[k] = (R)m.emissive[k];
+        }
+        L.radius = (R)p.v[3];
+        L.prim = i;
+        sc->light_prims[S->light_count] = i;
+        S->light_count++;
+    }
+    sc->light_count = S->light_count;
+    S->err = sc->d_err;
+    S->counters = nullptr;
+    return 0;
+}
+
+template <typename R> void fill_camera(const mt_camera *c, DevCamera<R> *o)
+{
+    for (int k = 0; k < 3; ++k) {
+        o->position[k] = (R)c->position[k];
+        o->lower_left[k] = (R)c->lower_left[k];
+        o->horizontal[k] = (R)c->horizontal[k];
+        o->vertical[k] = (R)c->vertical[k];
+    }
+    o->aperture = (R)c->aperture;
+    o->focus_distance = (R)c->focus_distance;
+    o->dome_radius = (R)c->dome_radius;
+    o->anamorphic_squeeze = (R)c->anamorphic_squeeze;
+}
+
+int set_device(const mt_scene *sc)
+{
+    CK(cudaSetDevice(sc->opts.device), "cudaSetDevice");
+    return 0;
+}
+
+// Check the device error word after a synchronised launch and clear it.
+int check_err_word(mt_scene *sc)
+{
+    unsigned e = 0;
+    CK(cudaMemcpy(&e, sc->d_err, sizeof e, cudaMemcpyDeviceToHost), "cudaMemcpy(err)");
+    sc->stats.error_flags = (int32_t)e;
+    if (e != 0) {
+        unsigned z = 0;
+        CK(cudaMemcpy(sc->d_err, &z, sizeof z, cudaMemcpyHostToDevice), "cudaMemcpy(err)");
+        if (e & ERR_STACK) return fail(MT_ERR_OVERFLOW, "traversal stack overflow");
+        if (e & ERR_QUEUE) return fail(MT_ERR_OVERFLOW, "wavefront queue overflow");
+        if (e & ERR_WHITTED) return fail(MT_ERR_OVERFLOW, "Whitted frame stack overflow");
+        if (e & ERR_WATCHDOG) return fail(MT_ERR_WATCHDOG, "a bounded device loop reached its cap");
+        return fail(MT_ERR_LAUNCH, "device error word 0x%x", e);
+    }
+    return 0;
+}
+
+int read_counters(mt_scene *sc)
+{
+    if (!sc->counting) return 0;
+    DevCounters c;
+    CK(cudaMemcpy(&c, sc->d_counters, sizeof c, cudaMemcpyDeviceToHost), "cudaMemcpy(counters)");
+    sc->stats.primary_rays = (int64_t)c.primary_rays;
+    sc->stats.extension_rays = (int64_t)c.extension_rays;
+    sc->stats.shadow_rays = (int64_t)c.shadow_rays;
+    sc->stats.node_visits = (int64_t)c.node_visits;
+    sc->stats.prim_tests = (int64_t)c.prim_tests;
+    return 0;
+}
+
+int reset_counters(mt_scene *sc)
+{
+    if (!sc->counting) return 0;
+    CK(cudaMemset(sc->d_counters, 0, sizeof(DevCounters)), "cudaMemset(counters)");
+    return 0;
+}
+
+template <typename R> DevScene<R> &dev_scene(mt_scene *sc);
+template <> DevScene<float> &dev_scene<float>(mt_scene *sc) { return sc->sf; }
+template <> DevScene<double> &dev_scene<double>(mt_scene *sc) { return sc->sd; }
+
+// Run one per-pixel render kernel over samples [s0, s1) into device memory.
+template <typename R>
+int render_dev(mt_scene *sc, const mt_camera *cam, int w, int h, int spp_total, int s0, int s1, int depth, int mode,
+               int out_kind, void *dout, cudaStream_t stream, bool timed)
+{
+    DevCamera<R> dc;
+    fill_camera(cam, &dc);
+    DevScene<R> S = dev_scene<R>(sc);
+    S.counters = sc->counting ? sc->d_counters : nullptr;
+    if (sc->opts.integrator == MT_INTEGRATOR_WAVEFRONT && mode == RENDER_PT) {
+        int rc = wavefront_render<R>(sc->wf, S, dc, w, h, s0, s1, depth, out_kind, dout, stream, &sc->opts,
+                                     timed ? sc->ev0 : nullptr, timed ? sc->ev1 : nullptr, &sc->stats.launches);
+        if (rc) return fail(rc, "wavefront render failed: %s", wavefront_last_error());
+        return 0;
+    }
+    if (timed) CK(cudaEventRecord(sc->ev0, stream), "cudaEventRecord");
+    CK(launch_render<R>(S, dc, w, h, spp_total, s0, s1, depth, mode, out_kind, dout, sc->opts.block_size, stream),
+       "render kernel launch");
+    if (timed) CK(cudaEventRecord(sc->ev1, stream), "cudaEventRecord");
+    sc->stats.launches = 1;
+    return 0;
+}
+
+int render_args(const mt_scene *sc, const mt_camera *cam, const void *out, int w, int h, int spp, int depth)
+{
+    if (sc == nullptr || cam == nullptr || out == nullptr) return fail(MT_ERR_NULL, "NULL pointer");
+    if (w <= 0 || h <= 0) return fail(MT_ERR_DIMS, "non-positive dimensions");
+    if (spp < 1 || depth < 0) return fail(MT_ERR_COUNTS, "bad sample / depth counts");
+    return 0;
+}
+
+// Full-frame render into a host buffer (RGB8 or mean float).
+int render_host(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, int depth, int mode, int out_kind,
+                void *host_out)
+{
+    int rc = render_args(sc, cam, host_out, w, h, spp, depth);
+    if (rc) return rc;
+    if (mode == RENDER_WHITTED && depth + 2 > kWhittedFrames)
+        return fail(MT_ERR_UNSUPPORTED, "Whitted depth %d exceeds the device frame stack (max %d)", depth,
+                    kWhittedFrames - 2);
+    if ((rc = set_device(sc))) return rc;
+    size_t bytes = (size_t)w * h * 3 * (out_kind == OUT_RGB8 ? 1 : sizeof(float));
+    void *dout = nullptr;
+    CK(cudaMalloc(&dout, bytes), "cudaMalloc(image)");
+    if ((rc = reset_counters(sc))) {
+        cudaFree(dout);
+        return rc;
+    }
+    if (sc->opts.precision == MT_PRECISION_FP64)
+        rc = render_dev<double>(sc, cam, w, h, spp, 0, spp, depth, mode, out_kind, dout, 0, true);
+    else
+        rc = render_dev<float>(sc, cam, w, h, spp, 0, spp, depth, mode, out_kind, dout, 0, true);
+    cudaError_t e = cudaSuccess;
+    if (!rc) {
+        e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(host_out, dout, bytes, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(dout);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "render");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
+    sc->stats.kernel_ms = ms;
+    if ((rc = read_counters(sc))) return rc;
+    return check_err_word(sc);
+}
+
+template <typename T> struct DevBuf {
+    T *p = nullptr;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, (n ? n : 1) * sizeof(T)); }
+};
+
+}  // namespace
+
+extern "C" {
+
+void mt_options_default(mt_options *o)
+{
+    if (!o) return;
+    memset(o, 0, sizeof *o);
+    o->precision = MT_PRECISION_FP32;
+    o->integrator = MT_INTEGRATOR_MEGAKERNEL;
+    o->block_size = 128;
+    o->queue_capacity = 0;
+    o->bvh_width = 2;
+    o->sort_threshold = 0;
+    o->use_graph = 1;
+    o->device = 0;
+}
+
+const char *mt_version(void) { return "mtgpu 0.1 (sm_100a)"; }
+const char *mt_last_error(void) { return g_last_error.c_str(); }
+
+int mt_scene_create(const mt_scene_desc *desc, const mt_options *opts, mt_scene **out)
+{
+    if (!desc || !out) return fail(MT_ERR_NULL, "NULL pointer");
+    *out = nullptr;
+    int rc = validate(desc);
+    if (rc) return rc;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0) return fail(MT_ERR_NO_DEVICE, "no CUDA device (%s)", cudaGetErrorString(e));
+
+    mt_scene *sc = new mt_scene();
+    if (opts) sc->opts = *opts;
+    else mt_options_default(&sc->opts);
+    if (sc->opts.block_size <= 0) sc->opts.block_size = 128;
+    if (sc->opts.device < 0 || sc->opts.device >= ndev) {
+        delete sc;
+        return fail(MT_ERR_INVALID, "device %d out of range", sc->opts.device);
+    }
+    sc->prim_count = desc->prim_count;
+    memset(&sc->stats, 0, sizeof sc->stats);
+    auto bail = [&](int code) {
+        mt_scene_release(sc);
+        return code;
+    };
+    if ((rc = set_device(sc))) return bail(rc);
+
+    build_bvh(desc->prims, desc->prim_count, &sc->bvh);
+    flatten_bvh(sc->bvh, &sc->flat);
+    if (sc->flat.depth + 2 > kStackSize)
+        return bail(fail(MT_ERR_UNSUPPORTED, "BVH depth %d exceeds the traversal stack (%d)", sc->flat.depth,
+                         kStackSize));
+
+    void *p = nullptr;
+    e = cudaMalloc(&p, sizeof(unsigned));
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
+    sc->allocs.push_back(p);
+    sc->d_err = (unsigned *)p;
+    cudaMemset(sc->d_err, 0, sizeof(unsigned));
+    e = cudaMalloc(&p, sizeof(DevCounters));
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(counters)"));
+    sc->allocs.push_back(p);
+    sc->d_counters = (DevCounters *)p;
+    cudaMemset(sc->d_counters, 0, sizeof(DevCounters));
+    if ((e = cudaEventCreate(&sc->ev0)) != cudaSuccess || (e = cudaEventCreate(&sc->ev1)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaEventCreate"));
+
+    if (sc->opts.precision == MT_PRECISION_FP64) rc = upload_scene<double>(sc, desc, &sc->sd);
+    else rc = upload_scene<float>(sc, desc, &sc->sf);
+    if (rc) return bail(rc);
+    *out = sc;
+    return 0;
+}
+
+void mt_scene_release(mt_scene *sc)
+{
+    if (!sc) return;
+    cudaSetDevice(sc->opts.device);
+    if (sc->wf) wavefront_destroy(sc->wf);
+    for (void *p : sc->allocs) cudaFree(p);
+    if (sc->ev0) cudaEventDestroy(sc->ev0);
+    if (sc->ev1) cudaEventDestroy(sc->ev1);
+    delete sc;
+}
+
+int mt_scene_get_info(const mt_scene *sc, mt_scene_info *info)
+{
+    if (!sc || !info) return fail(MT_ERR_NULL, "NULL pointer");
+    memset(info, 0, sizeof *info);
+    info->prim_count = sc->prim_count;
+    info->plane_count = (int32_t)sc->bvh.planes.size();
+    info->node_count = (int32_t)sc->bvh.nodes.size();
+    info->depth = sc->bvh.depth;
+    info->light_count = sc->light_count;
+    for (int i = 0; i < sc->light_count; ++i) info->light_prims[i] = sc->light_prims[i];
+    info->device_bytes = sc->device_bytes;
+    return 0;
+}
+
+int mt_scene_export_bvh(const mt_scene *sc, double *bounds6, int32_t *links4, int32_t *order, int32_t *node_count,
+                        int32_t *order_count)
+{
+    if (!sc) return fail(MT_ERR_NULL, "NULL pointer");
+    if (node_count) *node_count = (int32_t)sc->bvh.nodes.size();
+    if (order_count) *order_count = (int32_t)sc->bvh.order.size();
+    for (size_t i = 0; i < sc->bvh.nodes.size(); ++i) {
+        const HostNode &n = sc->bvh.nodes[i];
+        if (bounds6)
+            for (int k = 0; k < 3; ++k) {
+                bounds6[6 * i + k] = n.mn[k];
+                bounds6[6 * i + 3 + k] = n.mx[k];
+            }
+        if (links4) {
+            links4[4 * i] = n.left;
+            links4[4 * i + 1] = n.right;
+            links4[4 * i + 2] = n.first;
+            links4[4 * i + 3] = n.count;
+        }
+    }
+    if (order)
+        for (size_t i = 0; i < sc->bvh.order.size(); ++i) order[i] = sc->bvh.order[i];
+    return 0;
+}
+
+int mt_bvh_build_host(const mt_prim *prims, int32_t n, double *bounds6, int32_t *links4, int32_t *order,
+                      int32_t *node_count, int32_t *order_count, int32_t *depth)
+{
+    if (n < 0 || (n > 0 && !prims)) return fail(MT_ERR_NULL, "NULL pointer");
+    HostBvh b;
+    build_bvh(prims, n, &b);
+    if (node_count) *node_count = (int32_t)b.nodes.size();
+    if (order_count) *order_count = (int32_t)b.order.size();
+    if (depth) *depth = b.depth;
+    for (size_t i = 0; i < b.nodes.size(); ++i) {
+        const HostNode &nd = b.nodes[i];
+        if (bounds6)
+            for (int k = 0; k < 3; ++k) {
+                bounds6[6 * i + k] = nd.mn[k];
+                bounds6[6 * i + 3 + k] = nd.mx[k];
+            }
+        if (links4) {
+            links4[4 * i] = nd.left;
+            links4[4 * i + 1] = nd.right;
+            links4[4 * i + 2] = nd.first;
+            links4[4 * i + 3] = nd.count;
+        }
+    }
+    if (order)
+        for (size_t i = 0; i < b.order.size(); ++i) order[i] = b.order[i];
+    return 0;
+}
+
+// camera_create (src/camera.c:24-66) in host double arithmetic.
+void mt_camera_create(const double from[3], const double at[3], const double up[3], double vfov_deg, double aspect,
+                      mt_camera *out)
+{
+    if (!out) return;
+    memset(out, 0, sizeof *out);
+    double fwd_raw[3] = {at[0] - from[0], at[1] - from[1], at[2] - from[2]};
+    double forward[3];
+    normalize3(fwd_raw, forward);
+    if (forward[0] * forward[0] + forward[1] * forward[1] + forward[2] * forward[2] <= 1e-12) {
+        forward[0] = 0.0;
+        forward[1] = 0.0;
+        forward[2] = -1.0;
+    }
+    auto cross3 = [](const double *a, const double *b, double *o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    double right[3];
+    cross3(forward, up, right);
+    if (right[0] * right[0] + right[1] * right[1] + right[2] * right[2] <= 1e-12) {
+        double fb[3] = {0.0, 1.0, 0.0};
+        if (!(fabs(forward[1]) < 0.99)) {
+            fb[0] = 1.0;
+            fb[1] = 0.0;
+        }
+        cross3(forward, fb, right);
+    }
+    double rn[3];
+    normalize3(right, rn);
+    double true_up[3];
+    cross3(rn, forward, true_up);
+    double vfov_rad = vfov_deg * (3.14159265358979323846 / 180.0);
+    double half_h = tan(vfov_rad * 0.5);
+    double half_w = aspect * half_h;
+    for (int k = 0; k < 3; ++k) {
+        out->position[k] = from[k];
+        out->horizontal[k] = rn[k] * (2.0 * half_w);
+        out->vertical[k] = true_up[k] * (2.0 * half_h);
+    }
+    for (int k = 0; k < 3; ++k) {
+        double a = from[k] + forward[k];
+        double b = out->horizontal[k] * 0.5 + out->vertical[k] * 0.5;
+        out->lower_left[k] = a - b;
+    }
+    out->aperture = 0.0;
+    double dd[3] = {at[0] - from[0], at[1] - from[1], at[2] - from[2]};
+    out->focus_distance = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+    out->dome_radius = 0.0;
+    out->anamorphic_squeeze = 1.0;
+}
+
+int mt_pathtrace_render(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, int depth, unsigned char *rgb)
+{
+    return render_host(sc, cam, w, h, spp, depth, RENDER_PT, OUT_RGB8, rgb);
+}
+
+int mt_render_image(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, int depth, unsigned char *rgb)
+{
+    return render_host(sc, cam, w, h, spp, depth, RENDER_WHITTED, OUT_RGB8, rgb);
+}
+
+int mt_render_image_ex(mt_scene *sc, const mt_camera *cam, int w, int h, const mt_render_params *p,
+                       unsigned char *rgb)
+{
+    if (p == nullptr) return fail(MT_ERR_NULL, "NULL params");
+    int rc = render_args(sc, cam, rgb, w, h, p->samples_per_pixel, p->max_depth);
+    if (rc) return rc;
+    if (p->adaptive) return mt_render_image_adaptive(sc, cam, w, h, p, rgb);
+    return render_host(sc, cam, w, h, p->samples_per_pixel, p->max_depth, RENDER_WHITTED, OUT_RGB8, rgb);
+}
+
+int mt_render_linear(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, int depth, int mode, float *out)
+{
+    if (mode != MT_MODE_PATHTRACE && mode != MT_MODE_WHITTED) return fail(MT_ERR_INVALID, "bad mode %d", mode);
+    return render_host(sc, cam, w, h, spp, depth, mode == MT_MODE_PATHTRACE ? RENDER_PT : RENDER_WHITTED,
+                       OUT_MEAN_F32, out);
+}
+
+int mt_render_accumulate_device(mt_scene *sc, const mt_camera *cam, int w, int h, int s0, int s1, int depth, int mode,
+                                float *accum_dev, int accumulate, void *stream)
+{
+    int rc = render_args(sc, cam, accum_dev, w, h, s1 - s0, depth);
+    if (rc) return rc;
+    if (s0 < 0) return fail(MT_ERR_COUNTS, "negative first sample");
+    if ((rc = set_device(sc))) return rc;
+    int out_kind = accumulate ? OUT_ADD_F32 : OUT_SUM_F32;
+    int m = mode == MT_MODE_PATHTRACE ? RENDER_PT : RENDER_WHITTED;
+    if (sc->opts.precision == MT_PRECISION_FP64)
+        return render_dev<double>(sc, cam, w, h, s1, s0, s1, depth, m, out_kind, accum_dev, (cudaStream_t)stream,
+                                  false);
+    return render_dev<float>(sc, cam, w, h, s1, s0, s1, depth, m, out_kind, accum_dev, (cudaStream_t)stream, false);
+}
+
+int mt_get_stats(const mt_scene *sc, mt_stats *out)
+{
+    if (!sc || !out) return fail(MT_ERR_NULL, "NULL pointer");
+    *out = sc->stats;
+    return 0;
+}
+
+int mt_set_counting(mt_scene *sc, int enable)
+{
+    if (!sc) return fail(MT_ERR_NULL, "NULL pointer");
+    sc->counting = enable != 0;
+    sc->sf.counters = nullptr;
+    sc->sd.counters = nullptr;
+    return reset_counters(sc);
+}
+
+int mt_pathtrace_radiance_mode(mt_scene *sc, int n, const double *o, const double *d, int depth,
+                               const uint32_t *seeds, double *out, int mode)
+{
+    if (!sc || !o || !d || !seeds || !out) return fail(MT_ERR_NULL, "NULL pointer");
+    if (n <= 0) return 0;
+    int rc = set_device(sc);
+    if (rc) return rc;
+    DevBuf<double> dO, dD, dOut;
+    DevBuf<unsigned> dS;
+    CK(dO.alloc(3 * (size_t)n), "cudaMalloc");
+    CK(dD.alloc(3 * (size_t)n), "cudaMalloc");
+    CK(dOut.alloc(3 * (size_t)n), "cudaMalloc");
+    CK(dS.alloc((size_t)n), "cudaMalloc");
+    CK(cudaMemcpy(dO.p, o, 3 * n * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    CK(cudaMemcpy(dD.p, d, 3 * n * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    CK(cudaMemcpy(dS.p, seeds, n * sizeof(unsigned), cudaMemcpyHostToDevice), "cudaMemcpy");
+    if (sc->opts.precision == MT_PRECISION_FP64)
+        CK(launch_radiance<double>(sc->sd, n, dO.p, dD.p, depth, dS.p, dOut.p, mode, 0), "radiance launch");
+    else
+        CK(launch_radiance<float>(sc->sf, n, dO.p, dD.p, depth, dS.p, dOut.p, mode, 0), "radiance launch");
+    CK(cudaDeviceSynchronize(), "radiance kernel");
+    CK(cudaMemcpy(out, dOut.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return check_err_word(sc);
+}
+
+int mt_pathtrace_radiance(mt_scene *sc, int n, const double *o, const double *d, int depth, const uint32_t *seeds,
+                          double *out)
+{
+    return mt_pathtrace_radiance_mode(sc, n, o, d, depth, seeds, out, RENDER_PT);
+}
+
+int mt_whitted_trace(mt_scene *sc, int n, const double *o, const double *d, int depth, const uint32_t *seeds,
+                     double *out)
+{
+    if (depth + 2 > kWhittedFrames) return fail(MT_ERR_UNSUPPORTED, "Whitted depth too large");
+    return mt_pathtrace_radiance_mode(sc, n, o, d, depth, seeds, out, RENDER_WHITTED);
+}
+
+int mt_intersect(mt_scene *sc, int n, const double *o, const double *d, double tmin, double tmax, int32_t *prim,
+                 double *t, double *normal, int32_t *front, int32_t *mat)
+{
+    if (!sc || !o || !d || !prim) return fail(MT_ERR_NULL, "NULL pointer");
+    if (n <= 0) return 0;
+    int rc = set_device(sc);
+    if (rc) return rc;
+    DevBuf<double> dO, dD, dT, dN;
+    DevBuf<int> dP, dF, dM;
+    CK(dO.alloc(3 * (size_t)n), "cudaMalloc");
+    CK(dD.alloc(3 * (size_t)n), "cudaMalloc");
+    CK(dT.alloc((size_t)n), "cudaMalloc");
+    CK(dN.alloc(3 * (size_t)n), "cudaMalloc");
+    CK(dP.alloc((size_t)n), "cudaMalloc");
+    CK(dF.alloc((size_t)n), "cudaMalloc");
+    CK(dM.alloc((size_t)n), "cudaMalloc");
+    CK(cudaMemcpy(dO.p, o, 3 * n * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    CK(cudaMemcpy(dD.p, d, 3 * n * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    if (sc->opts.precision == MT_PRECISION_FP64)
+        CK(launch_intersect<double>(sc->sd, n, dO.p, dD.p, tmin, tmax, dP.p, dT.p, dN.p, dF.p, dM.p, 0), "launch");
+    else
+        CK(launch_intersect<float>(sc->sf, n, dO.p, dD.p, tmin, tmax, dP.p, dT.p, dN.p, dF.p, dM.p, 0), "launch");
+    CK(cudaDeviceSynchronize(), "intersect kernel");
+    CK(cudaMemcpy(prim, dP.p, n * sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (t) CK(cudaMemcpy(t, dT.p, n * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (normal) CK(cudaMemcpy(normal, dN.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (front) CK(cudaMemcpy(front, dF.p, n * sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (mat) CK(cudaMemcpy(mat, dM.p, n * sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return check_err_word(sc);
+}
+
+int mt_occluded(mt_scene *sc, int n, const double *o, const double *d, double tmin, double tmax, int32_t *occ)
+{
+    if (!sc || !o || !d || !occ) return fail(MT_ERR_NULL, "NULL pointer");
+    if (n <= 0) return 0;
+    int rc = set_device(sc);
+    if (rc) return rc;
+    DevBuf<double> dO, dD;
+    DevBuf<int> dOcc;
+    CK(dO.alloc(3 * (size_t)n), "cudaMalloc");
+    CK(dD.alloc(3 * (size_t)n), "cudaMalloc");
+    CK(dOcc.alloc((size_t)n), "cudaMalloc");
+    CK(cudaMemcpy(dO.p, o, 3 * n * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    CK(cudaMemcpy(dD.p, d, 3 * n * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    if (sc->opts.precision == MT_PRECISION_FP64)
+        CK(launch_occluded<double>(sc->sd, n, dO.p, dD.p, tmin, tmax, dOcc.p, 0), "launch");
+    else
+        CK(launch_occluded<float>(sc->sf, n, dO.p, dD.p, tmin, tmax, dOcc.p, 0), "launch");
+    CK(cudaDeviceSynchronize(), "occluded kernel");
+    CK(cudaMemcpy(occ, dOcc.p, n * sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return check_err_word(sc);
+}
+
+int mt_primary_rays(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, int mode, double *out)
+{
+    int rc = render_args(sc, cam, out, w, h, spp, 0);
+    if (rc) return rc;
+    if ((rc = set_device(sc))) return rc;
+    size_t n = (size_t)w * h * spp;
+    DevBuf<double> dR;
+    CK(dR.alloc(6 * n), "cudaMalloc");
+    int m = mode == MT_MODE_PATHTRACE ? RENDER_PT : RENDER_WHITTED;
+    if (sc->opts.precision == MT_PRECISION_FP64) {
+        DevCamera<double> dc;
+        fill_camera(cam, &dc);
+        CK(launch_primary<double>(sc->sd, dc, w, h, spp, m, dR.p, 0), "launch");
+    } else {
+        DevCamera<float> dc;
+        fill_camera(cam, &dc);
+        CK(launch_primary<float>(sc->sf, dc, w, h, spp, m, dR.p, 0), "launch");
+    }
+    CK(cudaDeviceSynchronize(), "primary kernel");
+    CK(cudaMemcpy(out, dR.p, 6 * n * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return 0;
+}
+
+}  // extern "C"

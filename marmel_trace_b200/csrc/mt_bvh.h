@@ -1,0 +1,47 @@
+// mt_bvh.h - host BVH builder and device-layout flattening.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/mtgpu.h"
+
+namespace mt {
+
+// Binary node in the reference's layout and order (BvhNode, src/bvh.c:50-57).
+struct HostNode {
+    double mn[3], mx[3];
+    int left, right, first, count;
+};
+
+struct HostBvh {
+    std::vector<HostNode> nodes;   // preorder, node 0 = root
+    std::vector<int> order;        // leaf-ordered prim indices (tree prims)
+    std::vector<int> planes;       // plane prim indices, file order
+    int depth = 0;                 // leaf depth, root = 1
+};
+
+// primitive_bounds (src/geometry.c:1503-1584) for the kinds on the GPU path.
+void prim_bounds(const mt_prim &p, double mn[3], double mx[3]);
+
+// bvh_build (src/bvh.c:364-422): binned SAH over 12 bins, leaf <= 4 prims,
+// median fallback, planes in a side list. Deterministic and identical to the
+// reference builder for the same primitive array.
+int build_bvh(const mt_prim *prims, int n, HostBvh *out);
+
+// Device-ready flattened tree (see mt_layout.h for the node record).
+struct FlatBvh {
+    std::vector<float> nodes;      // 16 floats per node (q0..q3; q3 holds ints)
+    std::vector<int> ref_prim;     // leaf-ordered prim index
+    int node_count = 0;
+    int depth = 0;                 // depth of the flattened inner-node tree
+};
+
+// Flatten `b` into two-child nodes with FP32 boxes rounded outward. Leaves
+// of more than 7 prims (the reference's coincident-centroid leaves) are split
+// into small subtrees with the same box; nearest-hit results do not depend on
+// the tree shape.
+int flatten_bvh(const HostBvh &b, FlatBvh *out);
+
+}  // namespace mt

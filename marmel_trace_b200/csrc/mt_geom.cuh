@@ -1,0 +1,779 @@
+// mt_geom.cuh - ray / primitive tests and BVH traversal.
+//
+// FP64 instantiation: the reference's tests restated operation by operation
+// (src/geometry.c:338-699,705-800,1373-1451) so hits, distances and normals
+// agree bit for bit.
+// FP32 instantiation: the same acceptance rules with two numerically robust
+// tests in place of the textbook forms:
+//   * triangles use the watertight test of Woop, Benthin and Wald, "Watertight
+//     Ray/Triangle Intersection", JCGT 2(1), 2013 (shear to the ray's dominant
+//     axis, 2D edge functions; no cracks along shared edges);
+//   * spheres use the perpendicular-distance discriminant of Haines et al.,
+//     "Precision Improvements for Ray/Sphere Intersection", Ray Tracing Gems
+//     ch. 7, 2019, which avoids the |o-c|^2 - r^2 cancellation.
+#pragma once
+
+#include "mt_layout.h"
+#include "mt_math.cuh"
+
+namespace mt {
+
+template <typename R> struct Hit {
+    R t;
+    R u, v;       // triangle barycentrics (weights of b and c)
+    int prim;     // reference prim_index
+    int code;     // kind << 28 | slot
+};
+
+// Per-ray precomputation shared by every node and primitive test.
+template <typename R> struct RayPre {
+    V3<R> o, d, inv;
+    // watertight-triangle shear (FP32 path)
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+template <typename R> MT_D RayPre<R> ray_pre(V3<R> o, V3<R> d)
+{
+    RayPre<R> p;
+    p.o = o;
+    p.d = d;
+    // 1/dir per component (src/bvh.c:571): IEEE infinities for zero components.
+    p.inv = v3<R>(R(1) / d.x, R(1) / d.y, R(1) / d.z);
+    float ax = fabsf((float)d.x), ay = fabsf((float)d.y), az = fabsf((float)d.z);
+    int kz = (ax > ay) ? ((ax > az) ? 0 : 2) : ((ay > az) ? 1 : 2);
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    float dz = kz == 0 ? (float)d.x : (kz == 1 ? (float)d.y : (float)d.z);
+    if (dz < 0.0f) {
+        int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    float dx = kx == 0 ? (float)d.x : (kx == 1 ? (float)d.y : (float)d.z);
+    float dy = ky == 0 ? (float)d.x : (ky == 1 ? (float)d.y : (float)d.z);
+    p.kx = kx;
+    p.ky = ky;
+    p.kz = kz;
+    p.sx = dx / dz;
+    p.sy = dy / dz;
+    p.sz = 1.0f / dz;
+    return p;
+}
+
+template <typename R> MT_D R comp(V3<R> v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+MT_D float comp4(float4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// ------------------------------------------------------------------
+// Spheres (intersect_sphere src/geometry.c:338-369, occluded_sphere :1373-1381)
+// ------------------------------------------------------------------
+MT_D bool sphere_t(const double *s, const RayPre<double> &rp, double tmin, double tmax, double *t_out)
+{
+    double radius = s[3];
+    if (radius <= 0.0) return false;
+    V3<double> l = sub(rp.o, v3(s[0], s[1], s[2]));
+    double half_b = dot(l, rp.d);
+    double c = length_sq(l) - radius * radius;
+    double disc = half_b * half_b - c;
+    if (disc < 0.0) return false;
+    double sq = sqrt(disc);
+    double t = -half_b - sq;
+    if (t < tmin) {
+        t = -half_b + sq;
+        if (t < tmin || t > tmax) return false;
+    } else if (t > tmax) {
+        return false;
+    }
+    *t_out = t;
+    return true;
+}
+
+MT_D bool sphere_t(const float *s, const RayPre<float> &rp, float tmin, float tmax, float *t_out)
+{
+    float radius = s[3];
+    if (radius <= 0.0f) return false;
+    V3<float> f = sub(rp.o, v3(s[0], s[1], s[2]));
+    float b = -dot(f, rp.d);
+    V3<float> l = add(f, scale(rp.d, b));           // component of f perpendicular to d
+    float r2 = radius * radius;
+    float disc = r2 - dot(l, l);
+    if (disc < 0.0f) return false;
+    float q = b + copysignf(sqrtf(disc), b);
+    float c = dot(f, f) - r2;
+    float t0, t1;
+    if (q == 0.0f) {
+        t0 = t1 = 0.0f;
+    } else {
+        t0 = c / q;
+        t1 = q;
+    }
+    if (t0 > t1) {
+        float tt = t0;
+        t0 = t1;
+        t1 = tt;
+    }
+    float t = t0;
+    if (t < tmin) {
+        t = t1;
+        if (t < tmin || t > tmax) return false;
+    } else if (t > tmax) {
+        return false;
+    }
+    *t_out = t;
+    return true;
+}
+
+// ------------------------------------------------------------------
+// Planes (intersect_plane src/geometry.c:372-393); the unit normal is
+// precomputed on the host with vec3_normalize's exact arithmetic.
+// ------------------------------------------------------------------
+template <typename R>
+MT_D bool plane_t(const R *p, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out)
+{
+    V3<R> n = v3(p[3], p[4], p[5]);
+    R denom = dot(d, n);
+    if (mfabs(denom) < R(1e-12)) return false;
+    R t = dot(sub(v3(p[0], p[1], p[2]), o), n) / denom;
+    if (t < tmin || t > tmax) return false;
+    *t_out = t;
+    return true;
+}
+
+// ------------------------------------------------------------------
+// Boxes: slab method with entry/exit face (intersect_box src/geometry.c:396-479)
+// and the any-hit variant (occluded_box :1392-1411), which orders its slab
+// distances with a swap instead of fmin/fmax.
+// ------------------------------------------------------------------
+template <typename R>
+MT_D bool box_t(const R *b, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out, int *axis_out, int *sign_out)
+{
+    R lo[3] = {b[0] - b[3], b[1] - b[4], b[2] - b[5]};
+    R hi[3] = {b[0] + b[3], b[1] + b[4], b[2] + b[5]};
+    R oo[3] = {o.x, o.y, o.z};
+    R dd[3] = {d.x, d.y, d.z};
+    R tn = -INFINITY, tf = INFINITY;
+    int entry_axis = -1, entry_sign = 0, exit_axis = -1, exit_sign = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R inv = R(1) / dd[i];
+        R t1 = (lo[i] - oo[i]) * inv;
+        R t2 = (hi[i] - oo[i]) * inv;
+        R t_near = mfmin(t1, t2);
+        R t_far = mfmax(t1, t2);
+        if (t_near > tn) {
+            tn = t_near;
+            entry_axis = i;
+            entry_sign = (inv > R(0)) ? -1 : 1;
+        }
+        if (t_far < tf) {
+            tf = t_far;
+            exit_axis = i;
+            exit_sign = (inv > R(0)) ? 1 : -1;
+        }
+        if (tf < tn) return false;
+    }
+    if (tn >= tmin && tn <= tmax) {
+        *t_out = tn;
+        *axis_out = entry_axis;
+        *sign_out = entry_sign;
+        return true;
+    }
+    if (tf >= tmin && tf <= tmax) {
+        *t_out = tf;
+        *axis_out = exit_axis;
+        *sign_out = exit_sign;
+        return true;
+    }
+    return false;
+}
+
+template <typename R> MT_D bool box_occluded(const R *b, V3<R> o, V3<R> d, R tmin, R tmax)
+{
+    R lo[3] = {b[0] - b[3], b[1] - b[4], b[2] - b[5]};
+    R hi[3] = {b[0] + b[3], b[1] + b[4], b[2] + b[5]};
+    R oo[3] = {o.x, o.y, o.z};
+    R dd[3] = {d.x, d.y, d.z};
+    R tn = -INFINITY, tf = INFINITY;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R inv = R(1) / dd[i];
+        R t1 = (lo[i] - oo[i]) * inv;
+        R t2 = (hi[i] - oo[i]) * inv;
+        if (t1 > t2) {
+            R tmp = t1;
+            t1 = t2;
+            t2 = tmp;
+        }
+        if (t1 > tn) tn = t1;
+        if (t2 < tf) tf = t2;
+        if (tn > tf) return false;
+    }
+    return (tn >= tmin && tn <= tmax) || (tf >= tmin && tf <= tmax);
+}
+
+// ------------------------------------------------------------------
+// Tapered capped cylinder (intersect_cylinder src/geometry.c:549-699).
+// Returns t and the outward normal (before facing the ray).
+// ------------------------------------------------------------------
+template <typename R>
+MT_D bool cylinder_hit(const R *c, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out, V3<R> *n_out)
+{
+    V3<R> pa = v3(c[0], c[1], c[2]);
+    V3<R> pb = v3(c[3], c[4], c[5]);
+    V3<R> A = sub(pb, pa);
+    R h = length(A);
+    if (h < R(1e-12)) return false;
+    V3<R> axis = scale(A, R(1) / h);
+    R r0 = c[6], r1 = c[7];
+    R k = (r1 - r0) / h;
+    V3<R> d0 = sub(o, pa);
+    R Od = dot(d, axis);
+    R d0d = dot(d0, axis);
+    V3<R> D_perp = sub(d, scale(axis, Od));
+    V3<R> d0_perp = sub(d0, scale(axis, d0d));
+    R ra = k * Od;
+    R rb = r0 + k * d0d;
+    R qa = length_sq(D_perp) - ra * ra;
+    R qb = dot(D_perp, d0_perp) - rb * ra;
+    R qc = length_sq(d0_perp) - rb * rb;
+
+    bool found = false;
+    R best_t = R(0);
+    V3<R> best_n = v3(R(0), R(0), R(0));
+
+    if (mfabs(qa) > R(1e-15)) {
+        R disc = qb * qb - qa * qc;
+        if (disc >= R(0)) {
+            R sq = msqrt(disc);
+            R roots[2];
+            roots[0] = (-qb - sq) / qa;
+            roots[1] = (-qb + sq) / qa;
+            if (roots[0] > roots[1]) {
+                R tmp = roots[0];
+                roots[0] = roots[1];
+                roots[1] = tmp;
+            }
+            for (int i = 0; i < 2; ++i) {
+                R t = roots[i];
+                if (t < tmin || t > tmax) continue;
+                R s = (d0d + t * Od) / h;
+                if (s < R(0) || s > R(1)) continue;
+                V3<R> point = at(o, d, t);
+                V3<R> axis_pt = add(pa, scale(axis, s * h));
+                V3<R> radial = sub(point, axis_pt);
+                R rlen = length(radial);
+                V3<R> radial_dir = (rlen > R(1e-15)) ? scale(radial, R(1) / rlen) : v3(R(0), R(0), R(0));
+                V3<R> n = sub(scale(radial_dir, h), scale(axis, r1 - r0));
+                n = normalize(n);
+                if (length_sq(n) < R(0.5)) n = radial_dir;
+                if (!found || t < best_t) {
+                    found = true;
+                    best_t = t;
+                    best_n = n;
+                }
+            }
+        }
+    } else if (mfabs(qb) > R(1e-15)) {
+        R t = -qc / (R(2) * qb);
+        if (t >= tmin && t <= tmax) {
+            R s = (d0d + t * Od) / h;
+            if (s >= R(0) && s <= R(1)) {
+                V3<R> point = at(o, d, t);
+                V3<R> axis_pt = add(pa, scale(axis, s * h));
+                V3<R> radial = sub(point, axis_pt);
+                V3<R> radial_dir = normalize(radial);
+                V3<R> n = sub(scale(radial_dir, h), scale(axis, r1 - r0));
+                n = normalize(n);
+                if (length_sq(n) < R(0.5)) n = radial_dir;
+                found = true;
+                best_t = t;
+                best_n = n;
+            }
+        }
+    }
+    if (mfabs(Od) > R(1e-15)) {
+        for (int cap = 0; cap < 2; ++cap) {
+            R s_cap = (cap == 0) ? R(0) : R(1);
+            R r_cap = (cap == 0) ? r0 : r1;
+            if (r_cap <= R(0)) continue;
+            V3<R> cap_center = (cap == 0) ? pa : pb;
+            R t = ((s_cap * h) - d0d) / Od;
+            if (t < tmin || t > tmax) continue;
+            V3<R> point = at(o, d, t);
+            V3<R> radial = sub(point, cap_center);
+            if (length_sq(radial) > r_cap * r_cap) continue;
+            V3<R> n = (cap == 0) ? neg(axis) : axis;
+            if (!found || t < best_t) {
+                found = true;
+                best_t = t;
+                best_n = n;
+            }
+        }
+    }
+    if (!found) return false;
+    *t_out = best_t;
+    *n_out = best_n;
+    return true;
+}
+
+// ------------------------------------------------------------------
+// Triangles
+// ------------------------------------------------------------------
+// FP64: Moller-Trumbore, two-sided, det guard 1e-9, barycentric slack 1e-9
+// (intersect_triangle src/geometry.c:482-538 / occluded_triangle :1414-1433).
+MT_D bool tri_t(const DevScene<double> &S, int slot, const RayPre<double> &rp, double tmin, double tmax,
+                double *t_out, double *u_out, double *v_out)
+{
+    const double *T = S.tris + 9 * (size_t)slot;
+    V3<double> a = v3(T[0], T[1], T[2]);
+    V3<double> e1 = v3(T[3], T[4], T[5]);
+    V3<double> e2 = v3(T[6], T[7], T[8]);
+    V3<double> pvec = cross(rp.d, e2);
+    double det = dot(e1, pvec);
+    if (fabs(det) < 1e-9) return false;
+    double inv_det = 1.0 / det;
+    V3<double> tvec = sub(rp.o, a);
+    double u = dot(tvec, pvec) * inv_det;
+    if (u < -1e-9 || u > 1.0 + 1e-9) return false;
+    V3<double> qvec = cross(tvec, e1);
+    double v = dot(rp.d, qvec) * inv_det;
+    if (v < -1e-9 || u + v > 1.0 + 1e-9) return false;
+    double t = dot(e2, qvec) * inv_det;
+    if (t < tmin || t > tmax) return false;
+    *t_out = t;
+    *u_out = u;
+    *v_out = v;
+    return true;
+}
+
+// FP32: watertight test (Woop, Benthin, Wald 2013). Vertices are stored
+// relative to nothing (v0, v1, v2) so the shear is applied to exact
+// differences from the ray origin.
+MT_D bool tri_t(const DevScene<float> &S, int slot, const RayPre<float> &rp, float tmin, float tmax,
+                float *t_out, float *u_out, float *v_out)
+{
+    const float4 *T = S.tri4 + 3 * (size_t)slot;
+    float4 q0 = __ldg(T), q1 = __ldg(T + 1), q2 = __ldg(T + 2);
+    float Akx = comp4(q0, rp.kx) - comp(rp.o, rp.kx), Aky = comp4(q0, rp.ky) - comp(rp.o, rp.ky),
+          Akz = comp4(q0, rp.kz) - comp(rp.o, rp.kz);
+    float Bkx = comp4(q1, rp.kx) - comp(rp.o, rp.kx), Bky = comp4(q1, rp.ky) - comp(rp.o, rp.ky),
+          Bkz = comp4(q1, rp.kz) - comp(rp.o, rp.kz);
+    float Ckx = comp4(q2, rp.kx) - comp(rp.o, rp.kx), Cky = comp4(q2, rp.ky) - comp(rp.o, rp.ky),
+          Ckz = comp4(q2, rp.kz) - comp(rp.o, rp.kz);
+    float Ax = Akx - rp.sx * Akz, Ay = Aky - rp.sy * Akz;
+    float Bx = Bkx - rp.sx * Bkz, By = Bky - rp.sy * Bkz;
+    float Cx = Ckx - rp.sx * Ckz, Cy = Cky - rp.sy * Ckz;
+    float U = Cx * By - Cy * Bx;
+    float V = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        // Edge case of the paper: re-evaluate the edge functions in double.
+        U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = U + V + W;
+    if (det == 0.0f) return false;
+    float Az = rp.sz * Akz, Bz = rp.sz * Bkz, Cz = rp.sz * Ckz;
+    float T_ = U * Az + V * Bz + W * Cz;
+    float rcp = 1.0f / det;
+    float t = T_ * rcp;
+    if (!(t >= tmin && t <= tmax)) return false;
+    *t_out = t;
+    *u_out = V * rcp;
+    *v_out = W * rcp;
+    return true;
+}
+
+// ------------------------------------------------------------------
+// Generic primitive tests by code (kind << 28 | slot)
+// ------------------------------------------------------------------
+template <typename R>
+MT_D bool prim_hit_t(const DevScene<R> &S, int code, const RayPre<R> &rp, R tmin, R tmax, R *t, R *u, R *v)
+{
+    int kind = code >> 28;
+    int slot = code & 0x0FFFFFFF;
+    *u = R(0);
+    *v = R(0);
+    switch (kind) {
+    case KIND_TRIANGLE:
+        return tri_t(S, slot, rp, tmin, tmax, t, u, v);
+    case KIND_SPHERE:
+        return sphere_t(S.spheres + 4 * (size_t)slot, rp, tmin, tmax, t);
+    case KIND_BOX: {
+        int ax, sg;
+        return box_t(S.boxes + 6 * (size_t)slot, rp.o, rp.d, tmin, tmax, t, &ax, &sg);
+    }
+    case KIND_CYLINDER: {
+        V3<R> n;
+        return cylinder_hit(S.cyls + 8 * (size_t)slot, rp.o, rp.d, tmin, tmax, t, &n);
+    }
+    default:
+        return false;
+    }
+}
+
+template <typename R>
+MT_D bool prim_occluded(const DevScene<R> &S, int code, const RayPre<R> &rp, R tmin, R tmax)
+{
+    int kind = code >> 28;
+    int slot = code & 0x0FFFFFFF;
+    R t, u, v;
+    switch (kind) {
+    case KIND_TRIANGLE:
+        return tri_t(S, slot, rp, tmin, tmax, &t, &u, &v);
+    case KIND_SPHERE:
+        return sphere_t(S.spheres + 4 * (size_t)slot, rp, tmin, tmax, &t);
+    case KIND_BOX:
+        return box_occluded(S.boxes + 6 * (size_t)slot, rp.o, rp.d, tmin, tmax);
+    case KIND_CYLINDER: {
+        V3<R> n;
+        return cylinder_hit(S.cyls + 8 * (size_t)slot, rp.o, rp.d, tmin, tmax, &t, &n);
+    }
+    default:
+        return false;
+    }
+}
+
+// ------------------------------------------------------------------
+// Two-child slab test on one 64-byte node (bvh_slab_2way, src/bvh.c:495-533).
+// ------------------------------------------------------------------
+template <typename R>
+MT_D void node_test(const float4 q0, const float4 q1, const float4 q2, const RayPre<R> &rp, R tmin, R tmax,
+                    bool *hl, bool *hr, R *tl, R *tr)
+{
+    R lx0 = (R(q0.x) - rp.o.x) * rp.inv.x, lx1 = (R(q0.y) - rp.o.x) * rp.inv.x;
+    R ly0 = (R(q0.z) - rp.o.y) * rp.inv.y, ly1 = (R(q0.w) - rp.o.y) * rp.inv.y;
+    R lz0 = (R(q2.x) - rp.o.z) * rp.inv.z, lz1 = (R(q2.y) - rp.o.z) * rp.inv.z;
+    R rx0 = (R(q1.x) - rp.o.x) * rp.inv.x, rx1 = (R(q1.y) - rp.o.x) * rp.inv.x;
+    R ry0 = (R(q1.z) - rp.o.y) * rp.inv.y, ry1 = (R(q1.w) - rp.o.y) * rp.inv.y;
+    R rz0 = (R(q2.z) - rp.o.z) * rp.inv.z, rz1 = (R(q2.w) - rp.o.z) * rp.inv.z;
+    R lenter = mfmax(mfmax(mfmin(lx0, lx1), mfmin(ly0, ly1)), mfmin(lz0, lz1));
+    R lexit = mfmin(mfmin(mfmax(lx0, lx1), mfmax(ly0, ly1)), mfmax(lz0, lz1));
+    R renter = mfmax(mfmax(mfmin(rx0, rx1), mfmin(ry0, ry1)), mfmin(rz0, rz1));
+    R rexit = mfmin(mfmin(mfmax(rx0, rx1), mfmax(ry0, ry1)), mfmax(rz0, rz1));
+    *hl = (lexit >= lenter && lexit >= tmin && lenter <= tmax);
+    *hr = (rexit >= renter && rexit >= tmin && renter <= tmax);
+    *tl = lenter < tmin ? tmin : lenter;
+    *tr = renter < tmin ? tmin : renter;
+}
+
+MT_D void count_add(unsigned long long *p, unsigned long long v)
+{
+    if (v) atomicAdd(p, v);
+}
+
+// ------------------------------------------------------------------
+// Nearest hit in [tmin, tmax] with the reference's tie-break: equal t goes
+// to the LOWEST prim_index (bvh_intersect, src/bvh.c:557-712), planes first
+// (src/bvh.c:579-591). Front-to-back order with a per-ray stack of
+// (child, entry distance); a popped entry farther than the running closest
+// hit is culled with the reference's strict `>` (src/bvh.c:631).
+// ------------------------------------------------------------------
+template <typename R>
+MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best)
+{
+    bool found = false;
+    R closest = tmax;
+    unsigned long long nvis = 0, ntest = 0;
+
+    for (int i = 0; i < S.plane_count; ++i) {
+        R t;
+        ++ntest;
+        if (plane_t(S.planes + 6 * (size_t)i, rp.o, rp.d, tmin, closest, &t)) {
+            int pi = S.plane_prims[i];
+            if (!found || t < best->t || (t == best->t && pi < best->prim)) {
+                best->t = t;
+                best->u = R(0);
+                best->v = R(0);
+                best->prim = pi;
+                best->code = (KIND_PLANE << 28) | i;
+                closest = t;
+                found = true;
+            }
+        }
+    }
+
+    if (S.node_count > 0) {
+        int stk_node[kStackSize];
+        R stk_t[kStackSize];
+        int sp = 0;
+        stk_node[sp] = 0;
+        stk_t[sp] = tmin;
+        ++sp;
+        while (sp > 0) {
+            --sp;
+            int node = stk_node[sp];
+            R te = stk_t[sp];
+            if (found && te > closest) continue;
+            if (node >= 0) {
+                const float4 *N = S.nodes + 4 * (size_t)node;
+                float4 q0 = __ldg(N), q1 = __ldg(N + 1), q2 = __ldg(N + 2);
+                int4 q3 = __ldg(reinterpret_cast<const int4 *>(N + 3));
+                bool hl, hr;
+                R tl, tr;
+                ++nvis;
+                node_test(q0, q1, q2, rp, tmin, closest, &hl, &hr, &tl, &tr);
+                int cl = q3.x, cr = q3.y;
+                if (sp + 2 > kStackSize) {
+                    atomicOr(S.err, ERR_STACK);
+                    break;
+                }
+                if (hl && hr) {
+                    if (tl <= tr) {
+                        stk_node[sp] = cr; stk_t[sp] = tr; ++sp;
+                        stk_node[sp] = cl; stk_t[sp] = tl; ++sp;
+                    } else {
+                        stk_node[sp] = cl; stk_t[sp] = tl; ++sp;
+                        stk_node[sp] = cr; stk_t[sp] = tr; ++sp;
+                    }
+                } else if (hl) {
+                    stk_node[sp] = cl; stk_t[sp] = tl; ++sp;
+                } else if (hr) {
+                    stk_node[sp] = cr; stk_t[sp] = tr; ++sp;
+                }
+            } else {
+                int leaf = ~node;
+                int first = leaf >> 3, count = leaf & 7;
+                for (int i = 0; i < count; ++i) {
+                    int2 ref = __ldg(S.refs + first + i);
+                    R t, u, v;
+                    ++ntest;
+                    if (prim_hit_t(S, ref.y, rp, tmin, closest, &t, &u, &v)) {
+                        if (!found || t < best->t || (t == best->t && ref.x < best->prim)) {
+                            best->t = t;
+                            best->u = u;
+                            best->v = v;
+                            best->prim = ref.x;
+                            best->code = ref.y;
+                            closest = t;
+                            found = true;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (S.counters) {
+        count_add(&S.counters->node_visits, nvis);
+        count_add(&S.counters->prim_tests, ntest);
+    }
+    return found;
+}
+
+// Any hit in [tmin, tmax] (bvh_occluded src/bvh.c:714-813 with the
+// primitive_occluded tests). The reference's last-occluder cache only
+// reorders the tests, so it is not needed for the same boolean.
+template <typename R> MT_D bool scene_any(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax)
+{
+    unsigned long long nvis = 0, ntest = 0;
+    bool hit = false;
+    for (int i = 0; i < S.plane_count && !hit; ++i) {
+        R t;
+        ++ntest;
+        if (plane_t(S.planes + 6 * (size_t)i, rp.o, rp.d, tmin, tmax, &t)) hit = true;
+    }
+    if (!hit && S.node_count > 0) {
+        int stk[kStackSize];
+        int sp = 0;
+        stk[sp++] = 0;
+        while (sp > 0 && !hit) {
+            int node = stk[--sp];
+            if (node >= 0) {
+                const float4 *N = S.nodes + 4 * (size_t)node;
+                float4 q0 = __ldg(N), q1 = __ldg(N + 1), q2 = __ldg(N + 2);
+                int4 q3 = __ldg(reinterpret_cast<const int4 *>(N + 3));
+                bool hl, hr;
+                R tl, tr;
+                ++nvis;
+                node_test(q0, q1, q2, rp, tmin, tmax, &hl, &hr, &tl, &tr);
+                if (sp + 2 > kStackSize) {
+                    atomicOr(S.err, ERR_STACK);
+                    break;
+                }
+                if (hl && hr) {
+                    if (tl <= tr) {
+                        stk[sp++] = q3.y;
+                        stk[sp++] = q3.x;
+                    } else {
+                        stk[sp++] = q3.x;
+                        stk[sp++] = q3.y;
+                    }
+                } else if (hl) {
+                    stk[sp++] = q3.x;
+                } else if (hr) {
+                    stk[sp++] = q3.y;
+                }
+            } else {
+                int leaf = ~node;
+                int first = leaf >> 3, count = leaf & 7;
+                for (int i = 0; i < count; ++i) {
+                    int2 ref = __ldg(S.refs + first + i);
+                    ++ntest;
+                    if (prim_occluded(S, ref.y, rp, tmin, tmax)) {
+                        hit = true;
+                        break;
+                    }
+                }
+            }
+        }
+    }
+    if (S.counters) {
+        count_add(&S.counters->node_visits, nvis);
+        count_add(&S.counters->prim_tests, ntest);
+    }
+    return hit;
+}
+
+// scene_intersect / scene_occluded entry semantics: a direction that is not
+// unit length (|d|^2 off by more than 1e-12) is normalised first
+// (src/bvh.c:563-566, :720-723).
+template <typename R> MT_D V3<R> unit_dir(V3<R> d)
+{
+    R len_sq = length_sq(d);
+    if (len_sq > R(0) && mfabs(len_sq - R(1)) > R(1e-12)) d = normalize(d);
+    return d;
+}
+
+// Full hit record of the reference (Hit, src/geometry.h:74-83).
+template <typename R> struct SurfaceHit {
+    R t;
+    V3<R> point;
+    V3<R> normal;   // unit, facing the incoming ray
+    int prim;
+    int material;
+    int front_face;
+};
+
+// geo_store_hit (src/geometry.c:78-91): orient the unit normal against the ray.
+template <typename R>
+MT_D void store_hit(SurfaceHit<R> *out, R t, V3<R> point, V3<R> n, V3<R> d)
+{
+    bool front = dot(d, n) < R(0);
+    out->t = t;
+    out->point = point;
+    out->normal = front ? n : neg(n);
+    out->front_face = front ? 1 : 0;
+}
+
+// Recover point / normal / front face / material for a traversal hit.
+template <typename R>
+MT_D void finish_hit(const DevScene<R> &S, V3<R> o, V3<R> d, const Hit<R> &h, SurfaceHit<R> *out)
+{
+    int kind = h.code >> 28;
+    int slot = h.code & 0x0FFFFFFF;
+    out->prim = h.prim;
+    out->material = __ldg(S.prim_info + h.prim).y;
+    V3<R> point = at(o, d, h.t);
+    switch (kind) {
+    case KIND_SPHERE: {
+        const R *s = S.spheres + 4 * (size_t)slot;
+        V3<R> n = scale(sub(point, v3(s[0], s[1], s[2])), R(1) / s[3]);
+        store_hit(out, h.t, point, n, d);
+        break;
+    }
+    case KIND_PLANE: {
+        const R *p = S.planes + 6 * (size_t)slot;
+        store_hit(out, h.t, point, v3(p[3], p[4], p[5]), d);
+        break;
+    }
+    case KIND_BOX: {
+        R t;
+        int axis = -1, sign = 0;
+        box_t(S.boxes + 6 * (size_t)slot, o, d, h.t, h.t, &t, &axis, &sign);
+        V3<R> n;
+        if (axis < 0) {
+            n = neg(d);
+        } else {
+            n = v3(R(0), R(0), R(0));
+            if (axis == 0) n.x = R(sign);
+            else if (axis == 1) n.y = R(sign);
+            else n.z = R(sign);
+        }
+        store_hit(out, h.t, point, n, d);
+        break;
+    }
+    case KIND_CYLINDER: {
+        R t;
+        V3<R> n;
+        cylinder_hit(S.cyls + 8 * (size_t)slot, o, d, h.t, h.t, &t, &n);
+        store_hit(out, h.t, point, n, d);
+        break;
+    }
+    case KIND_TRIANGLE:
+    default: {
+        V3<R> e1, e2;
+        bool smooth;
+        if constexpr (sizeof(R) == 8) {
+            const R *T = S.tris + 9 * (size_t)slot;
+            e1 = v3(T[3], T[4], T[5]);
+            e2 = v3(T[6], T[7], T[8]);
+            smooth = S.tri_smooth[slot] != 0;
+        } else {
+            const float4 *T = S.tri4 + 3 * (size_t)slot;
+            float4 a = __ldg(T), b = __ldg(T + 1), c = __ldg(T + 2);
+            e1 = v3<R>(b.x - a.x, b.y - a.y, b.z - a.z);
+            e2 = v3<R>(c.x - a.x, c.y - a.y, c.z - a.z);
+            smooth = __float_as_int(b.w) != 0;
+        }
+        V3<R> n;
+        bool have = false;
+        if (smooth) {
+            const R *N = S.tri_normals + 9 * (size_t)slot;
+            R w = R(1) - h.u - h.v;
+            n = add(scale(v3(N[0], N[1], N[2]), w), add(scale(v3(N[3], N[4], N[5]), h.u), scale(v3(N[6], N[7], N[8]), h.v)));
+            R nlen = length(n);
+            if (nlen > R(1e-12)) {
+                n = scale(n, R(1) / nlen);
+                have = true;
+            }
+        }
+        if (!have) {
+            n = cross(e1, e2);
+            R nlen = length(n);
+            n = (nlen > R(0)) ? scale(n, R(1) / nlen) : v3(R(0), R(1), R(0));
+        }
+        store_hit(out, h.t, point, n, d);
+        break;
+    }
+    }
+}
+
+// scene_intersect (src/scene.c:767-775) with the full hit record.
+template <typename R>
+MT_D bool scene_intersect(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax, SurfaceHit<R> *out)
+{
+    d = unit_dir(d);
+    RayPre<R> rp = ray_pre(o, d);
+    Hit<R> h;
+    if (S.counters) atomicAdd(&S.counters->extension_rays, 1ull);
+    if (!scene_nearest(S, rp, tmin, tmax, &h)) return false;
+    finish_hit(S, o, d, h, out);
+    return true;
+}
+
+// scene_occluded (src/scene.c:804-811).
+template <typename R> MT_D bool scene_occluded(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax)
+{
+    d = unit_dir(d);
+    RayPre<R> rp = ray_pre(o, d);
+    if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
+    return scene_any(S, rp, tmin, tmax);
+}
+
+// primitive_intersect on one emissive-light sphere by prim_index
+// (src/pathtrace.c:594, src/render.c:536): only the distance is needed.
+template <typename R>
+MT_D bool light_sphere_t(const DevScene<R> &S, int prim, V3<R> o, V3<R> d, R tmin, R tmax, R *t)
+{
+    d = unit_dir(d);
+    int2 info = __ldg(S.prim_info + prim);
+    int slot = info.x & 0x0FFFFFFF;
+    RayPre<R> rp;
+    rp.o = o;
+    rp.d = d;
+    return sphere_t(S.spheres + 4 * (size_t)slot, rp, tmin, tmax, t);
+}
+
+}  // namespace mt

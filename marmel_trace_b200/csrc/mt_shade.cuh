@@ -1,0 +1,582 @@
+// mt_shade.cuh - materials, procedural sky, noise, water and BSDF sampling.
+//
+// Each function restates the reference function cited beside it in the
+// reference's expression order, so the FP64 instantiation reproduces the
+// reference's doubles; the FP32 instantiation evaluates the same formulas in
+// single precision with CUDA's float math functions.
+#pragma once
+
+#include "mt_geom.cuh"
+
+namespace mt {
+
+template <typename R> MT_D V3<R> mat3(const R *p) { return v3(p[0], p[1], p[2]); }
+
+// ------------------------------------------------------------------
+// Noise (src/noise.c:31-55,158-187,272-294)
+// ------------------------------------------------------------------
+MT_D uint32_t noise_mix(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+MT_D uint32_t noise_hash(int x, int y, int z, uint32_t seed)
+{
+    uint32_t h = seed + 0x9e3779b9u;
+    h ^= (uint32_t)x * 0x85ebca6bu;
+    h ^= (uint32_t)y * 0xc2b2ae35u;
+    h ^= (uint32_t)z * 0x27d4eb2fu;
+    return noise_mix(h);
+}
+
+template <typename R> MT_D R noise_rand01(int x, int y, int z, uint32_t seed)
+{
+    return R(noise_hash(x, y, z, seed)) / R(4294967295.0);
+}
+
+template <typename R> MT_D R noise_fade(R t) { return t * t * t * (t * (t * R(6) - R(15)) + R(10)); }
+template <typename R> MT_D R noise_lerp(R a, R b, R t) { return a + t * (b - a); }
+template <typename R> MT_D R noise_clamp(R v, R lo, R hi)
+{
+    if (v < lo) return lo;
+    if (v > hi) return hi;
+    return v;
+}
+
+// noise_perlin2 (src/noise.c:158-187)
+template <typename R> MT_D R noise_perlin2(R x, R y, uint32_t seed)
+{
+    R fx = mfloor(x);
+    R fy = mfloor(y);
+    int ix = (int)fx;
+    int iy = (int)fy;
+    R rx = x - fx;
+    R ry = y - fy;
+    R u = noise_fade(rx);
+    R v = noise_fade(ry);
+    const R tp = R(2) * Const<R>::pi;
+    R a00 = noise_rand01<R>(ix, iy, 0, seed) * tp;
+    R a10 = noise_rand01<R>(ix + 1, iy, 0, seed) * tp;
+    R a01 = noise_rand01<R>(ix, iy + 1, 0, seed) * tp;
+    R a11 = noise_rand01<R>(ix + 1, iy + 1, 0, seed) * tp;
+    R s00, c00, s10, c10, s01, c01, s11, c11;
+    msincos(a00, &s00, &c00);
+    msincos(a10, &s10, &c10);
+    msincos(a01, &s01, &c01);
+    msincos(a11, &s11, &c11);
+    R d00 = c00 * rx + s00 * ry;
+    R d10 = c10 * (rx - R(1)) + s10 * ry;
+    R d01 = c01 * rx + s01 * (ry - R(1));
+    R d11 = c11 * (rx - R(1)) + s11 * (ry - R(1));
+    R x0 = noise_lerp(d00, d10, u);
+    R x1 = noise_lerp(d01, d11, u);
+    R val = noise_lerp(x0, x1, v);
+    return noise_clamp(val * R(1.4142135623730951), R(-1), R(1));
+}
+
+// noise_fbm2 with lacunarity 2 and gain 0.5 (src/noise.c:272-294)
+template <typename R> MT_D R noise_fbm2(R x, R y, int octaves, uint32_t seed)
+{
+    int n = octaves <= 0 ? 1 : octaves;
+    R amp = R(1), freq = R(1), sum = R(0), norm = R(0);
+    for (int i = 0; i < n; ++i) {
+        sum += amp * noise_perlin2(x * freq, y * freq, seed);
+        norm += amp;
+        amp *= R(0.5);
+        freq *= R(2);
+    }
+    if (norm <= R(0)) return R(0);
+    return noise_clamp(sum / norm, R(-1), R(1));
+}
+
+// ------------------------------------------------------------------
+// Sky (sky_sample, src/material.c:473-600,956: gradient, sun glow, planar
+// clouds; the volumetric/star/nebula/galaxy branches are rejected on upload)
+// ------------------------------------------------------------------
+template <typename R> MT_D R smoothstep(R e0, R e1, R x)
+{
+    R denom = e1 - e0;
+    if (denom == R(0)) return x < e0 ? R(0) : R(1);
+    R t = mat_clamp01((x - e0) / denom);
+    return t * t * (R(3) - R(2) * t);
+}
+
+template <typename R> MT_D R pow_nonneg(R base, R e)
+{
+    if (base <= R(0)) return R(0);
+    return mpow(base, e);
+}
+
+template <typename R> MT_D V3<R> sky_sample(V3<R> dir, const DevSky<R> &sky)
+{
+    R h = mat_clamp01(dir.y);
+    R t = pow_nonneg(h, sky.gradient_gamma);
+    V3<R> base = lerp(mat3(sky.horizon_color), mat3(sky.zenith_color), t);
+    V3<R> sun_color = mat3(sky.sun_color);
+    R cos_sun = dot(dir, mat3(sky.sun_dir));
+    if (cos_sun > R(0)) {
+        R glow = pow_nonneg(cos_sun, sky.sun_glow_exponent) * sky.sun_glow_strength;
+        base = add(base, scale(sun_color, glow));
+    }
+    if (dir.y > R(0.03)) {
+        R tt = sky.cloud_height / dir.y;
+        R px = dir.x * tt;
+        R pz = dir.z * tt;
+        int octaves = sky.cloud_octaves;
+        if (octaves < 1) octaves = 1;
+        R raw = noise_fbm2(px * sky.cloud_scale, pz * sky.cloud_scale, octaves, sky.seed);
+        R density = mat_clamp01(R(0.5) * (raw + R(1)));
+        R a = sky.cloud_coverage - sky.cloud_softness;
+        R b = sky.cloud_coverage + sky.cloud_softness;
+        R alpha = smoothstep(a, b, density);
+        alpha = pow_nonneg(alpha, sky.cloud_sharpness);
+        alpha *= smoothstep(R(0), R(0.15), dir.y);
+        if (alpha > R(0)) {
+            R shadow = R(0.6) + R(0.4) * alpha;
+            V3<R> cloud_color = scale(v3(R(0.95), R(0.95), R(0.98)), shadow);
+            R lit = cos_sun > R(0) ? cos_sun : R(0);
+            V3<R> lit_cloud = add(cloud_color, scale(mul(cloud_color, sun_color), R(0.35) * lit));
+            base = lerp(base, lit_cloud, alpha);
+        }
+    }
+    if (!(base.x >= R(0))) base.x = R(0);
+    if (!(base.y >= R(0))) base.y = R(0);
+    if (!(base.z >= R(0))) base.z = R(0);
+    return base;
+}
+
+// sky_basis / sampling_basis: least-aligned world axis, Gram-Schmidt
+// (src/material.c:1062-1075, src/sampling.c:52-77; the caller normalises n).
+template <typename R> MT_D void basis(V3<R> n, V3<R> *t, V3<R> *b)
+{
+    V3<R> axis;
+    if (mfabs(n.x) <= mfabs(n.y) && mfabs(n.x) <= mfabs(n.z)) axis = v3(R(1), R(0), R(0));
+    else if (mfabs(n.y) <= mfabs(n.z)) axis = v3(R(0), R(1), R(0));
+    else axis = v3(R(0), R(0), R(1));
+    *t = normalize(cross(axis, n));
+    *b = cross(n, *t);
+}
+
+// sky_sun_disk_dir (src/material.c:1077-1107)
+template <typename R> MT_D V3<R> sun_disk_dir(V3<R> sun_dir, R radius_deg, R r1, R r2)
+{
+    if (radius_deg <= R(0)) return sun_dir;
+    V3<R> n = normalize(sun_dir);
+    if (length_sq(n) == R(0)) return v3(R(0), R(1), R(0));
+    if (r1 < R(0)) r1 = R(0); else if (r1 > R(1)) r1 = R(1);
+    if (r2 < R(0)) r2 = R(0); else if (r2 > R(1)) r2 = R(1);
+    R radius_rad = radius_deg * (Const<R>::pi / R(180));
+    R offset = msqrt(r1) * radius_rad;
+    R theta = R(2) * Const<R>::pi * r2;
+    V3<R> t, b;
+    basis(n, &t, &b);
+    R st, ct;
+    msincos(theta, &st, &ct);
+    V3<R> radial = add(scale(t, ct), scale(b, st));
+    V3<R> dir = add(n, scale(radial, mtan(offset)));
+    return normalize(dir);
+}
+
+// light_sphere_sample_dir (src/material.c:1113-1146)
+template <typename R> MT_D V3<R> light_sphere_sample_dir(V3<R> w, R cos_alpha_max, R u1, R u2)
+{
+    const R rmax = sizeof(R) == 8 ? R(0.9999999999999999) : R(0.99999994f);
+    w = normalize(w);
+    if (length_sq(w) == R(0)) return v3(R(0), R(1), R(0));
+    if (!(cos_alpha_max >= R(0))) cos_alpha_max = R(0);
+    else if (cos_alpha_max > R(1)) cos_alpha_max = R(1);
+    if (!(u1 > R(0))) u1 = R(0);
+    else if (u1 > rmax) u1 = rmax;
+    if (!(u2 > R(0))) u2 = R(0);
+    else if (u2 > rmax) u2 = rmax;
+    R cos_alpha = R(1) - u1 * (R(1) - cos_alpha_max);
+    R sin_alpha = msqrt(R(1) - cos_alpha * cos_alpha);
+    R phi = R(2) * Const<R>::pi * u2;
+    V3<R> t, b;
+    basis(w, &t, &b);
+    R sp, cp;
+    msincos(phi, &sp, &cp);
+    V3<R> dir = add(add(scale(t, sin_alpha * cp), scale(b, sin_alpha * sp)), scale(w, cos_alpha));
+    return normalize(dir);
+}
+
+// ------------------------------------------------------------------
+// Water (water_normal src/material.c:1171-1217, water_attenuate :1238-1267)
+// ------------------------------------------------------------------
+template <typename R> MT_D V3<R> water_normal(R x, R z, R time)
+{
+    // WATER_WAVES (src/material.c:1159-1166): ax, az, w = 2 pi / lambda, amp, speed, phase
+    const R tp = R(2) * Const<R>::pi;
+    const R ax[4] = {R(0.9584), R(0.7071), R(-0.4061), R(0.2005)};
+    const R az[4] = {R(0.2855), R(-0.7071), R(0.9138), R(0.9797)};
+    const R w[4] = {tp / R(24), tp / R(13), tp / R(7), tp / R(4)};
+    const R amp[4] = {R(0.18), R(0.1), R(0.05), R(0.025)};
+    const R speed[4] = {R(1.0), R(1.4), R(2.0), R(2.6)};
+    const R phase[4] = {R(0.0), R(1.7), R(3.1), R(0.6)};
+    R dhdx = R(0), dhdz = R(0);
+    for (int i = 0; i < 4; ++i) {
+        R u = (ax[i] * x + az[i] * z) * w[i] + phase[i] + time * speed[i] * w[i];
+        R c = mcos(u) * amp[i] * w[i];
+        dhdx += c * ax[i];
+        dhdz += c * az[i];
+    }
+    const R freq = R(0.35), namp = R(0.06), e = R(0.02);
+    const uint32_t seed = 1337u;
+    R hL = noise_fbm2((x - e) * freq, z * freq, 4, seed);
+    R hR = noise_fbm2((x + e) * freq, z * freq, 4, seed);
+    R hD = noise_fbm2(x * freq, (z - e) * freq, 4, seed);
+    R hU = noise_fbm2(x * freq, (z + e) * freq, 4, seed);
+    dhdx += namp * (hR - hL) / (R(2) * e);
+    dhdz += namp * (hU - hD) / (R(2) * e);
+    V3<R> n = normalize(v3(-dhdx, R(1), -dhdz));
+    if (length_sq(n) < R(1e-12)) return v3(R(0), R(1), R(0));
+    if (n.y < R(0)) n = neg(n);
+    return n;
+}
+
+template <typename R> MT_D R water_transmittance(R absorption, R depth)
+{
+    if (absorption == R(0)) return R(1);
+    R t = mexp(-absorption * depth);
+    if (!(t > R(0))) return R(0);
+    if (t > R(1)) return R(1);
+    return t;
+}
+
+template <typename R> MT_D V3<R> water_attenuate(const DevMaterial<R> &m, V3<R> inner, R depth)
+{
+    R d = depth > R(0) ? depth : R(0);
+    V3<R> tr = v3(water_transmittance(m.absorption[0], d), water_transmittance(m.absorption[1], d),
+                  water_transmittance(m.absorption[2], d));
+    V3<R> out = v3(inner.x * tr.x + m.deep_color[0] * (R(1) - tr.x),
+                   inner.y * tr.y + m.deep_color[1] * (R(1) - tr.y),
+                   inner.z * tr.z + m.deep_color[2] * (R(1) - tr.z));
+    if (!(out.x >= R(0))) out.x = R(0);
+    if (!(out.y >= R(0))) out.y = R(0);
+    if (!(out.z >= R(0))) out.z = R(0);
+    return out;
+}
+
+// scene_water_height (src/scene.c:1109-1153)
+template <typename R> MT_D R water_height(const DevScene<R> &S, R x, R z)
+{
+    if (!S.ocean.enabled) return S.water_level;
+    const DevOcean<R> &o = S.ocean;
+    R y = o.center[1];
+    R dir_x = o.direction[0], dir_z = o.direction[2];
+    R dlen = msqrt(dir_x * dir_x + dir_z * dir_z);
+    if (dlen > R(1e-12)) {
+        dir_x /= dlen;
+        dir_z /= dlen;
+    } else {
+        dir_x = R(1);
+        dir_z = R(0);
+    }
+    R wl = o.wavelength <= R(0) ? R(12) : o.wavelength;
+    R amp = o.amplitude;
+    R chop_wl = o.chop_wavelength > R(0) ? o.chop_wavelength : wl * R(0.25);
+    R chop_amp = o.chop > R(0) ? o.chop : amp * R(0.25);
+    R lambda[4] = {wl, wl * R(0.52), chop_wl, chop_wl * R(0.40)};
+    R A[4] = {amp, amp * R(0.38), chop_amp, chop_amp * R(0.32)};
+    R angle[4] = {R(0.0), R(0.628), R(-0.488), R(1.134)};
+    R phi[4] = {R(0.0), R(1.7) + R(o.seed % 100u) * R(0.03), R(3.1) + R((o.seed * 7u) % 100u) * R(0.03),
+                R(0.8) + R((o.seed * 13u) % 100u) * R(0.03)};
+    for (int h = 0; h < 4; ++h) {
+        R ca = mcos(angle[h]);
+        R sa = msin(angle[h]);
+        R dx_h = ca * dir_x - sa * dir_z;
+        R dz_h = sa * dir_x + ca * dir_z;
+        R k_h = (R(2) * Const<R>::pi) / lambda[h];
+        R theta = k_h * (dx_h * x + dz_h * z) + phi[h];
+        y += A[h] * mcos(theta);
+    }
+    return y;
+}
+
+// ------------------------------------------------------------------
+// Local shading
+// ------------------------------------------------------------------
+// material_shade_local: Blinn-Phong without 1/pi (src/material.c:157-188)
+template <typename R>
+MT_D V3<R> shade_local(const DevMaterial<R> &m, V3<R> N, V3<R> L, V3<R> V, V3<R> light)
+{
+    R ndl = dot(N, L);
+    if (ndl <= R(0)) return v3(R(0), R(0), R(0));
+    V3<R> diffuse = scale(mul(mat3(m.albedo), light), ndl);
+    V3<R> h = add(L, V);
+    V3<R> spec = v3(R(0), R(0), R(0));
+    if (length_sq(h) > R(1e-12)) {
+        V3<R> H = normalize(h);
+        R ndh = dot(N, H);
+        if (ndh > R(0)) {
+            R spec_term = pow_nonneg(ndh, m.shininess);
+            spec = scale(mul(mat3(m.specular), light), spec_term);
+        }
+    }
+    return add(diffuse, spec);
+}
+
+// material_roughness_to_alpha (src/material.c:227-232)
+template <typename R> MT_D R roughness_to_alpha(R roughness)
+{
+    R r = mat_clamp01(roughness);
+    R a = r * r;
+    return a < R(1e-4) ? R(1e-4) : a;
+}
+
+template <typename R> MT_D R d_ggx(R ndh, R a)
+{
+    R a2 = a * a;
+    R d = ndh * ndh * (a2 - R(1)) + R(1);
+    return a2 / (Const<R>::pi * d * d);
+}
+
+// g_smith_schlick (src/material.c:207-218, same as pt_g_smith_schlick :192-200
+// up to the NaN behaviour of the clamp)
+template <typename R> MT_D R g_smith_schlick(R ndl, R ndv, R roughness)
+{
+    R k = (roughness + R(1)) * (roughness + R(1)) / R(8);
+    if (k < R(0)) k = R(0);
+    else if (k > R(1)) k = R(1);
+    R gl = ndl / (ndl * (R(1) - k) + k);
+    R gv = ndv / (ndv * (R(1) - k) + k);
+    return gl * gv;
+}
+
+// fresnel_schlick_rgb (src/material.c:142-151): clamps the cosine only
+template <typename R> MT_D V3<R> fresnel_schlick_rgb(R cos_theta, V3<R> f0)
+{
+    R c = mat_clamp01(cos_theta);
+    R mm = R(1) - c;
+    R m2 = mm * mm;
+    R k = m2 * m2 * mm;
+    return v3(f0.x + (R(1) - f0.x) * k, f0.y + (R(1) - f0.y) * k, f0.z + (R(1) - f0.z) * k);
+}
+
+// material_shade_pbr: Cook-Torrance GGX + Smith-Schlick + Schlick F at NdotV,
+// kD-weighted Lambert (src/material.c:234-290)
+template <typename R>
+MT_D V3<R> shade_pbr(const DevMaterial<R> &m, V3<R> N, V3<R> L, V3<R> V, V3<R> light)
+{
+    R ndl = dot(N, L);
+    if (ndl <= R(0)) return v3(R(0), R(0), R(0));
+    R ndv = dot(N, V);
+    if (ndv <= R(0)) return v3(R(0), R(0), R(0));
+    R metallic = mat_clamp01(m.metallic);
+    R alpha = roughness_to_alpha(m.roughness);
+    V3<R> h = add(L, V);
+    R ndh = R(0);
+    if (length_sq(h) > R(1e-12)) {
+        ndh = dot(N, normalize(h));
+        if (ndh < R(0)) ndh = R(0);
+    }
+    V3<R> albedo = mat3(m.albedo);
+    V3<R> f0 = lerp(v3(R(0.04), R(0.04), R(0.04)), albedo, metallic);
+    V3<R> F = fresnel_schlick_rgb(ndv, f0);
+    R D = d_ggx(ndh, alpha);
+    R G = g_smith_schlick(ndl, ndv, mat_clamp01(m.roughness));
+    R denom = R(4) * ndl * ndv;
+    R spec_scale = (denom > R(0)) ? (D * G / denom) : R(0);
+    V3<R> spec = scale(F, spec_scale);
+    V3<R> kd = scale(sub(v3(R(1), R(1), R(1)), F), (R(1) - metallic));
+    V3<R> f_diff = scale(mul(kd, albedo), R(1) / Const<R>::pi);
+    V3<R> f = add(f_diff, spec);
+    return scale(mul(light, f), ndl);
+}
+
+template <typename R>
+MT_D V3<R> shade(const DevMaterial<R> &m, V3<R> N, V3<R> L, V3<R> V, V3<R> light)
+{
+    return m.pbr ? shade_pbr(m, N, L, V, light) : shade_local(m, N, L, V, light);
+}
+
+// fresnel_schlick (scalar, src/material.c:134-140)
+template <typename R> MT_D R fresnel_schlick(R cos_theta, R f0)
+{
+    R c = mat_clamp01(cos_theta);
+    R mm = R(1) - c;
+    R m2 = mm * mm;
+    return f0 + (R(1) - f0) * (m2 * m2 * mm);
+}
+
+// material_ambient (src/material.c:351-374)
+template <typename R> MT_D V3<R> material_ambient(const DevMaterial<R> &m, V3<R> N, const DevSky<R> &sky)
+{
+    V3<R> groundish = scale(mat3(sky.horizon_color), R(0.45));
+    V3<R> skyish = mat3(sky.zenith_color);
+    R w = mat_clamp01(R(0.5) + R(0.5) * N.y);
+    V3<R> hemi = lerp(groundish, skyish, w);
+    return scale(mul(mat3(m.albedo), hemi), R(0.15));
+}
+
+// material_sample_glossy_dir (src/material.c:303-349)
+template <typename R>
+MT_D V3<R> sample_glossy_dir(const DevMaterial<R> &m, V3<R> N, V3<R> incident, R r1, R r2)
+{
+    const R rmax = sizeof(R) == 8 ? R(0.9999999999999999) : R(0.99999994f);
+    V3<R> mirror = reflect(incident, N);
+    if (m.roughness <= R(1e-6)) return mirror;
+    R alpha = roughness_to_alpha(m.roughness);
+    R a2 = alpha * alpha;
+    if (!(r1 > R(0))) r1 = R(0);
+    else if (r1 > rmax) r1 = rmax;
+    if (!(r2 > R(0))) r2 = R(0);
+    else if (r2 > rmax) r2 = rmax;
+    R cos_theta = msqrt((R(1) - r1) / (R(1) + (a2 - R(1)) * r1));
+    R sin_theta = msqrt(R(1) - cos_theta * cos_theta);
+    R phi = R(2) * Const<R>::pi * r2;
+    V3<R> t, b;
+    basis(N, &t, &b);
+    R sp, cp;
+    msincos(phi, &sp, &cp);
+    V3<R> H = add(add(scale(t, sin_theta * cp), scale(b, sin_theta * sp)), scale(N, cos_theta));
+    H = normalize(H);
+    V3<R> Rr = reflect(incident, H);
+    if (!(dot(Rr, N) > R(0))) return mirror;
+    return normalize(Rr);
+}
+
+// ------------------------------------------------------------------
+// Monte-Carlo sampling (src/sampling.c:40-281)
+// ------------------------------------------------------------------
+template <typename R> MT_D R clamp_uniform(R u)
+{
+    const R rmax = sizeof(R) == 8 ? R(0.9999999999999999) : R(0.99999994f);
+    if (!(u > R(0))) return R(0);
+    if (u > rmax) return rmax;
+    return u;
+}
+
+// sampling_basis with its defensive normalisation (src/sampling.c:52-77)
+template <typename R> MT_D void sampling_basis(V3<R> n, V3<R> *t, V3<R> *b)
+{
+    V3<R> nn = normalize(n);
+    if (length_sq(nn) <= R(0)) nn = v3(R(0), R(1), R(0));
+    basis(nn, t, b);
+}
+
+// sampling_cosine_hemisphere (src/sampling.c:83-107)
+template <typename R> MT_D V3<R> cosine_hemisphere(V3<R> n, R u1, R u2)
+{
+    V3<R> nn = normalize(n);
+    if (length_sq(nn) <= R(0)) nn = v3(R(0), R(1), R(0));
+    R r1 = clamp_uniform(u1);
+    R r2 = clamp_uniform(u2);
+    R r = msqrt(r1);
+    R phi = R(2) * Const<R>::pi * r2;
+    R sp, cp;
+    msincos(phi, &sp, &cp);
+    R x = r * cp;
+    R y = r * sp;
+    R z = msqrt(mfmax(R(0), R(1) - r1));
+    V3<R> t, b;
+    sampling_basis(nn, &t, &b);
+    V3<R> d = add(add(scale(t, x), scale(b, y)), scale(nn, z));
+    return normalize(d);
+}
+
+// sampling_fresnel_schlick_rgb: clamps cosine AND f0 (src/sampling.c:134-149)
+template <typename R> MT_D R sampling_fresnel_schlick(R cos_theta, R f0)
+{
+    R c = mat_clamp01(cos_theta);
+    R f = mat_clamp01(f0);
+    R mm = R(1) - c;
+    R m2 = mm * mm;
+    R k = m2 * m2 * mm;
+    return f + (R(1) - f) * k;
+}
+template <typename R> MT_D V3<R> sampling_fresnel_schlick_rgb(R cos_theta, V3<R> f0)
+{
+    return v3(sampling_fresnel_schlick(cos_theta, f0.x), sampling_fresnel_schlick(cos_theta, f0.y),
+              sampling_fresnel_schlick(cos_theta, f0.z));
+}
+
+// sampling_fresnel_dielectric: exact unpolarised Fresnel (src/sampling.c:162-181)
+template <typename R> MT_D R fresnel_dielectric(R cos_i, R eta)
+{
+    R c = mat_clamp01(cos_i);
+    R e = eta > R(0) ? eta : R(0);
+    R sin2_t = e * e * (R(1) - c * c);
+    if (sin2_t >= R(1)) return R(1);
+    R cos_t = msqrt(R(1) - sin2_t);
+    R rs = (e * c - cos_t) / (e * c + cos_t);
+    R rp = (e * cos_t - c) / (e * cos_t + c);
+    R f = R(0.5) * (rs * rs + rp * rp);
+    return mat_clamp01(f);
+}
+
+// sampling_refract (src/sampling.c:183-211)
+template <typename R> MT_D bool sampling_refract(V3<R> incident, V3<R> n, R eta, V3<R> *out)
+{
+    V3<R> i = normalize(incident);
+    V3<R> nn = normalize(n);
+    if (length_sq(i) <= R(0) || length_sq(nn) <= R(0)) return false;
+    R e = eta > R(0) ? eta : R(0);
+    R cos_i = -dot(i, nn);
+    R sin2_t = e * e * (R(1) - cos_i * cos_i);
+    if (sin2_t >= R(1)) return false;
+    R cos_t = msqrt(R(1) - sin2_t);
+    R k = e * cos_i - cos_t;
+    V3<R> t = v3(e * i.x + k * nn.x, e * i.y + k * nn.y, e * i.z + k * nn.z);
+    *out = normalize(t);
+    return true;
+}
+
+// vec3_refract (src/vec3.c:54-66), used by the Whitted renderer
+template <typename R> MT_D V3<R> vec3_refract(V3<R> i, V3<R> n, R eta)
+{
+    R cos_i = -dot(i, n);
+    R sin2_t = eta * eta * (R(1) - cos_i * cos_i);
+    if (sin2_t > R(1)) return v3(R(0), R(0), R(0));
+    R cos_t = msqrt(R(1) - sin2_t);
+    R k = eta * cos_i - cos_t;
+    return v3(eta * i.x + k * n.x, eta * i.y + k * n.y, eta * i.z + k * n.z);
+}
+
+// sampling_specular_probability (src/sampling.c:217-231)
+template <typename R> MT_D R specular_probability(R metallic, R roughness, R f0_scalar)
+{
+    R m = mat_clamp01(metallic);
+    R r = mat_clamp01(roughness);
+    R f0 = mat_clamp01(f0_scalar);
+    R p = f0 + (R(1) - f0) * m;
+    p *= R(1) - R(0.5) * r * (R(1) - m);
+    return pt_clamp(p, R(1e-3), R(1));
+}
+
+// sampling_ggx_half_vector (src/sampling.c:242-268)
+template <typename R> MT_D V3<R> ggx_half_vector(V3<R> n, R alpha, R u1, R u2)
+{
+    V3<R> nn = normalize(n);
+    if (length_sq(nn) <= R(0)) nn = v3(R(0), R(1), R(0));
+    R a = alpha > R(1e-4) ? alpha : R(1e-4);
+    R a2 = a * a;
+    R r1 = clamp_uniform(u1);
+    R r2 = clamp_uniform(u2);
+    R cos_theta = msqrt((R(1) - r1) / (R(1) + (a2 - R(1)) * r1));
+    R sin_theta = msqrt(mfmax(R(0), R(1) - cos_theta * cos_theta));
+    R phi = R(2) * Const<R>::pi * r2;
+    V3<R> t, b;
+    sampling_basis(nn, &t, &b);
+    R sp, cp;
+    msincos(phi, &sp, &cp);
+    V3<R> h = add(add(scale(t, sin_theta * cp), scale(b, sin_theta * sp)), scale(nn, cos_theta));
+    return normalize(h);
+}
+
+// sampling_ggx_pdf (src/sampling.c:270-281)
+template <typename R> MT_D R ggx_pdf(R n_dot_h, R h_dot_v, R alpha)
+{
+    if (!(h_dot_v > R(0)) || !(n_dot_h > R(0))) return R(0);
+    R a = alpha > R(1e-4) ? alpha : R(1e-4);
+    R ndh = n_dot_h > R(1) ? R(1) : n_dot_h;
+    R D = d_ggx(ndh, a);
+    return D * ndh / (R(4) * h_dot_v);
+}
+
+}  // namespace mt

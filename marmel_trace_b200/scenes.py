@@ -1,0 +1,241 @@
+"""Seeded synthetic scenes with the shapes of the benchmark configurations,
+plus a writer for the reference's scene text format.
+
+There is no public dataset for this renderer: every workload is generated
+here from a fixed seed. Each generator returns a `SceneDesc` whose primitive
+order is the reference's prim_index order; `to_scene_text` writes the same
+scene in the reference's format (docs/scene_format.md) with every float in
+shortest round-trip form, so the reference's parser rebuilds bit-identical
+doubles.
+
+    spheres_scene (config "C1"): 320x240, 8 spp, depth 5; ground plane + 64
+        spheres (seed 1): 50% Lambert, 25% PBR metal, 25% glass.
+    torus_field_scene (config "C2"): 1920x1080, 64 spp, depth 8; 4096
+        instances of a 256-triangle torus (1,048,576 triangles, seed 2), PBR
+        GGX materials, 8 emissive sphere lights, ground plane, sun and sky.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from ._capi import MATERIAL_DTYPE, PRIM_DTYPE, PRIM_BOX, PRIM_CYLINDER, PRIM_PLANE, PRIM_SPHERE, PRIM_TRIANGLE
+from .api import SceneDesc, default_sky, normalize
+
+
+def material(albedo=(0.0, 0.0, 0.0), specular=(0.0, 0.0, 0.0), shininess=0.0, reflectivity=0.0, transparency=0.0,
+             ior=1.0, absorption=(0.0, 0.0, 0.0), deep_color=(0.0, 0.0, 0.0), metallic=0.0, roughness=0.0,
+             emissive=(0.0, 0.0, 0.0), pbr=0, is_water=0, beer_lambert=0) -> np.ndarray:
+    m = np.zeros(1, MATERIAL_DTYPE)
+    m["albedo"] = albedo
+    m["specular"] = specular
+    m["shininess"] = shininess
+    m["reflectivity"] = reflectivity
+    m["transparency"] = transparency
+    m["ior"] = ior
+    m["absorption"] = absorption
+    m["deep_color"] = deep_color
+    m["metallic"] = metallic
+    m["roughness"] = roughness
+    m["emissive"] = emissive
+    m["pbr"] = pbr
+    m["is_water"] = is_water
+    m["beer_lambert"] = beer_lambert
+    return m[0]
+
+
+def glass_material() -> np.ndarray:
+    """`type = glass` preset (sd_glass_preset in the reference's parser)."""
+    return material(albedo=(0.02, 0.02, 0.02), specular=(1.0, 1.0, 1.0), shininess=256.0, transparency=1.0, ior=1.5)
+
+
+def water_material() -> np.ndarray:
+    """`type = water` preset (sd_water_preset in the reference's parser)."""
+    return material(albedo=(0.05, 0.15, 0.20), specular=(0.9, 0.9, 0.9), shininess=256.0, reflectivity=1.0,
+                    transparency=0.85, ior=1.33, is_water=1, absorption=(0.45, 0.12, 0.06),
+                    deep_color=(0.02, 0.10, 0.16))
+
+
+def light_material(color, intensity) -> np.ndarray:
+    """Material the reference builds for a `light` block (src/scene.c:1517-1524)."""
+    c = tuple(float(x) for x in color)
+    return material(albedo=c, emissive=tuple(x * float(intensity) for x in c), roughness=1.0, pbr=1)
+
+
+def prims_array(n: int) -> np.ndarray:
+    return np.zeros(n, PRIM_DTYPE)
+
+
+def set_sphere(p, center, radius, mat):
+    p["kind"] = PRIM_SPHERE
+    p["material"] = mat
+    p["v"][:3] = center
+    p["v"][3] = radius
+
+
+def set_plane(p, point, normal, mat):
+    p["kind"] = PRIM_PLANE
+    p["material"] = mat
+    p["v"][:3] = point
+    p["v"][3:6] = normalize(normal)  # prim_plane normalises the normal once
+
+
+# ---------------------------------------------------------------------
+# C1: ground plane + 64 spheres
+# ---------------------------------------------------------------------
+def spheres_scene(seed: int = 1, n_spheres: int = 64, metal_reflectivity: float = 0.5) -> SceneDesc:
+    rng = np.random.default_rng(seed)
+    mats = [material(albedo=(0.5, 0.5, 0.5))]  # ground: Lambert grey
+    kinds = np.array([0] * (n_spheres // 2) + [1] * (n_spheres // 4) + [2] * (n_spheres - n_spheres // 2 - n_spheres // 4))
+    rng.shuffle(kinds)
+    centers = np.stack([rng.uniform(-10, 10, n_spheres), rng.uniform(0.2, 3.0, n_spheres),
+                        rng.uniform(-10, 10, n_spheres)], axis=1)
+    radii = rng.uniform(0.2, 1.0, n_spheres)
+    prims = prims_array(1 + n_spheres)
+    set_plane(prims[0], (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 0)
+    for i in range(n_spheres):
+        if kinds[i] == 0:
+            mats.append(material(albedo=tuple(rng.uniform(0.1, 0.9, 3))))
+        elif kinds[i] == 1:
+            mats.append(material(albedo=tuple(rng.uniform(0.5, 0.95, 3)), metallic=1.0,
+                                 roughness=float(rng.uniform(0.05, 0.6)), pbr=1, reflectivity=metal_reflectivity))
+        else:
+            mats.append(glass_material())
+        set_sphere(prims[1 + i], centers[i], radii[i], 1 + i)
+    sky = default_sky(sun_dir=normalize((0.3, 0.8, 0.5)))
+    return SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=sky,
+                     camera=dict(eye=(0.0, 2.0, -10.0), target=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), vfov=45.0))
+
+
+# ---------------------------------------------------------------------
+# C2: 4096 tori (1,048,576 triangles), PBR, 8 emissive sphere lights
+# ---------------------------------------------------------------------
+def torus_mesh(n_major: int = 16, n_minor: int = 8, R: float = 1.0, r: float = 0.35) -> np.ndarray:
+    """Triangles (n_major * n_minor * 2, 3, 3) of a torus around +Y."""
+    u = np.arange(n_major) * (2 * math.pi / n_major)
+    v = np.arange(n_minor) * (2 * math.pi / n_minor)
+    uu, vv = np.meshgrid(u, v, indexing="ij")
+    verts = np.stack([(R + r * np.cos(vv)) * np.cos(uu), r * np.sin(vv), (R + r * np.cos(vv)) * np.sin(uu)], axis=-1)
+    tris = []
+    for i in range(n_major):
+        for j in range(n_minor):
+            a = verts[i, j]
+            b = verts[(i + 1) % n_major, j]
+            c = verts[(i + 1) % n_major, (j + 1) % n_minor]
+            d = verts[i, (j + 1) % n_minor]
+            tris.append((a, b, c))
+            tris.append((a, c, d))
+    return np.array(tris, np.float64)
+
+
+def random_rotations(rng, n: int) -> np.ndarray:
+    """Uniform random rotation matrices (from unit quaternions)."""
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], axis=1)
+
+
+def torus_field_scene(seed: int = 2, n_instances: int = 4096, n_materials: int = 32, n_lights: int = 8,
+                      area: float = 100.0) -> SceneDesc:
+    rng = np.random.default_rng(seed)
+    mesh = torus_mesh()
+    ntri = len(mesh)
+    scale = rng.uniform(0.5, 3.0, n_instances)
+    rot = random_rotations(rng, n_instances)
+    pos = np.stack([rng.uniform(-area / 2, area / 2, n_instances), scale * 0.35 + rng.uniform(0.0, 1.0, n_instances),
+                    rng.uniform(-area / 2, area / 2, n_instances)], axis=1)
+    mat_of = rng.integers(0, n_materials, n_instances)
+    # (inst, tri, vert, xyz) = R @ (s * v) + p
+    tv = np.einsum("nij,tkj->ntki", rot, mesh) * scale[:, None, None, None] + pos[:, None, None, :]
+
+    mats = [material(albedo=(0.45, 0.45, 0.42), roughness=0.8, pbr=1)]  # ground: rough PBR dielectric
+    for _ in range(n_materials):
+        metal = float(rng.uniform() < 0.3)
+        mats.append(material(albedo=tuple(rng.uniform(0.2, 0.9, 3)), metallic=metal,
+                             roughness=float(rng.uniform(0.02, 0.9)), pbr=1))
+    light_pos = np.stack([rng.uniform(-40, 40, n_lights), rng.uniform(2.0, 6.0, n_lights),
+                          rng.uniform(-40, 40, n_lights)], axis=1)
+    light_int = rng.uniform(5.0, 20.0, n_lights)
+    first_light_mat = len(mats)
+    for k in range(n_lights):
+        mats.append(light_material((1.0, 1.0, 1.0), light_int[k]))
+
+    n = 1 + n_instances * ntri + n_lights
+    prims = prims_array(n)
+    set_plane(prims[0], (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 0)
+    tri = prims[1:1 + n_instances * ntri]
+    tri["kind"] = PRIM_TRIANGLE
+    tri["material"] = np.repeat(1 + mat_of, ntri)
+    tri["v"] = tv.reshape(-1, 9)
+    for k in range(n_lights):
+        set_sphere(prims[1 + n_instances * ntri + k], light_pos[k], 0.5, first_light_mat + k)
+    return SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=default_sky(),
+                     camera=dict(eye=(0.0, 14.0, -62.0), target=(0.0, 0.0, -5.0), up=(0.0, 1.0, 0.0), vfov=50.0))
+
+
+# ---------------------------------------------------------------------
+# Reference scene text
+# ---------------------------------------------------------------------
+def _f(x) -> str:
+    return repr(float(x))
+
+
+def _v(v) -> str:
+    return " ".join(_f(c) for c in v)
+
+
+def to_scene_text(desc: SceneDesc) -> str:
+    """Write `desc` in the reference's scene format. Primitive and material
+    order are preserved, so the reference's prim_index order matches."""
+    lines = []
+    names = [f"m{i}" for i in range(len(desc.materials))]
+    if desc.water_material >= 0:
+        lines.append(f"water_level = {_f(desc.water_level)}")
+        lines.append(f"water_material = {names[desc.water_material]}")
+    if desc.camera:
+        c = desc.camera
+        lines += ["camera {", f"    eye = {_v(c['eye'])}", f"    target = {_v(c['target'])}", f"    up = {_v(c['up'])}",
+                  f"    vfov = {_f(c['vfov'])}", "}"]
+    s = desc.sky
+    lines.append("sky {")
+    for k in ("sun_dir", "sun_color", "horizon_color", "zenith_color"):
+        lines.append(f"    {k} = {_v(s[k])}")
+    for k in ("gradient_gamma", "sun_glow_exponent", "sun_glow_strength", "cloud_height", "cloud_scale",
+              "cloud_coverage", "cloud_softness", "cloud_sharpness"):
+        lines.append(f"    {k} = {_f(s[k])}")
+    lines.append(f"    cloud_octaves = {int(s['cloud_octaves'])}")
+    lines.append(f"    seed = {int(s['seed'])}")
+    lines.append(f"    sun_radius = {_f(s['sun_radius'])}")
+    lines.append("}")
+    for i, m in enumerate(desc.materials):
+        lines.append(f"material {names[i]} {{")
+        for k in ("albedo", "specular", "absorption", "deep_color", "emissive"):
+            lines.append(f"    {k} = {_v(m[k])}")
+        for k in ("shininess", "reflectivity", "transparency", "ior", "metallic", "roughness"):
+            lines.append(f"    {k} = {_f(m[k])}")
+        for k in ("is_water", "beer_lambert", "pbr"):
+            lines.append(f"    {k} = {int(m[k])}")
+        lines.append("}")
+    for p in desc.prims:
+        mat = names[p["material"]]
+        v = p["v"]
+        k = int(p["kind"])
+        if k == PRIM_SPHERE:
+            lines += ["sphere {", f"    center = {_v(v[:3])}", f"    radius = {_f(v[3])}", f"    material = {mat}", "}"]
+        elif k == PRIM_PLANE:
+            lines += ["plane {", f"    point = {_v(v[:3])}", f"    normal = {_v(v[3:6])}", f"    material = {mat}", "}"]
+        elif k == PRIM_BOX:
+            lines += ["box {", f"    center = {_v(v[:3])}", f"    half = {_v(v[3:6])}", f"    material = {mat}", "}"]
+        elif k == PRIM_TRIANGLE:
+            lines += ["triangle {", f"    a = {_v(v[:3])}", f"    b = {_v(v[3:6])}", f"    c = {_v(v[6:9])}",
+                      f"    material = {mat}", "}"]
+        elif k == PRIM_CYLINDER:
+            lines += ["cylinder {", f"    base = {_v(v[:3])}", f"    top = {_v(v[3:6])}", f"    r_bottom = {_f(v[6])}",
+                      f"    r_top = {_f(v[7])}", f"    material = {mat}", "}"]
+    return "\n".join(lines) + "\n"

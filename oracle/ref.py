@@ -1,0 +1,270 @@
+"""ctypes access to the oracle: the reference renderer compiled from its own
+sources into oracle/_ref/libmtref.so by oracle/Makefile.
+
+TEST INFRASTRUCTURE ONLY. Imported by tests/, by __graft_entry__.smoke() as
+the checker, and by the CPU-baseline leg of bench.py. The GPU product path
+never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_ref" / "libmtref.so"
+CLI = HERE / "_ref" / "raytracer"
+REF_DIR = Path(os.environ.get("MT_REF_DIR", "/root/reference"))
+
+P, I, D, U = C.c_void_p, C.c_int, C.c_double, C.c_uint
+
+_SIG = {
+    "mtref_load_text": (P, [C.c_char_p, I, I, C.c_char_p, I]),
+    "mtref_load_file": (P, [C.c_char_p, I, I, C.c_char_p, I]),
+    "mtref_from_desc": (P, [P, P]),
+    "mtref_free": (None, [P]),
+    "mtref_prim_count": (I, [P]),
+    "mtref_material_count": (I, [P]),
+    "mtref_lights": (I, [P, P]),
+    "mtref_export": (I, [P, P, P, P, P]),
+    "mtref_set_camera": (None, [P, P]),
+    "mtref_camera_create": (None, [P, P, P, D, D, P]),
+    "mtref_intersect": (I, [P, I, P, P, D, D, P, P, P, P, P]),
+    "mtref_intersect_linear": (I, [P, I, P, P, D, D, P, P]),
+    "mtref_occluded": (I, [P, I, P, P, D, D, P]),
+    "mtref_water_height": (D, [P, D, D]),
+    "mtref_pt_hash3": (U, [U, U, U]),
+    "mtref_pt_rand01": (D, [U, U, U]),
+    "mtref_pt_to_byte": (C.c_ubyte, [D]),
+    "mtref_pathtrace_render": (I, [P, I, I, I, I, P]),
+    "mtref_pt_primary_rays": (I, [P, I, I, I, P]),
+    "mtref_pathtrace_radiance": (I, [P, I, P, P, I, P, P]),
+    "mtref_pathtrace_linear": (I, [P, I, I, I, I, I, P, I]),
+    "mtref_render_hash3": (U, [U, U, U]),
+    "mtref_to_byte": (C.c_ubyte, [D]),
+    "mtref_render_image": (I, [P, I, I, I, I, P]),
+    "mtref_render_image_ex": (I, [P, I, I, I, I, I, I, D, P]),
+    "mtref_render_last_seconds": (D, []),
+    "mtref_wh_primary_rays": (I, [P, I, I, I, P]),
+    "mtref_whitted_trace": (I, [P, I, P, P, I, P, P]),
+    "mtref_whitted_linear": (I, [P, I, I, I, I, P, I]),
+    "mtref_bvh_export": (I, [P, P, P, P, P, P, P, P, P]),
+    "mtref_bvh_count": (I, [P, I, P, P, D, D, P, P, P]),
+}
+
+_lib = None
+
+
+def available() -> bool:
+    return LIB.exists() or (REF_DIR / "src").is_dir()
+
+
+def build() -> None:
+    """Compile the oracle (needs the reference sources; never run on the GPU box)."""
+    if not (REF_DIR / "src").is_dir():
+        raise RuntimeError(f"reference sources not found at {REF_DIR}")
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF_DIR={REF_DIR}", "cpu", "-j8"], check=True)
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB.exists():
+        build()
+    lib = C.CDLL(str(LIB))
+    for name, (res, args) in _SIG.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class RefScene:
+    """A reference `Scene` + `Camera` held by the oracle library."""
+
+    def __init__(self, handle):
+        if not handle:
+            raise RuntimeError("oracle scene construction failed")
+        self.lib = load()
+        self.h = C.c_void_p(handle)
+
+    @classmethod
+    def from_text(cls, text: str | None, width: int, height: int) -> "RefScene":
+        lib = load()
+        err = C.create_string_buffer(512)
+        h = lib.mtref_load_text(text.encode() if text is not None else None, width, height, err, 512)
+        if not h:
+            raise RuntimeError(f"reference parser: {err.value.decode()}")
+        return cls(h)
+
+    @classmethod
+    def from_file(cls, path: str, width: int, height: int) -> "RefScene":
+        lib = load()
+        err = C.create_string_buffer(512)
+        h = lib.mtref_load_file(str(path).encode(), width, height, err, 512)
+        if not h:
+            raise RuntimeError(f"reference parser: {err.value.decode()}")
+        return cls(h)
+
+    @classmethod
+    def from_desc(cls, desc, camera=None) -> "RefScene":
+        lib = load()
+        cd = desc.c_desc()
+        h = lib.mtref_from_desc(C.byref(cd), C.byref(camera.c) if camera is not None else None)
+        return cls(h)
+
+    def free(self):
+        if self.h and self.h.value:
+            self.lib.mtref_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def set_camera(self, cam):
+        self.lib.mtref_set_camera(self.h, C.byref(cam.c))
+
+    def export(self):
+        """Scene -> (SceneDesc, Camera) through the reference-side binding."""
+        from marmel_trace_b200 import _capi as capi
+        from marmel_trace_b200.api import Camera, SceneDesc
+
+        n = self.lib.mtref_prim_count(self.h)
+        m = self.lib.mtref_material_count(self.h)
+        prims = np.zeros(n, capi.PRIM_DTYPE)
+        mats = np.zeros(m, capi.MATERIAL_DTYPE)
+        d = capi.MtSceneDesc()
+        cam = capi.MtCamera()
+        rc = self.lib.mtref_export(self.h, _p(prims), _p(mats), C.byref(d), C.byref(cam))
+        if rc != 0:
+            raise RuntimeError(f"binding export failed with code {rc}")
+        s = d.sky
+        sky = dict(
+            sun_dir=tuple(s.sun_dir), sun_color=tuple(s.sun_color), horizon_color=tuple(s.horizon_color),
+            zenith_color=tuple(s.zenith_color), gradient_gamma=s.gradient_gamma,
+            sun_glow_exponent=s.sun_glow_exponent, sun_glow_strength=s.sun_glow_strength,
+            cloud_height=s.cloud_height, cloud_scale=s.cloud_scale, cloud_coverage=s.cloud_coverage,
+            cloud_softness=s.cloud_softness, cloud_sharpness=s.cloud_sharpness, cloud_octaves=s.cloud_octaves,
+            cloud_thickness=s.cloud_thickness, seed=s.seed, sun_radius=s.sun_radius,
+        )
+        desc = SceneDesc(prims=prims, materials=mats, sky=sky, water_level=d.water_level,
+                         water_material=d.water_material, fog_density=d.fog_density)
+        return desc, Camera(cam)
+
+    def lights(self):
+        buf = np.zeros(8, np.int32)
+        n = self.lib.mtref_lights(self.h, _p(buf))
+        return buf[:n].copy()
+
+    # -- queries ------------------------------------------------------
+    def intersect(self, o, d, tmin=1e-4, tmax=1e30):
+        o = np.ascontiguousarray(o, np.float64)
+        d = np.ascontiguousarray(d, np.float64)
+        n = len(o)
+        prim = np.zeros(n, np.int32)
+        t = np.zeros(n)
+        nrm = np.zeros((n, 3))
+        front = np.zeros(n, np.int32)
+        mat = np.zeros(n, np.int32)
+        self.lib.mtref_intersect(self.h, n, _p(o), _p(d), tmin, tmax, _p(prim), _p(t), _p(nrm), _p(front), _p(mat))
+        return prim, t, nrm, front, mat
+
+    def intersect_linear(self, o, d, tmin=1e-4, tmax=1e30):
+        o = np.ascontiguousarray(o, np.float64)
+        d = np.ascontiguousarray(d, np.float64)
+        prim = np.zeros(len(o), np.int32)
+        t = np.zeros(len(o))
+        self.lib.mtref_intersect_linear(self.h, len(o), _p(o), _p(d), tmin, tmax, _p(prim), _p(t))
+        return prim, t
+
+    def occluded(self, o, d, tmin, tmax):
+        o = np.ascontiguousarray(o, np.float64)
+        d = np.ascontiguousarray(d, np.float64)
+        occ = np.zeros(len(o), np.int32)
+        self.lib.mtref_occluded(self.h, len(o), _p(o), _p(d), tmin, tmax, _p(occ))
+        return occ
+
+    # -- renderers ----------------------------------------------------
+    def pathtrace_render(self, w, h, spp, depth):
+        out = np.zeros((h, w, 3), np.uint8)
+        rc = self.lib.mtref_pathtrace_render(self.h, w, h, spp, depth, _p(out))
+        if rc != 0:
+            raise RuntimeError(f"pathtrace_render returned {rc}")
+        return out
+
+    def pathtrace_linear(self, w, h, spp, depth, s0=0, threads=None):
+        """Per-pixel mean linear radiance over samples [s0, s0+spp)."""
+        out = np.zeros((h, w, 3), np.float64)
+        nt = threads or os.cpu_count() or 1
+        self.lib.mtref_pathtrace_linear(self.h, w, h, s0, spp, depth, _p(out), nt)
+        return out / spp
+
+    def whitted_render(self, w, h, spp, depth):
+        out = np.zeros((h, w, 3), np.uint8)
+        rc = self.lib.mtref_render_image(self.h, w, h, spp, depth, _p(out))
+        if rc != 0:
+            raise RuntimeError(f"render_image returned {rc}")
+        return out
+
+    def whitted_linear(self, w, h, spp, depth, threads=None):
+        out = np.zeros((h, w, 3), np.float64)
+        nt = threads or os.cpu_count() or 1
+        self.lib.mtref_whitted_linear(self.h, w, h, spp, depth, _p(out), nt)
+        return out
+
+    def primary_rays(self, w, h, spp, mode="pathtrace"):
+        out = np.zeros((h * w * spp, 6), np.float64)
+        fn = self.lib.mtref_pt_primary_rays if mode == "pathtrace" else self.lib.mtref_wh_primary_rays
+        fn(self.h, w, h, spp, _p(out))
+        return out
+
+    def radiance(self, o, d, depth, seeds, mode="pathtrace"):
+        o = np.ascontiguousarray(o, np.float64)
+        d = np.ascontiguousarray(d, np.float64)
+        s = np.ascontiguousarray(seeds, np.uint32)
+        out = np.zeros((len(s), 3))
+        fn = self.lib.mtref_pathtrace_radiance if mode == "pathtrace" else self.lib.mtref_whitted_trace
+        fn(self.h, len(s), _p(o), _p(d), depth, _p(s), _p(out))
+        return out
+
+    def bvh_export(self):
+        n, m, pc, dep = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self.lib.mtref_bvh_export(self.h, None, None, None, C.byref(n), C.byref(m), None, C.byref(pc), C.byref(dep))
+        b = np.zeros((n.value, 6))
+        l = np.zeros((n.value, 4), np.int32)
+        o = np.zeros(m.value, np.int32)
+        pl = np.zeros(max(pc.value, 1), np.int32)
+        self.lib.mtref_bvh_export(self.h, _p(b), _p(l), _p(o), C.byref(n), C.byref(m), _p(pl), C.byref(pc),
+                                  C.byref(dep))
+        return b, l, o, pl[: pc.value], dep.value
+
+    def bvh_count(self, o, d, tmin=1e-4, tmax=1e30):
+        o = np.ascontiguousarray(o, np.float64)
+        d = np.ascontiguousarray(d, np.float64)
+        np_, pt, lv = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self.lib.mtref_bvh_count(self.h, len(o), _p(o), _p(d), tmin, tmax, C.byref(np_), C.byref(pt), C.byref(lv))
+        return np_.value, pt.value, lv.value
+
+
+def pt_hash3(a, b, c) -> int:
+    return load().mtref_pt_hash3(a, b, c)
+
+
+def pt_rand01(a, b, c) -> float:
+    return load().mtref_pt_rand01(a, b, c)
+
+
+def to_byte(x) -> int:
+    return load().mtref_to_byte(x)
