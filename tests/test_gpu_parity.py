@@ -125,13 +125,24 @@ def test_radiance_fp64_exact(oracle, c1):
     w, h, spp = 64, 48, 1
     rs, cam = _ref_and_cam(oracle, c1, w, h)
     rays = rs.primary_rays(w, h, spp)
-    seeds = np.arange(len(rays), dtype=np.uint32) * 2654435761 % (2**32)
-    want = rs.radiance(rays[:, :3], rays[:, 3:], 5, seeds.astype(np.uint32))
+    seeds = ((np.arange(len(rays), dtype=np.uint64) * 2654435761) % (2**32)).astype(np.uint32)
+    want = rs.radiance(rays[:, :3], rays[:, 3:], 5, seeds)
     with mt.GpuScene(c1, precision="fp64") as g:
-        got = g.radiance(rays[:, :3], rays[:, 3:], 5, seeds.astype(np.uint32))
+        got = g.radiance(rays[:, :3], rays[:, 3:], 5, seeds)
     exact = np.all(got == want, axis=1)
     assert exact.mean() > 0.999, f"{(~exact).sum()} of {len(exact)} paths differ"
-    assert np.allclose(got, want, rtol=1e-9, atol=1e-12) or exact.mean() > 0.999
+
+
+def test_whitted_trace_fp64_exact(oracle, c1):
+    w, h, spp = 48, 36, 1
+    rs, cam = _ref_and_cam(oracle, c1, w, h)
+    rays = rs.primary_rays(w, h, spp, "whitted")
+    seeds = ((np.arange(len(rays), dtype=np.uint64) * 2246822519) % (2**32)).astype(np.uint32)
+    want = rs.radiance(rays[:, :3], rays[:, 3:], 5, seeds, mode="whitted")
+    with mt.GpuScene(c1, precision="fp64") as g:
+        got = g.radiance(rays[:, :3], rays[:, 3:], 5, seeds, mode="whitted")
+    exact = np.all(got == want, axis=1)
+    assert exact.mean() > 0.999, f"{(~exact).sum()} of {len(exact)} Whitted samples differ"
 
 
 def test_default_scene_whitted_matches_reference_bytes(oracle, mtlib):
