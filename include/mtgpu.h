@@ -299,7 +299,8 @@ typedef struct {
     int64_t extension_rays;   /* nearest-hit rays incl. primary                  */
     int64_t shadow_rays;      /* NEE / any-hit rays                              */
     int64_t node_visits;      /* inner nodes whose two child boxes were tested   */
-    int64_t prim_tests;       /* primitive intersection tests                    */
+    int64_t prim_tests;       /* primitive intersection tests (planes included)  */
+    int64_t tri_tests;        /* of which triangle tests                         */
     int32_t launches;         /* kernels launched                                */
     int32_t error_flags;      /* device error word (0 = clean)                   */
 } mt_stats;

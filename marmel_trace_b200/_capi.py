@@ -171,6 +171,7 @@ class MtStats(C.Structure):
         ("shadow_rays", C.c_int64),
         ("node_visits", C.c_int64),
         ("prim_tests", C.c_int64),
+        ("tri_tests", C.c_int64),
         ("launches", C.c_int32),
         ("error_flags", C.c_int32),
     ]

@@ -359,6 +359,7 @@ int read_counters(mt_scene *sc)
     sc->stats.shadow_rays = (int64_t)c.shadow_rays;
     sc->stats.node_visits = (int64_t)c.node_visits;
     sc->stats.prim_tests = (int64_t)c.prim_tests;
+    sc->stats.tri_tests = (int64_t)c.tri_tests;
     return 0;
 }
 
@@ -696,9 +697,18 @@ int mt_render_accumulate_device(mt_scene *sc, const mt_camera *cam, int w, int h
     return render_dev<float>(sc, cam, w, h, s1, s0, s1, depth, m, out_kind, accum_dev, (cudaStream_t)stream, false);
 }
 
-int mt_get_stats(const mt_scene *sc, mt_stats *out)
+int mt_get_stats(const mt_scene *csc, mt_stats *out)
 {
-    if (!sc || !out) return fail(MT_ERR_NULL, "NULL pointer");
+    if (!csc || !out) return fail(MT_ERR_NULL, "NULL pointer");
+    mt_scene *sc = const_cast<mt_scene *>(csc);
+    if (sc->counting) {
+        // Asynchronous launches (mt_render_accumulate_device) leave the
+        // counters on the device: wait for them and read them here.
+        int rc = set_device(sc);
+        if (rc) return rc;
+        CK(cudaDeviceSynchronize(), "mt_get_stats");
+        if ((rc = read_counters(sc))) return rc;
+    }
     *out = sc->stats;
     return 0;
 }

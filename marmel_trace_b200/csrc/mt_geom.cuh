@@ -476,7 +476,7 @@ MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tma
 {
     bool found = false;
     R closest = tmax;
-    unsigned long long nvis = 0, ntest = 0;
+    unsigned long long nvis = 0, ntest = 0, ntri = 0;
 
     for (int i = 0; i < S.plane_count; ++i) {
         R t;
@@ -540,6 +540,7 @@ MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tma
                     int2 ref = __ldg(S.refs + first + i);
                     R t, u, v;
                     ++ntest;
+                    ntri += (ref.y >> 28) == KIND_TRIANGLE;
                     if (prim_hit_t(S, ref.y, rp, tmin, closest, &t, &u, &v)) {
                         if (!found || t < best->t || (t == best->t && ref.x < best->prim)) {
                             best->t = t;
@@ -558,6 +559,7 @@ MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tma
     if (S.counters) {
         count_add(&S.counters->node_visits, nvis);
         count_add(&S.counters->prim_tests, ntest);
+        count_add(&S.counters->tri_tests, ntri);
     }
     return found;
 }
@@ -567,7 +569,7 @@ MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tma
 // reorders the tests, so it is not needed for the same boolean.
 template <typename R> MT_D bool scene_any(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax)
 {
-    unsigned long long nvis = 0, ntest = 0;
+    unsigned long long nvis = 0, ntest = 0, ntri = 0;
     bool hit = false;
     for (int i = 0; i < S.plane_count && !hit; ++i) {
         R t;
@@ -611,6 +613,7 @@ template <typename R> MT_D bool scene_any(const DevScene<R> &S, const RayPre<R> 
                 for (int i = 0; i < count; ++i) {
                     int2 ref = __ldg(S.refs + first + i);
                     ++ntest;
+                    ntri += (ref.y >> 28) == KIND_TRIANGLE;
                     if (prim_occluded(S, ref.y, rp, tmin, tmax)) {
                         hit = true;
                         break;
@@ -622,6 +625,7 @@ template <typename R> MT_D bool scene_any(const DevScene<R> &S, const RayPre<R> 
     if (S.counters) {
         count_add(&S.counters->node_visits, nvis);
         count_add(&S.counters->prim_tests, ntest);
+        count_add(&S.counters->tri_tests, ntri);
     }
     return hit;
 }

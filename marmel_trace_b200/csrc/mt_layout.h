@@ -105,7 +105,8 @@ struct DevCounters {
     unsigned long long shadow_rays;
     unsigned long long node_visits;
     unsigned long long prim_tests;
-    unsigned long long pad[3];
+    unsigned long long tri_tests;
+    unsigned long long pad[2];
 };
 
 template <typename R> struct DevScene {
