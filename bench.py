@@ -6,17 +6,23 @@ emissive sphere lights, ground plane, sun and sky; seed 2) at 64 samples per
 pixel and depth 8 -- 132,710,400 path samples. Step k renders the sample
 window [64k, 64k+64), so successive steps refine the same image.
 
-value     : whole-job Msamples/s (device time, CUDA events on the launching
-            stream, max over ranks), inputs resident in HBM.
-e2e       : the same metric through the drop-in entry point
-            mt_pathtrace_render (camera from host memory, RGB8 image read back
-            to host memory every step).
-roofline  : dominant kernel against the measured HBM copy bandwidth, with the
-            canonical BVH2 byte accounting per ray (64 B per node pair, 48 B
-            per triangle, 16 B per sphere, 48 B of ray + hit record).
-time_to_rmse : linear-RGB RMSE 1e-3 reached at N* = mean(sigma^2) / 1e-6
-            samples per pixel for this unbiased estimator; sigma^2 is measured
-            from the timed frames themselves (variance of the per-frame means).
+value        : whole-job Msamples/s of the wavefront integrator (device time,
+               CUDA events on the launching stream, max over ranks), inputs
+               resident in HBM, L2 flushed between steps.
+plain_gpu    : the same frames through the megakernel (one thread per pixel,
+               the "plain GPU" form of the same estimator).
+e2e          : the same metric through the drop-in entry point
+               mt_pathtrace_render (camera from host memory, RGB8 image read
+               back to host memory every step).
+roofline     : dominant kernel (nearest-hit traversal: the wavefront's extend
+               stage) against the measured HBM copy bandwidth, canonical BVH2
+               accounting per ray: 64 B per node pair, 48 B per triangle,
+               16 B per other primitive, 48 B of ray + hit record.
+time_to_rmse : both integrators evaluate the same unbiased estimator with the
+               same random streams, so linear-RGB RMSE after N samples per
+               pixel is sqrt(mean sigma^2 / N); N* = mean(sigma^2) / 1e-6 and
+               the time to reach it follows from each integrator's
+               throughput. sigma^2 is measured from the timed frames.
 
 --impl reference times the reference's own multithreaded CPU path tracer
 (oracle/_ref, compiled from the reference sources) on the same scene.
@@ -26,6 +32,7 @@ scaling, no data-path collective).
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -40,16 +47,13 @@ os.environ.setdefault("RAYTRACER_NO_PROGRESS", "1")
 
 import numpy as np  # noqa: E402
 
-W, H, SPP, DEPTH = 1920, 1080, 64, 8
-WORKLOAD = "torus-field 1920x1080, 64 spp, depth 8, 1,048,576 triangles + 8 emissive spheres + plane (seed 2)"
-METRIC = "Msamples/s (1080p 64-spp path tracing, 1M-triangle PBR scene; time-to-RMSE 1e-3 beside)"
+W, H, DEPTH = 1920, 1080, 8
+WORKLOAD = "torus-field 1920x1080, 64 spp per step, depth 8, 1,048,576 triangles + 8 emissive spheres + plane (seed 2)"
+METRIC = "Msamples/s (1080p 64-spp path tracing, 1M-triangle PBR scene; wavefront vs plain GPU; time-to-RMSE 1e-3 beside)"
 
 
 def _dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
 class ClockSampler:
@@ -110,8 +114,7 @@ class ClockSampler:
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
-        d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
 
 
@@ -121,14 +124,48 @@ def build_scene():
     return scenes.torus_field_scene()
 
 
-def algorithmic_bytes(stats, samples_counted: int, samples_launch: int) -> float:
-    """Canonical BVH2 accounting (64 B per node pair, 48 B per triangle,
-    16 B per other primitive, 48 B ray + hit record per ray), scaled from the
-    counted launch to one timed launch."""
-    rays = stats.extension_rays + stats.shadow_rays
-    other = stats.prim_tests - stats.tri_tests
-    b = 64.0 * stats.node_visits + 48.0 * stats.tri_tests + 16.0 * other + 48.0 * rays
-    return b * samples_launch / samples_counted
+def traversal_bytes(st, kind: str) -> float:
+    """Canonical BVH2 bytes of the counted launch (nearest-hit or any-hit)."""
+    if kind == "nearest":
+        nodes, prims, tris, rays = st.node_visits, st.prim_tests, st.tri_tests, st.extension_rays
+    else:
+        nodes, prims, tris, rays = st.any_node_visits, st.any_prim_tests, st.any_tri_tests, st.shadow_rays
+    return 64.0 * nodes + 48.0 * tris + 16.0 * (prims - tris) + 48.0 * rays
+
+
+class Frames:
+    """Timed progressive frames through mt_render_accumulate_device."""
+
+    def __init__(self, g, cam, spp, torch):
+        self.g, self.cam, self.spp, self.torch = g, cam, spp, torch
+        self.stream = torch.cuda.current_stream()
+        self.accum = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
+
+    def render(self, k: int, spp: int | None = None, base: int = 0):
+        from marmel_trace_b200 import _capi
+
+        n = spp or self.spp
+        s0 = base + k * n
+        rc = self.g.lib.mt_render_accumulate_device(self.g.h, self.cam.ref, W, H, s0, s0 + n, DEPTH, 0,
+                                                    self.accum.data_ptr(), 0, self.stream.cuda_stream)
+        _capi.check(rc, "mt_render_accumulate_device")
+
+    def timed(self, steps: int, warmup: int, flush, keep_means: bool = False, base: int = 0):
+        torch = self.torch
+        for k in range(warmup):
+            self.render(k, base=10_000 + base)
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        means = []
+        for k in range(steps):
+            flush.zero_()
+            ev[k][0].record(self.stream)
+            self.render(k, base=base)
+            ev[k][1].record(self.stream)
+            if keep_means:
+                means.append((self.accum / self.spp).cpu())  # outside the events
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in ev], means
 
 
 def run_ours(args):
@@ -140,99 +177,112 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     import marmel_trace_b200 as mt
     from marmel_trace_b200 import _capi
 
+    SPP = args.spp
     desc = build_scene()
     cam = desc.make_camera(W, H)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
     g = mt.GpuScene(desc, precision="fp32", integrator=args.integrator, device=local)
-    lib = g.lib
-    stream = torch.cuda.current_stream()
-    accum = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+    fr = Frames(g, cam, SPP, torch)
 
-    def step(k: int, acc: int):
-        rc = lib.mt_render_accumulate_device(g.h, cam.ref, W, H, k * SPP, (k + 1) * SPP, DEPTH, 0,
-                                             accum.data_ptr(), acc, stream.cuda_stream)
-        _capi.check(rc, "mt_render_accumulate_device")
-
-    # counting pass (untimed): rays, node pairs, primitive tests per sample
+    # counting pass (untimed): rays, node pairs and primitive tests per sample
     g.set_counting(True)
-    cnt_spp = 4
-    rc = lib.mt_render_accumulate_device(g.h, cam.ref, W, H, 10_000, 10_000 + cnt_spp, DEPTH, 0, accum.data_ptr(), 0,
-                                         stream.cuda_stream)
-    _capi.check(rc, "count pass")
-    torch.cuda.synchronize()
+    fr.render(0, spp=4, base=20_000)
     cnt = g.stats()
     g.set_counting(False)
+    n_counted = W * H * 4
 
-    for k in range(args.warmup):
-        step(1000 + k, 0)
-    torch.cuda.synchronize()
-
-    frame_means = []
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         t_wall = time.perf_counter()
-        for k in range(args.steps):
-            flush.zero_()
-            ev[k][0].record(stream)
-            step(k, 0)
-            ev[k][1].record(stream)
-            if k < 8:
-                frame_means.append((accum / SPP).cpu())  # untimed readback between steps
-        torch.cuda.synchronize()
+        ms, means = fr.timed(args.steps, args.warmup, flush, keep_means=True)
         t_wall = time.perf_counter() - t_wall
     if dist:
         dist.barrier()
-    ms = [a.elapsed_time(b) for a, b in ev]
     dev_s = sum(ms) / 1e3
     if dist:
         t = torch.tensor([dev_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_s = float(t.item())
-    samples = W * H * SPP * args.steps * world
-    value = samples / dev_s / 1e6
-    st = g.stats()
+    samples_per_rank = W * H * SPP * args.steps
+    value = samples_per_rank * world / dev_s / 1e6
+    launches = int(g.stats().launches)
 
     # e2e through the drop-in entry point (host camera in, host RGB8 out)
     rgb = np.zeros((H, W, 3), np.uint8)
     e2e_ms = []
-    for k in range(0 if args.no_e2e else max(1, min(args.steps, 3))):
+    for _ in range(0 if args.no_e2e else max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        _capi.check(lib.mt_pathtrace_render(g.h, cam.ref, W, H, SPP, DEPTH, rgb.ctypes.data), "mt_pathtrace_render")
+        _capi.check(g.lib.mt_pathtrace_render(g.h, cam.ref, W, H, SPP, DEPTH, rgb.ctypes.data), "mt_pathtrace_render")
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_val = (W * H * SPP) / (statistics.median(e2e_ms) / 1e3) / 1e6 * world if e2e_ms else None
+    e2e_val = W * H * SPP / (statistics.median(e2e_ms) / 1e3) / 1e6 * world if e2e_ms else None
 
-    # time to RMSE 1e-3 from the measured per-pixel variance of 64-spp frames
+    # dominant-kernel duration: one frame with every stage bracketed by events
+    stage = None
+    if args.integrator == "wavefront":
+        gp = mt.GpuScene(desc, precision="fp32", integrator="wavefront", use_graph=-1, device=local)
+        fp = Frames(gp, cam, SPP, torch)
+        fp.render(0, base=30_000)
+        gp.set_counting(False)  # resets the stage timers
+        flush.zero_()
+        fp.render(0, base=40_000)
+        torch.cuda.synchronize()
+        st = gp.stats()
+        stage = {"extend_ms": st.stage_ms[0], "shade_ms": st.stage_ms[1], "shadow_ms": st.stage_ms[2],
+                 "other_ms": st.stage_ms[3], "extend_launches": int(st.stage_launches[0]),
+                 "shadow_launches": int(st.stage_launches[2])}
+        gp.release()
+        del fp
+
+    # plain-GPU comparison (megakernel) on the same kind of frames
+    plain = None
+    if args.integrator == "wavefront" and not args.no_plain:
+        gm = mt.GpuScene(desc, precision="fp32", integrator="megakernel", device=local)
+        fm = Frames(gm, cam, SPP, torch)
+        pms, _ = fm.timed(args.plain_steps, 1, flush, base=50_000)
+        plain = W * H * SPP * len(pms) / (sum(pms) / 1e3) / 1e6
+        gm.release()
+        del fm
+
+    # time to RMSE 1e-3
     ttr = None
-    if len(frame_means) >= 3:
-        fm = torch.stack(frame_means).double()
-        var64 = fm.var(dim=0, unbiased=True).mean().item()  # variance of a 64-spp mean, per channel
-        sigma2 = var64 * SPP
+    if len(means) >= 3:
+        fm_ = torch.stack(means).double()
+        var_frame = fm_.var(dim=0, unbiased=True).mean().item()  # variance of a SPP-sample mean, per channel
+        sigma2 = var_frame * SPP
         n_star = sigma2 / 1e-6
-        ttr = {"rmse_target": 1e-3, "spp_needed": n_star, "seconds": n_star * W * H / (value * 1e6 / world),
-               "sigma2_per_sample": sigma2, "rmse_at_64spp": var64 ** 0.5,
-               "method": "N* = mean per-pixel sample variance / 1e-6 (unbiased estimator); variance measured "
-                         "across the timed frames"}
+        ttr = {"rmse_target": 1e-3, "sigma2_per_sample": sigma2, "rmse_per_frame": var_frame ** 0.5,
+               "spp_needed": n_star,
+               "seconds_wavefront" if args.integrator == "wavefront" else "seconds": n_star * W * H / (value / world * 1e6)}
+        if plain:
+            ttr["seconds_plain_gpu"] = n_star * W * H / (plain * 1e6)
+            ttr["speedup_vs_plain"] = (value / world) / plain
 
     peak, peak_kind = peaks()
-    kernel_s = (sum(ms) / 1e3) / args.steps  # this rank's average launch duration
-    alg = algorithmic_bytes(cnt, W * H * cnt_spp, W * H * SPP)
-    achieved = alg / kernel_s / 1e9
-    rays_per_sample = (cnt.extension_rays + cnt.shadow_rays) / (W * H * cnt_spp)
+    rays_per_sample = (cnt.extension_rays + cnt.shadow_rays) / n_counted
+    if stage:
+        alg = traversal_bytes(cnt, "nearest") * (W * H * SPP) / n_counted
+        achieved = alg / (stage["extend_ms"] / 1e3) / 1e9
+        kernel = "k_wf_extend<float> (nearest-hit traversal; per-stage CUDA events over one 64-spp frame)"
+        per_launch = alg / stage["extend_launches"]
+    else:
+        alg = (traversal_bytes(cnt, "nearest") + traversal_bytes(cnt, "any")) * (W * H * SPP) / n_counted
+        achieved = alg / (sum(ms) / 1e3 / args.steps) / 1e9
+        kernel = "k_render<float, PT> (megakernel)"
+        per_launch = alg
     traffic = None
     tf = ROOT / "profiles" / "traffic_bytes_per_sample.json"
     if tf.exists():
         tv = json.loads(tf.read_text()).get(args.integrator)
         if tv:
-            traffic = tv * W * H * SPP
+            traffic = tv * W * H * SPP / (stage["extend_launches"] if stage else 1)
 
     out = {
         "metric": METRIC,
@@ -249,18 +299,19 @@ def run_ours(args):
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": SPP, "depth": DEPTH,
                    "integrator": args.integrator, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between timed steps (256 MB write); scene 90 MB < L2"},
+                   "l2": "flushed between timed steps (256 MB write); the 90 MB scene fits in L2"},
+        "plain_gpu_msamples_s": round(plain, 3) if plain else None,
         "mrays_per_s": round(value * rays_per_sample, 2),
         "rays_per_sample": round(rays_per_sample, 3),
         "time_to_rmse": ttr,
+        "stage_ms": stage,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
-                     "kernel": "k_render<float, PT> (megakernel)" if args.integrator == "megakernel" else "wavefront",
-                     "algorithmic_bytes_per_launch": alg},
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                     "kernel": kernel, "algorithmic_bytes_per_launch": per_launch},
         "e2e": {"value": round(e2e_val, 3) if e2e_val else None, "unit": "Msamples/s", "h2d_bytes_per_step": 128,
                 "d2h_bytes_per_step": W * H * 3, "entry_point": "mt_pathtrace_render"},
-        "gpu_launches": int(st.launches) * args.steps,
+        "gpu_launches": launches * args.steps,
         "wall_s_timed_loop": round(t_wall, 3),
     }
     if rank == 0:
@@ -293,12 +344,10 @@ def cpu_baseline(desc, cam, spp: int):
 
 
 def run_reference(args):
-    rank, world, local = _dist_env()
+    rank, world, _ = _dist_env()
     if rank != 0:
         return
     from oracle import ref
-
-    import marmel_trace_b200 as mt  # noqa: F401  (camera_create through the C ABI's host code)
 
     desc = build_scene()
     cam = desc.make_camera(W, H)
@@ -314,7 +363,7 @@ def run_reference(args):
         rs.pathtrace_render(W, H, spp, DEPTH)
         times.append(time.perf_counter() - t0)
     value = W * H * spp * len(times) / sum(times) / 1e6
-    out = {
+    print(json.dumps({
         "impl": "reference",
         "metric": METRIC,
         "value": round(value, 4),
@@ -334,8 +383,7 @@ def run_reference(args):
                          "sample": f"each step: pathtrace_render full frame at {spp} spp (bounded sample of the "
                                    f"64-spp workload)"},
         "e2e": {"value": round(value, 4), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(out), flush=True)
+    }), flush=True)
 
 
 def main():
@@ -344,15 +392,15 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--integrator", default="megakernel", choices=["megakernel", "wavefront"])
+    ap.add_argument("--integrator", default="wavefront", choices=["megakernel", "wavefront"])
+    ap.add_argument("--spp", type=int, default=64, help="samples per pixel per step")
     ap.add_argument("--cpu-spp", type=int, default=1)
+    ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--spp", type=int, default=SPP, help="samples per pixel per step (profiling cases)")
-    ap.add_argument("--no-e2e", action="store_true", help="skip the e2e leg (profiling cases)")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
-    globals()["SPP"] = args.spp
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -195,7 +195,8 @@ typedef struct {
     int32_t queue_capacity;  /* wavefront paths in flight, 0 = library default  */
     int32_t bvh_width;       /* 2, 4 or 8; 0 = library default                  */
     int32_t sort_threshold;  /* wavefront: sort by material above this many paths (0 = never) */
-    int32_t use_graph;       /* wavefront: capture the spp loop in a CUDA graph */
+    int32_t use_graph;       /* wavefront: 1 = capture the sample window in a CUDA graph,
+                                0 = plain launches, -1 = plain launches timed per stage */
     int32_t device;          /* CUDA device ordinal                             */
 } mt_options;
 
@@ -298,11 +299,19 @@ typedef struct {
     int64_t primary_rays;     /* camera rays                                     */
     int64_t extension_rays;   /* nearest-hit rays incl. primary                  */
     int64_t shadow_rays;      /* NEE / any-hit rays                              */
-    int64_t node_visits;      /* inner nodes whose two child boxes were tested   */
-    int64_t prim_tests;       /* primitive intersection tests (planes included)  */
+    int64_t node_visits;      /* nearest-hit queries: inner nodes whose two child
+                                 boxes were tested                               */
+    int64_t prim_tests;       /* nearest-hit primitive tests (planes included)   */
     int64_t tri_tests;        /* of which triangle tests                         */
+    int64_t any_node_visits;  /* the same three for any-hit (shadow) queries     */
+    int64_t any_prim_tests;
+    int64_t any_tri_tests;
     int32_t launches;         /* kernels launched                                */
     int32_t error_flags;      /* device error word (0 = clean)                   */
+    /* Wavefront stage timing (use_graph < 0 only; reset by mt_set_counting):
+     * device ms and launches of extend, shade, shadow and the other kernels. */
+    double  stage_ms[4];
+    int64_t stage_launches[4];
 } mt_stats;
 int mt_get_stats(const mt_scene *scene, mt_stats *out);
 /* Enable (1) or disable (0) the ray / node counters (off by default: they

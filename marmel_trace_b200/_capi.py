@@ -172,8 +172,13 @@ class MtStats(C.Structure):
         ("node_visits", C.c_int64),
         ("prim_tests", C.c_int64),
         ("tri_tests", C.c_int64),
+        ("any_node_visits", C.c_int64),
+        ("any_prim_tests", C.c_int64),
+        ("any_tri_tests", C.c_int64),
         ("launches", C.c_int32),
         ("error_flags", C.c_int32),
+        ("stage_ms", C.c_double * 4),
+        ("stage_launches", C.c_int64 * 4),
     ]
 
 

@@ -33,6 +33,7 @@ UNITS = [
     ("mt_kernels_f32.cu", []),
     ("mt_kernels_f64.cu", ["--fmad=false"]),
     ("mt_wavefront.cu", []),
+    ("mt_wavefront_f64.cu", ["--fmad=false"]),
     ("mt_bvh.cpp", []),
 ]
 

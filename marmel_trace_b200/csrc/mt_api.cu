@@ -271,6 +271,11 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     S->prim_count = n;
     S->material_count = d->material_count;
     S->water_material = d->water_material;
+    // pt_occluded_segment passes through water and transparency > 0.8
+    // (src/pathtrace.c:516); without such a material it is an any-hit query.
+    S->has_passthrough = 0;
+    for (int i = 0; i < d->material_count; ++i)
+        if (d->materials[i].is_water || d->materials[i].transparency > 0.8) S->has_passthrough = 1;
     S->water_level = (R)d->water_level;
     S->ocean.enabled = d->ocean.enabled;
     S->ocean.seed = d->ocean.seed;
@@ -360,6 +365,9 @@ int read_counters(mt_scene *sc)
     sc->stats.node_visits = (int64_t)c.node_visits;
     sc->stats.prim_tests = (int64_t)c.prim_tests;
     sc->stats.tri_tests = (int64_t)c.tri_tests;
+    sc->stats.any_node_visits = (int64_t)c.any_node_visits;
+    sc->stats.any_prim_tests = (int64_t)c.any_prim_tests;
+    sc->stats.any_tri_tests = (int64_t)c.any_tri_tests;
     return 0;
 }
 
@@ -384,7 +392,7 @@ int render_dev(mt_scene *sc, const mt_camera *cam, int w, int h, int spp_total, 
     DevScene<R> S = dev_scene<R>(sc);
     S.counters = sc->counting ? sc->d_counters : nullptr;
     if (sc->opts.integrator == MT_INTEGRATOR_WAVEFRONT && mode == RENDER_PT) {
-        int rc = wavefront_render<R>(sc->wf, S, dc, w, h, s0, s1, depth, out_kind, dout, stream, &sc->opts,
+        int rc = wavefront_render(sc->wf, S, dc, w, h, s0, s1, depth, out_kind, dout, stream, &sc->opts,
                                      timed ? sc->ev0 : nullptr, timed ? sc->ev1 : nullptr, &sc->stats.launches);
         if (rc) return fail(rc, "wavefront render failed: %s", wavefront_last_error());
         return 0;
@@ -709,6 +717,13 @@ int mt_get_stats(const mt_scene *csc, mt_stats *out)
         CK(cudaDeviceSynchronize(), "mt_get_stats");
         if ((rc = read_counters(sc))) return rc;
     }
+    double ms[4];
+    long long nl[4];
+    wavefront_stage_times(sc->wf, ms, nl);
+    for (int i = 0; i < 4; ++i) {
+        sc->stats.stage_ms[i] = ms[i];
+        sc->stats.stage_launches[i] = nl[i];
+    }
     *out = sc->stats;
     return 0;
 }
@@ -719,6 +734,7 @@ int mt_set_counting(mt_scene *sc, int enable)
     sc->counting = enable != 0;
     sc->sf.counters = nullptr;
     sc->sd.counters = nullptr;
+    wavefront_reset_stage_times(sc->wf);
     return reset_counters(sc);
 }
 

@@ -623,9 +623,9 @@ template <typename R> MT_D bool scene_any(const DevScene<R> &S, const RayPre<R> 
         }
     }
     if (S.counters) {
-        count_add(&S.counters->node_visits, nvis);
-        count_add(&S.counters->prim_tests, ntest);
-        count_add(&S.counters->tri_tests, ntri);
+        count_add(&S.counters->any_node_visits, nvis);
+        count_add(&S.counters->any_prim_tests, ntest);
+        count_add(&S.counters->any_tri_tests, ntri);
     }
     return hit;
 }

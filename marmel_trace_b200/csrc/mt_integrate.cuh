@@ -145,6 +145,11 @@ MT_D bool pt_occluded_segment(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R 
     V3<R> cur_o = o;
     R remaining = tmax;
     if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
+    if (!S.has_passthrough) {
+        // No material lets the segment through: the walk below stops at its
+        // first hit, so "occluded" is exactly "any hit in [tmin, tmax]".
+        return scene_any(S, ray_pre(o, unit_dir(d)), tmin, tmax);
+    }
     for (int step = 0; step < 6; ++step) {
         SurfaceHit<R> h;
         if (!scene_intersect(S, cur_o, d, tmin, remaining, &h)) return false;

@@ -106,7 +106,10 @@ struct DevCounters {
     unsigned long long node_visits;
     unsigned long long prim_tests;
     unsigned long long tri_tests;
-    unsigned long long pad[2];
+    unsigned long long any_node_visits;   // the same three for any-hit queries
+    unsigned long long any_prim_tests;
+    unsigned long long any_tri_tests;
+    unsigned long long pad;
 };
 
 template <typename R> struct DevScene {
@@ -129,6 +132,7 @@ template <typename R> struct DevScene {
     int material_count;
     int light_count;
     int water_material;
+    int has_passthrough;   // some material lets shadow rays through (water, transparency > 0.8)
     R water_level;
     DevOcean<R> ocean;
     DevSky<R> sky;

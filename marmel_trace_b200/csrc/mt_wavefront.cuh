@@ -1,0 +1,495 @@
+// mt_wavefront.cuh - wavefront path tracer: per-bounce stage kernels over
+// compacted queues (device side).
+//
+// A batch holds every pixel of the image times `batch_spp` samples. Bounce b
+// of all live paths runs as three kernels:
+//   extend  : nearest hit of every queued ray (pure traversal, few registers)
+//   shade   : medium / emission / NEE set-up / BSDF sample / Russian roulette
+//             (pathtrace_radiance's loop body, src/pathtrace.c:835-1018); NEE
+//             connections go to the shadow queue, surviving paths to the next
+//             ray queue. Both queues are compacted with one atomicAdd per
+//             warp (ballot + popc), so terminated paths stop occupying lanes.
+//   shadow  : pt_occluded_segment for every NEE connection; the visible
+//             contribution lands in the path's NEE slot for that light.
+// The NEE slots are summed into the path radiance in light order (then the
+// sun) at the path's next shade or at the end of the batch, which is the
+// order the reference adds them. Per-sample radiance is reduced into the
+// pixel accumulator in sample order, as pt_render_pixel sums it.
+#pragma once
+
+#include "mt_integrate.cuh"
+#include "mt_launch.h"
+
+namespace mt {
+
+static constexpr int kNeeSlots = kMaxLights + 1;  // 8 sphere lights + the sun
+
+template <typename R> struct WfRay {
+    R o[3];
+    R d[3];
+    int slot;
+    int pad;
+};
+
+template <typename R> struct WfHit {
+    R t, u, v;
+    int prim;
+    int code;
+};
+
+template <typename R> struct WfPath {
+    R throughput[3];
+    R radiance[3];
+    uint32_t seed_key;
+    int medium;
+    int last_specular;
+    int pad;
+};
+
+template <typename R> struct WfShadow {
+    R o[3];
+    R d[3];
+    R tmax;
+    R contrib[3];
+    int slot;
+    int li;
+};
+
+// Parameters that change between calls live in device memory, so one
+// captured CUDA graph serves every call with the same shape.
+template <typename R> struct WfParams {
+    DevCamera<R> cam;
+    void *out;
+    int w, h, wh;
+    int s0;            // first sample of the window
+    int spp_window;    // samples in the window
+    int out_kind;
+};
+
+struct WfCounters {
+    int ray_count[2];
+    int shadow_count;
+    int pad;
+};
+
+// Warp-aggregated queue append: one atomicAdd per warp, lanes get
+// consecutive slots in lane order.
+MT_D int warp_append(int *counter, bool want)
+{
+    unsigned mask = __activemask();
+    unsigned ballot = __ballot_sync(mask, want);
+    if (!ballot) return -1;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(ballot) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(ballot));
+    base = __shfl_sync(mask, base, leader);
+    if (!want) return -1;
+    return base + __popc(ballot & ((1u << lane) - 1u));
+}
+
+// ------------------------------------------------------------------
+// generate: primary rays of a batch (pt_render_pixel, src/pathtrace.c:1053-1086)
+// ------------------------------------------------------------------
+template <typename R>
+__global__ void k_wf_generate(const DevScene<R> S, const WfParams<R> *P, int batch, int batch_spp, int n_paths,
+                              WfPath<R> *paths, WfRay<R> *rays, WfCounters *C, R *nee)
+{
+    const WfParams<R> p = *P;
+    const int n_round = (n_paths + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x) * (gridDim.x * blockDim.x);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += gridDim.x * blockDim.x) {
+        if (q >= n_paths) {
+            warp_append(&C->ray_count[0], false);
+            continue;
+        }
+        int s = p.s0 + batch * batch_spp + q / p.wh;
+        int pix = q % p.wh;
+        int x = pix % p.w, y = pix / p.w;
+        Ray3<R> ray = pt_primary(S, p.cam, p.w, p.h, x, y, s);
+        WfPath<R> st;
+        for (int k = 0; k < 3; ++k) {
+            st.throughput[k] = R(1);
+            st.radiance[k] = R(0);
+        }
+        st.seed_key = hash3((uint32_t)x, (uint32_t)y, (uint32_t)s);
+        st.last_specular = 1;
+        st.pad = 0;
+        // medium if the eye is under water (src/pathtrace.c:821-826)
+        st.medium = -1;
+        if (S.water_material >= 0) {
+            R w_h = water_height(S, ray.o.x, ray.o.z);
+            if (ray.o.y < w_h && S.water_material < S.material_count) st.medium = S.water_material;
+        }
+        V3<R> d = normalize(ray.d);
+        for (int k = 0; k < kNeeSlots * 3; ++k) nee[(size_t)q * kNeeSlots * 3 + k] = R(0);
+        paths[q] = st;
+        bool live = length_sq(d) > R(0);  // degenerate primary ray: zero radiance
+        int at = warp_append(&C->ray_count[0], live);
+        if (live) {
+            WfRay<R> r;
+            r.o[0] = ray.o.x; r.o[1] = ray.o.y; r.o[2] = ray.o.z;
+            r.d[0] = d.x; r.d[1] = d.y; r.d[2] = d.z;
+            r.slot = q;
+            r.pad = 0;
+            rays[at] = r;
+        }
+    }
+    if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->primary_rays, (unsigned long long)n_paths);
+}
+
+// ------------------------------------------------------------------
+// extend: nearest hit (scene_intersect, src/scene.c:767 -> src/bvh.c:557)
+// ------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_wf_extend(const DevScene<R> S, const WfRay<R> *rays, const WfCounters *C,
+                                                   int which, WfHit<R> *hits)
+{
+    const int n = C->ray_count[which];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const WfRay<R> r = rays[q];
+        V3<R> o = v3(r.o[0], r.o[1], r.o[2]);
+        V3<R> d = unit_dir(v3(r.d[0], r.d[1], r.d[2]));
+        RayPre<R> rp = ray_pre(o, d);
+        Hit<R> h;
+        WfHit<R> out;
+        if (scene_nearest(S, rp, R(1e-4), R(1e30), &h)) {
+            out.t = h.t;
+            out.u = h.u;
+            out.v = h.v;
+            out.prim = h.prim;
+            out.code = h.code;
+        } else {
+            out.t = R(0);
+            out.u = R(0);
+            out.v = R(0);
+            out.prim = -1;
+            out.code = 0;
+        }
+        hits[q] = out;
+    }
+    if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->extension_rays, (unsigned long long)n);
+}
+
+template <typename R> MT_D void gather_nee(const DevScene<R> &S, R *nee_slot, V3<R> *radiance)
+{
+    V3<R> sum = v3(R(0), R(0), R(0));
+    for (int li = 0; li < S.light_count; ++li)
+        sum = add(sum, v3(nee_slot[3 * li], nee_slot[3 * li + 1], nee_slot[3 * li + 2]));
+    if (S.light_count > 0) *radiance = add(*radiance, sum);
+    *radiance = add(*radiance, v3(nee_slot[3 * kMaxLights], nee_slot[3 * kMaxLights + 1], nee_slot[3 * kMaxLights + 2]));
+    for (int k = 0; k < kNeeSlots * 3; ++k) nee_slot[k] = R(0);
+}
+
+template <typename R>
+MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> d, R tmax, V3<R> contrib, int slot,
+                      int li)
+{
+    int at = warp_append(&C->shadow_count, want);
+    if (want) {
+        WfShadow<R> s;
+        s.o[0] = o.x; s.o[1] = o.y; s.o[2] = o.z;
+        s.d[0] = d.x; s.d[1] = d.y; s.d[2] = d.z;
+        s.tmax = tmax;
+        s.contrib[0] = contrib.x; s.contrib[1] = contrib.y; s.contrib[2] = contrib.z;
+        s.slot = slot;
+        s.li = li;
+        sq[at] = s;
+    }
+}
+
+// ------------------------------------------------------------------
+// shade: one bounce of pathtrace_radiance (src/pathtrace.c:835-1018)
+// ------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
+                                                  WfCounters *C, int which, int b, int max_depth, WfPath<R> *paths,
+                                                  R *nee, WfRay<R> *rays_out, WfShadow<R> *sq)
+{
+    const int n = C->ray_count[which];
+    const int stride = gridDim.x * blockDim.x;
+    // Every lane of a warp walks the same number of iterations, so the
+    // warp-wide queue appends below always see the whole warp.
+    const int n_round = (n + stride - 1) / stride * stride;
+    const V3<R> zero = v3(R(0), R(0), R(0));
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
+        const bool active = q < n;
+        WfPath<R> st;
+        int slot = -1, prim = -1;
+        V3<R> throughput = zero, radiance = zero;
+        V3<R> beta = zero;       // throughput before the BSDF update: NEE weight
+        V3<R> P = zero, N = zero, V = zero;
+        V3<R> next_o = zero, next_d = zero;
+        int mat = -1;
+        bool shade_hit = false, do_sun = false, cont = false;
+        if (active) {
+            const WfRay<R> r = rays_in[q];
+            const WfHit<R> hh = hits[q];
+            slot = r.slot;
+            prim = hh.prim;
+            st = paths[slot];
+            throughput = v3(st.throughput[0], st.throughput[1], st.throughput[2]);
+            radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
+            if (b > 0) gather_nee(S, nee + (size_t)slot * kNeeSlots * 3, &radiance);
+            const V3<R> ro = v3(r.o[0], r.o[1], r.o[2]);
+            const V3<R> d = v3(r.d[0], r.d[1], r.d[2]);
+            if (hh.prim < 0) {
+                // escaped: medium fallback depth then the sky (src/pathtrace.c:837-857)
+                if (st.medium >= 0) {
+                    pt_apply_medium(S.materials[st.medium], R(5.0), &throughput, &radiance);
+                    st.medium = -1;
+                }
+                radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
+            } else {
+                Hit<R> th;
+                th.t = hh.t;
+                th.u = hh.u;
+                th.v = hh.v;
+                th.prim = hh.prim;
+                th.code = hh.code;
+                SurfaceHit<R> h;
+                finish_hit(S, ro, unit_dir(d), th, &h);
+                if (st.medium >= 0) pt_apply_medium(S.materials[st.medium], h.t, &throughput, &radiance);
+                if (h.material < 0 || h.material >= S.material_count) {
+                    radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
+                } else {
+                    const DevMaterial<R> &m = S.materials[h.material];
+                    P = h.point;
+                    N = h.normal;
+                    if (m.is_water) {
+                        if (mfabs(h.normal.y) > R(0.999) && mfabs(h.normal.x) < R(1e-4) && mfabs(h.normal.z) < R(1e-4))
+                            N = water_normal(P.x, P.z, R(0));
+                    }
+                    if (dot(N, d) > R(0)) N = neg(N);
+                    N = normalize(N);
+                    if (length_sq(N) > R(0)) {
+                        V = neg(d);
+                        mat = h.material;
+                        shade_hit = true;
+                        beta = throughput;
+                        if (b == 0 || st.last_specular) radiance = add(radiance, mul(throughput, mat3(m.emissive)));
+                        if (b == 0 && length_sq(mat3(m.atmosphere_glow)) > R(1e-6))
+                            radiance = add(radiance, mul(throughput, atmosphere_term(m, N, V, mat3(S.sky.sun_dir))));
+                        do_sun = (b == 0 || (b == 1 && st.medium >= 0 && st.last_specular));
+                        // BSDF sample, throughput update, medium, roulette, advance
+                        uint32_t kb = hash3(st.seed_key ^ PT_KEY, (uint32_t)b, 0u);
+                        R u1 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_A);
+                        R u2 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_B);
+                        R u_lobe = rand01<R>(kb, (uint32_t)b, PT_CH_LOBE);
+                        R u_glass = rand01<R>(kb, (uint32_t)b, PT_CH_GLASS);
+                        V3<R> wi, w;
+                        int refracted = 0, sampled_specular = 0;
+                        bool ok;
+                        if (m.pbr)
+                            ok = pt_sample_pbr(m, N, d, V, u1, u2, u_lobe, &wi, &w, &sampled_specular);
+                        else
+                            ok = pt_sample_legacy(m, N, d, V, h.front_face, u1, u2, u_lobe, u_glass, &wi, &w,
+                                                  &refracted, &sampled_specular);
+                        if (ok) {
+                            st.last_specular = sampled_specular;
+                            throughput = mul(throughput, w);
+                            if (finite3(throughput) && pt_max_component(throughput) > R(0)) {
+                                if (refracted && (m.is_water || m.beer_lambert))
+                                    st.medium = h.front_face ? h.material : -1;
+                                bool alive = true;
+                                if (b >= 2) {  // PT_RR_START_BOUNCE (src/pathtrace.c:69)
+                                    R qv = pt_clamp01(pt_max_component(throughput));
+                                    if (!(qv > R(0))) {
+                                        alive = false;
+                                    } else {
+                                        R u_rr = rand01<R>(kb, (uint32_t)b, PT_CH_RR);
+                                        if (u_rr >= qv) alive = false;
+                                        else throughput = scale(throughput, R(1) / qv);
+                                    }
+                                }
+                                if (alive && b < max_depth) {
+                                    V3<R> offset = refracted ? scale(wi, R(1e-4))
+                                                             : scale(N, dot(wi, N) >= R(0) ? R(1e-4) : R(-1e-4));
+                                    next_o = add(P, offset);
+                                    next_d = wi;
+                                    cont = true;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        // ---- NEE connections of this bounce (lights in order, then the sun) ----
+        // pt_nee_emissive (src/pathtrace.c:576-606)
+        for (int li = 0; li < S.light_count; ++li) {
+            bool want = false;
+            V3<R> so = zero, wi = zero, contrib = zero;
+            R tmax = R(0);
+            if (shade_hit) {
+                const DevLight<R> &lt = S.lights[li];
+                if (lt.prim != prim) {
+                    V3<R> to_c = sub(mat3(lt.center), P);
+                    R dc2 = length_sq(to_c);
+                    R dc = msqrt(dc2);
+                    if (dc > lt.radius) {
+                        R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
+                        R Omega = R(2) * R(3.14159265358979323846) * (R(1) - cos_mx);
+                        if (Omega > R(0)) {
+                            V3<R> w = scale(to_c, R(1) / dc);
+                            R u1 = rand01<R>(st.seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
+                            R u2 = rand01<R>(st.seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
+                            wi = light_sphere_sample_dir(w, cos_mx, u1, u2);
+                            if (finite3(wi) && dot(N, wi) > R(0)) {
+                                so = add(P, scale(N, R(1e-3)));
+                                R lt_t;
+                                if (light_sphere_t(S, lt.prim, so, wi, R(1e-3), R(1e30), &lt_t)) {
+                                    V3<R> lit = shade(S.materials[mat], N, wi, V, mat3(lt.emissive));
+                                    contrib = mul(beta, scale(lit, Omega));
+                                    tmax = lt_t - R(1e-3);
+                                    want = true;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            push_shadow(sq, C, want, so, wi, tmax, contrib, slot, li);
+        }
+        {
+            // pt_nee_sun (src/pathtrace.c:534-556)
+            bool want = false;
+            V3<R> so = zero, L = zero, contrib = zero;
+            if (shade_hit && do_sun) {
+                R r1 = rand01<R>(st.seed_key, (uint32_t)b, PT_CH_NEE_SUN_A);
+                R r2 = rand01<R>(st.seed_key, (uint32_t)b, PT_CH_NEE_SUN_B);
+                L = sun_disk_dir(mat3(S.sky.sun_dir), S.sky.sun_radius, r1, r2);
+                if (finite3(L) && dot(N, L) > R(0)) {
+                    so = add(P, scale(N, R(1e-3)));
+                    R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
+                    R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
+                    V3<R> lit = shade(S.materials[mat], N, L, V, mat3(S.sky.sun_color));
+                    contrib = mul(beta, scale(lit, Omega));
+                    want = true;
+                }
+            }
+            push_shadow(sq, C, want, so, L, R(1e30), contrib, slot, kMaxLights);
+        }
+        // ---- next ray ----
+        int at = warp_append(&C->ray_count[which ^ 1], cont);
+        if (cont) {
+            WfRay<R> nr;
+            nr.o[0] = next_o.x; nr.o[1] = next_o.y; nr.o[2] = next_o.z;
+            nr.d[0] = next_d.x; nr.d[1] = next_d.y; nr.d[2] = next_d.z;
+            nr.slot = slot;
+            nr.pad = 0;
+            rays_out[at] = nr;
+        }
+        if (active) {
+            st.throughput[0] = throughput.x;
+            st.throughput[1] = throughput.y;
+            st.throughput[2] = throughput.z;
+            st.radiance[0] = radiance.x;
+            st.radiance[1] = radiance.y;
+            st.radiance[2] = radiance.z;
+            paths[slot] = st;
+        }
+    }
+}
+
+// ------------------------------------------------------------------
+// shadow: pt_occluded_segment (src/pathtrace.c:504-532) per NEE connection
+// ------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
+                                                   R *nee)
+{
+    const int n = C->shadow_count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const WfShadow<R> s = sq[q];
+        V3<R> o = v3(s.o[0], s.o[1], s.o[2]);
+        V3<R> d = v3(s.d[0], s.d[1], s.d[2]);
+        V3<R> atten;
+        bool occ;
+        if (S.has_passthrough) {
+            occ = pt_occluded_segment(S, o, d, R(1e-3), s.tmax, &atten);
+        } else {
+            // No material lets a shadow ray through: the chained nearest-hit
+            // walk stops at its first hit, so it equals an any-hit query.
+            atten = v3(R(1), R(1), R(1));
+            if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
+            occ = scene_any(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
+        }
+        V3<R> res = v3(R(0), R(0), R(0));
+        if (!occ) {
+            bool dark = s.li == kMaxLights && atten.x < R(1e-4) && atten.y < R(1e-4) && atten.z < R(1e-4);
+            if (!dark) res = mul(v3(s.contrib[0], s.contrib[1], s.contrib[2]), atten);
+        }
+        R *slot = nee + ((size_t)s.slot * kNeeSlots + s.li) * 3;
+        slot[0] = res.x;
+        slot[1] = res.y;
+        slot[2] = res.z;
+    }
+}
+
+// ------------------------------------------------------------------
+// finalize + reduce: per-sample radiance (final clamp of
+// src/pathtrace.c:1020-1027) and the per-pixel sum in sample order
+// ------------------------------------------------------------------
+template <typename R>
+__global__ void k_wf_finalize(const DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, R *sample_buf)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_paths; q += gridDim.x * blockDim.x) {
+        const WfPath<R> st = paths[q];
+        V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
+        gather_nee(S, nee + (size_t)q * kNeeSlots * 3, &radiance);
+        if (!finite3(radiance)) radiance = v3(R(0), R(0), R(0));
+        if (radiance.x < R(0)) radiance.x = R(0);
+        if (radiance.y < R(0)) radiance.y = R(0);
+        if (radiance.z < R(0)) radiance.z = R(0);
+        sample_buf[3 * (size_t)q] = radiance.x;
+        sample_buf[3 * (size_t)q + 1] = radiance.y;
+        sample_buf[3 * (size_t)q + 2] = radiance.z;
+    }
+}
+
+template <typename R>
+__global__ void k_wf_reduce(const WfParams<R> *P, int batch_spp, int first_batch, int last_batch,
+                            const R *sample_buf, R *acc)
+{
+    const WfParams<R> p = *P;
+    for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < p.wh; pix += gridDim.x * blockDim.x) {
+        V3<R> a = v3(R(0), R(0), R(0));
+        if (!first_batch) a = v3(acc[3 * (size_t)pix], acc[3 * (size_t)pix + 1], acc[3 * (size_t)pix + 2]);
+        for (int j = 0; j < batch_spp; ++j) {
+            const R *sb = sample_buf + 3 * ((size_t)j * p.wh + pix);
+            a = add(a, v3(sb[0], sb[1], sb[2]));
+        }
+        if (!last_batch) {
+            acc[3 * (size_t)pix] = a.x;
+            acc[3 * (size_t)pix + 1] = a.y;
+            acc[3 * (size_t)pix + 2] = a.z;
+            continue;
+        }
+        size_t o = 3 * (size_t)pix;
+        if (p.out_kind == OUT_RGB8) {
+            V3<R> mean = scale(a, R(1) / R(p.spp_window));
+            unsigned char *op = (unsigned char *)p.out + o;
+            op[0] = to_byte(mean.x);
+            op[1] = to_byte(mean.y);
+            op[2] = to_byte(mean.z);
+        } else if (p.out_kind == OUT_MEAN_F32) {
+            V3<R> mean = scale(a, R(1) / R(p.spp_window));
+            float *op = (float *)p.out + o;
+            op[0] = (float)mean.x;
+            op[1] = (float)mean.y;
+            op[2] = (float)mean.z;
+        } else if (p.out_kind == OUT_SUM_F32) {
+            float *op = (float *)p.out + o;
+            op[0] = (float)a.x;
+            op[1] = (float)a.y;
+            op[2] = (float)a.z;
+        } else {
+            float *op = (float *)p.out + o;
+            op[0] += (float)a.x;
+            op[1] += (float)a.y;
+            op[2] += (float)a.z;
+        }
+    }
+}
+
+}  // namespace mt

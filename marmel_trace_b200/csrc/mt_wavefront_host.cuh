@@ -1,0 +1,249 @@
+// mt_wavefront_host.cuh - host driver of the wavefront integrator (one
+// arithmetic type per translation unit).
+//
+// The whole sample window [s0, s1) of a frame is captured once into a CUDA
+// graph: for every batch, generate -> (extend, shade, shadow) x (depth + 1)
+// -> finalize -> reduce, plus the queue-counter resets. Values that change
+// from call to call (camera, window start, output pointer) are read by the
+// kernels from a device-side parameter block that is refreshed by one
+// asynchronous copy before each graph launch, so a graph is re-captured only
+// when the frame's shape changes (size, batch split, depth).
+#pragma once
+
+#include <string.h>
+
+#include <string>
+
+#include "mt_wavefront.cuh"
+#include "mt_wavefront.h"
+
+namespace mt {
+
+struct WavefrontState {
+    int elem = 0;              // sizeof(R) of the buffers below
+    size_t cap_paths = 0;      // path slots allocated
+    int light_count = -1;
+    void *paths = nullptr, *rays[2] = {nullptr, nullptr}, *hits = nullptr, *nee = nullptr, *shadow = nullptr;
+    void *sample_buf = nullptr, *acc = nullptr, *params = nullptr;
+    WfCounters *counters = nullptr;
+    size_t acc_pixels = 0;
+    void *h_params = nullptr;  // pinned host copy of the parameter block
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::string key;
+    int grid = 0;              // persistent grid (blocks) of the stage kernels
+    cudaEvent_t kev[64];       // per-kernel timing events (profiling mode)
+    bool kev_init = false;
+    double kernel_ms[4] = {0, 0, 0, 0};  // extend, shade, shadow, other (profiling mode)
+    long long kernel_launches[4] = {0, 0, 0, 0};
+};
+
+namespace wfdetail {
+inline std::string &last_error()
+{
+    static thread_local std::string e;
+    return e;
+}
+inline int fail(int code, const char *what, cudaError_t e)
+{
+    last_error() = std::string(what) + ": " + cudaGetErrorString(e);
+    return code;
+}
+}  // namespace wfdetail
+
+#define WF_CK(call, what)                                                                               \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return wfdetail::fail(e_ == cudaErrorMemoryAllocation ? MT_ERR_OOM : MT_ERR_LAUNCH, what, e_); \
+    } while (0)
+
+inline void wf_free(WavefrontState *st)
+{
+    void **bufs[] = {&st->paths, &st->rays[0], &st->rays[1], &st->hits, &st->nee, &st->shadow, &st->sample_buf,
+                     &st->acc, &st->params};
+    for (void **b : bufs) {
+        if (*b) cudaFree(*b);
+        *b = nullptr;
+    }
+    if (st->counters) cudaFree(st->counters);
+    st->counters = nullptr;
+    if (st->exec) cudaGraphExecDestroy(st->exec);
+    st->exec = nullptr;
+    st->key.clear();
+    st->cap_paths = 0;
+    st->acc_pixels = 0;
+}
+
+// Grow the buffers to hold `n_paths` path slots and `wh` pixels.
+template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t wh, int light_count)
+{
+    if (st->elem == (int)sizeof(R) && st->cap_paths >= n_paths && st->acc_pixels >= wh && st->light_count == light_count)
+        return 0;
+    wf_free(st);
+    st->elem = sizeof(R);
+    st->light_count = light_count;
+    size_t nshadow = n_paths * (size_t)(light_count + 1);
+    WF_CK(cudaMalloc(&st->paths, n_paths * sizeof(WfPath<R>)), "cudaMalloc(paths)");
+    WF_CK(cudaMalloc(&st->rays[0], n_paths * sizeof(WfRay<R>)), "cudaMalloc(rays)");
+    WF_CK(cudaMalloc(&st->rays[1], n_paths * sizeof(WfRay<R>)), "cudaMalloc(rays)");
+    WF_CK(cudaMalloc(&st->hits, n_paths * sizeof(WfHit<R>)), "cudaMalloc(hits)");
+    WF_CK(cudaMalloc(&st->nee, n_paths * kNeeSlots * 3 * sizeof(R)), "cudaMalloc(nee)");
+    WF_CK(cudaMalloc(&st->shadow, (nshadow ? nshadow : 1) * sizeof(WfShadow<R>)), "cudaMalloc(shadow)");
+    WF_CK(cudaMalloc(&st->sample_buf, n_paths * 3 * sizeof(R)), "cudaMalloc(samples)");
+    WF_CK(cudaMalloc(&st->acc, wh * 3 * sizeof(R)), "cudaMalloc(acc)");
+    WF_CK(cudaMalloc(&st->params, sizeof(WfParams<R>)), "cudaMalloc(params)");
+    WF_CK(cudaMalloc((void **)&st->counters, sizeof(WfCounters)), "cudaMalloc(counters)");
+    if (!st->h_params) WF_CK(cudaMallocHost(&st->h_params, 256), "cudaMallocHost(params)");
+    st->cap_paths = n_paths;
+    st->acc_pixels = wh;
+    return 0;
+}
+
+// Enqueue one frame window. In profiling mode (`prof`), every stage kernel is
+// bracketed by CUDA events and its time is added to st->kernel_ms.
+template <typename R>
+int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch_spp, int n_batches, int depth,
+               cudaStream_t s, bool prof, int block)
+{
+    const int wh = w * h;
+    const int n_paths = wh * batch_spp;
+    WfPath<R> *paths = (WfPath<R> *)st->paths;
+    WfRay<R> *rays[2] = {(WfRay<R> *)st->rays[0], (WfRay<R> *)st->rays[1]};
+    WfHit<R> *hits = (WfHit<R> *)st->hits;
+    R *nee = (R *)st->nee;
+    WfShadow<R> *sq = (WfShadow<R> *)st->shadow;
+    R *sample_buf = (R *)st->sample_buf;
+    R *acc = (R *)st->acc;
+    const WfParams<R> *P = (const WfParams<R> *)st->params;
+    WfCounters *C = st->counters;
+    const int g = st->grid;
+    int ev = 0;
+    auto tic = [&]() {
+        if (prof) cudaEventRecord(st->kev[ev & 63], s);
+    };
+    auto toc = [&](int kind) {
+        if (!prof) return;
+        cudaEventRecord(st->kev[(ev + 1) & 63], s);
+        cudaEventSynchronize(st->kev[(ev + 1) & 63]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, st->kev[ev & 63], st->kev[(ev + 1) & 63]);
+        st->kernel_ms[kind] += ms;
+        st->kernel_launches[kind] += 1;
+        ev += 2;
+    };
+    for (int batch = 0; batch < n_batches; ++batch) {
+        WF_CK(cudaMemsetAsync(C, 0, sizeof(WfCounters), s), "memset(counters)");
+        tic();
+        k_wf_generate<R><<<g, block, 0, s>>>(S, P, batch, batch_spp, n_paths, paths, rays[0], C, nee);
+        toc(3);
+        int which = 0;
+        for (int b = 0; b <= depth; ++b) {
+            tic();
+            k_wf_extend<R><<<g, block, 0, s>>>(S, rays[which], C, which, hits);
+            toc(0);
+            WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
+            WF_CK(cudaMemsetAsync(&C->shadow_count, 0, sizeof(int), s), "memset(shadow_count)");
+            tic();
+            k_wf_shade<R><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee, rays[which ^ 1],
+                                              sq);
+            toc(1);
+            tic();
+            k_wf_shadow<R><<<g, block, 0, s>>>(S, sq, C, nee);
+            toc(2);
+            which ^= 1;
+        }
+        tic();
+        k_wf_finalize<R><<<g, block, 0, s>>>(S, n_paths, paths, nee, sample_buf);
+        k_wf_reduce<R><<<g, block, 0, s>>>(P, batch_spp, batch == 0, batch == n_batches - 1, sample_buf, acc);
+        toc(3);
+    }
+    WF_CK(cudaGetLastError(), "wavefront launch");
+    return 0;
+}
+
+template <typename R>
+int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCamera<R> &cam, int w, int h, int s0,
+                          int s1, int depth, int out_kind, void *out, cudaStream_t stream, const mt_options *opts,
+                          cudaEvent_t ev0, cudaEvent_t ev1, int32_t *launches)
+{
+    if (!st) st = new WavefrontState();
+    const int wh = w * h;
+    const int spp = s1 - s0;
+    // Batch size: the largest divisor of the window whose paths fit the queue.
+    long long cap = opts && opts->queue_capacity > 0 ? opts->queue_capacity : (8ll << 20);
+    if (cap < wh) cap = wh;
+    int batch_spp = 1;
+    for (int d = spp; d >= 1; --d)
+        if (spp % d == 0 && (long long)wh * d <= cap) {
+            batch_spp = d;
+            break;
+        }
+    int n_batches = spp / batch_spp;
+    int rc = wf_reserve<R>(st, (size_t)wh * batch_spp, (size_t)wh, S.light_count);
+    if (rc) return rc;
+    int block = 128;
+    if (!st->grid) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_extend<R>, block, 0);
+        if (per_sm < 1) per_sm = 1;
+        st->grid = sms * per_sm;
+    }
+    // parameter block
+    WfParams<R> hp;
+    memset(&hp, 0, sizeof hp);
+    hp.cam = cam;
+    hp.out = out;
+    hp.w = w;
+    hp.h = h;
+    hp.wh = wh;
+    hp.s0 = s0;
+    hp.spp_window = spp;
+    hp.out_kind = out_kind;
+    bool prof = opts && opts->use_graph < 0;   // profiling mode: no graph, per-kernel events
+    bool use_graph = !prof && (!opts || opts->use_graph != 0);
+    if (prof && !st->kev_init) {
+        for (int i = 0; i < 64; ++i) cudaEventCreate(&st->kev[i]);
+        st->kev_init = true;
+    }
+    if (ev0) WF_CK(cudaEventRecord(ev0, stream), "cudaEventRecord");
+    // The parameter copy is ordered on `stream` before the graph / kernels.
+    cudaStreamSynchronize(stream);  // the pinned block may still be in use by a previous copy
+    memcpy(st->h_params, &hp, sizeof hp);
+    WF_CK(cudaMemcpyAsync(st->params, st->h_params, sizeof hp, cudaMemcpyHostToDevice, stream), "params copy");
+    int kernels_per_window = n_batches * (3 * (depth + 1) + 3);
+    if (use_graph) {
+        char key[256];
+        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p", (int)sizeof(R), w, h, batch_spp, n_batches, depth,
+                 (const void *)S.nodes);
+        if (!st->exec || st->key != key) {
+            if (st->exec) cudaGraphExecDestroy(st->exec);
+            st->exec = nullptr;
+            if (!st->cap_stream) WF_CK(cudaStreamCreateWithFlags(&st->cap_stream, cudaStreamNonBlocking), "stream");
+            WF_CK(cudaStreamBeginCapture(st->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            int erc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, st->cap_stream, false, block);
+            cudaGraph_t graph = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(st->cap_stream, &graph);
+            if (erc) {
+                if (graph) cudaGraphDestroy(graph);
+                return erc;
+            }
+            WF_CK(ce, "end capture");
+            cudaError_t ie = cudaGraphInstantiate(&st->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            WF_CK(ie, "graph instantiate");
+            st->key = key;
+        }
+        WF_CK(cudaGraphLaunch(st->exec, stream), "graph launch");
+    } else {
+        rc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, stream, prof, block);
+        if (rc) return rc;
+    }
+    if (ev1) WF_CK(cudaEventRecord(ev1, stream), "cudaEventRecord");
+    if (launches) *launches = kernels_per_window;
+    return 0;
+}
+
+}  // namespace mt
