@@ -250,6 +250,24 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
 
     std::vector<float4> nodes(fb.nodes.size() / 4);
     if (!fb.nodes.empty()) memcpy(nodes.data(), fb.nodes.data(), fb.nodes.size() * sizeof(float));
+    // Leaves whose primitives are all triangles point straight at their
+    // (consecutive) triangle slots, skipping the reference indirection.
+    std::vector<int> tri_prim(ntri > 0 ? ntri : 1, 0);
+    for (size_t k = 0; k < refs.size(); ++k)
+        if ((refs[k].y >> 28) == KIND_TRIANGLE) tri_prim[refs[k].y & 0x0FFFFFFF] = refs[k].x;
+    for (size_t i = 0; i < nodes.size() / 4; ++i) {
+        int *q3 = reinterpret_cast<int *>(&nodes[4 * i + 3]);
+        for (int side = 0; side < 2; ++side) {
+            int c = q3[side];
+            if (c >= 0) continue;
+            int leaf = ~c;
+            int first = leaf >> 4, count = leaf & 7;
+            if (count == 0) continue;
+            bool all_tri = true;
+            for (int j = 0; j < count; ++j) all_tri = all_tri && (refs[first + j].y >> 28) == KIND_TRIANGLE;
+            if (all_tri) q3[side] = ~(((refs[first].y & 0x0FFFFFFF) << 4) | (1 << 3) | count);
+        }
+    }
 
     int rc = 0;
     if ((rc = sc->upload(nodes, &S->nodes))) return rc;
@@ -258,6 +276,8 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     if ((rc = sc->upload(tris, &S->tris))) return rc;
     if ((rc = sc->upload(tri_normals, &S->tri_normals))) return rc;
     if ((rc = sc->upload(tri_smooth, &S->tri_smooth))) return rc;
+    if (sizeof(R) == 8 && ntri > 0)
+        if ((rc = sc->upload(tri_prim, &S->tri_prim))) return rc;
     if ((rc = sc->upload(spheres, &S->spheres))) return rc;
     if ((rc = sc->upload(boxes, &S->boxes))) return rc;
     if ((rc = sc->upload(cyls, &S->cyls))) return rc;
@@ -267,6 +287,7 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     if ((rc = sc->upload(mats, &S->materials))) return rc;
 
     S->node_count = fb.node_count;
+    S->stack_depth = fb.depth + 1;  // pushes happen only on the way down
     S->plane_count = (int)plane_prims.size();
     S->prim_count = n;
     S->material_count = d->material_count;
@@ -507,9 +528,11 @@ int mt_scene_create(const mt_scene_desc *desc, const mt_options *opts, mt_scene 
 
     build_bvh(desc->prims, desc->prim_count, &sc->bvh);
     flatten_bvh(sc->bvh, &sc->flat);
-    if (sc->flat.depth + 2 > kStackSize)
+    if (sc->flat.depth + 1 > kStackSize)
         return bail(fail(MT_ERR_UNSUPPORTED, "BVH depth %d exceeds the traversal stack (%d)", sc->flat.depth,
                          kStackSize));
+    if (sc->flat.ref_prim.size() >= (size_t(1) << 26))
+        return bail(fail(MT_ERR_UNSUPPORTED, "more than 2^26 tree primitives"));
 
     void *p = nullptr;
     e = cudaMalloc(&p, sizeof(unsigned));

@@ -278,7 +278,9 @@ struct Flattener {
     {
         if (count <= 7) {
             if (depth > max_depth) max_depth = depth;
-            return ~((first << 3) | count);
+            // ~((first << 4) | (tri_only << 3) | count); the triangle-only
+            // flag is set at upload time, when primitive kinds are known.
+            return ~((first << 4) | count);
         }
         int node = alloc_node();
         if (depth + 1 > max_depth) max_depth = depth + 1;

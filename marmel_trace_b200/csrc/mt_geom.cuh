@@ -459,20 +459,51 @@ MT_D void node_test(const float4 q0, const float4 q1, const float4 q2, const Ray
     *tr = renter < tmin ? tmin : renter;
 }
 
+// ------------------------------------------------------------------
+// BVH traversal.
+//
+// Each thread keeps its traversal stack in dynamic shared memory: entry k of
+// thread t lives at mt_stack_smem[k * blockDim.x + t], so the 32 lanes of a
+// warp touch 32 different banks. Every kernel that traverses launches with
+// S.stack_depth * blockDim.x * 4 bytes of dynamic shared memory; the stack
+// depth is the flattened tree's depth + 1, which bounds the stack by
+// construction (a push only happens on the way down).
+//
+// Loop shape ("while-while", Aila and Laine, "Understanding the Efficiency of
+// Ray Traversal on GPUs", HPG 2009): descend through inner nodes keeping the
+// nearer child in a register and pushing the farther one, until the walk
+// reaches a leaf; then test the leaf's primitives; then pop.
+// ------------------------------------------------------------------
+extern __shared__ int mt_stack_smem[];
+
+static constexpr int kEmpty = (int)0x80000000;  // INT_MIN: no node
+
+// Child code of a leaf: ~((first << 4) | (tri_only << 3) | count), count <= 7.
+// For a triangle-only leaf `first` is the first triangle slot (the slots of
+// one leaf are consecutive); otherwise it indexes the primitive references.
+MT_HD int leaf_code(int first, int tri_only, int count) { return ~((first << 4) | (tri_only << 3) | count); }
+
+template <typename R> MT_D int tri_prim_index(const DevScene<R> &S, int slot);
+template <> MT_D int tri_prim_index<float>(const DevScene<float> &S, int slot)
+{
+    return __float_as_int(__ldg(&S.tri4[3 * (size_t)slot].w));
+}
+template <> MT_D int tri_prim_index<double>(const DevScene<double> &S, int slot) { return __ldg(S.tri_prim + slot); }
+
 MT_D void count_add(unsigned long long *p, unsigned long long v)
 {
     if (v) atomicAdd(p, v);
 }
 
-// ------------------------------------------------------------------
-// Nearest hit in [tmin, tmax] with the reference's tie-break: equal t goes
-// to the LOWEST prim_index (bvh_intersect, src/bvh.c:557-712), planes first
-// (src/bvh.c:579-591). Front-to-back order with a per-ray stack of
-// (child, entry distance); a popped entry farther than the running closest
-// hit is culled with the reference's strict `>` (src/bvh.c:631).
-// ------------------------------------------------------------------
-template <typename R>
-MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best)
+// Nearest hit (ANY = false) or any hit (ANY = true) in [tmin, tmax].
+// Nearest hit keeps the reference's semantics exactly: planes first
+// (src/bvh.c:579-591), then the tree; each primitive is tested against
+// [tmin, closest] and an equal t goes to the LOWEST prim_index
+// (src/bvh.c:641-646). Node order and culling only change the amount of
+// work, never the result. Any hit is bvh_occluded's boolean
+// (src/bvh.c:714-813); the last-occluder cache there only reorders tests.
+template <typename R, bool ANY>
+MT_D bool traverse(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best)
 {
     bool found = false;
     R closest = tmax;
@@ -483,6 +514,10 @@ MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tma
         ++ntest;
         if (plane_t(S.planes + 6 * (size_t)i, rp.o, rp.d, tmin, closest, &t)) {
             int pi = S.plane_prims[i];
+            if (ANY) {
+                found = true;
+                break;
+            }
             if (!found || t < best->t || (t == best->t && pi < best->prim)) {
                 best->t = t;
                 best->u = R(0);
@@ -495,53 +530,83 @@ MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tma
         }
     }
 
-    if (S.node_count > 0) {
-        int stk_node[kStackSize];
-        R stk_t[kStackSize];
+    if (S.node_count > 0 && !(ANY && found)) {
+        int *stk = mt_stack_smem + threadIdx.x;
+        const int stride = blockDim.x;
+        const int cap = S.stack_depth;
         int sp = 0;
-        stk_node[sp] = 0;
-        stk_t[sp] = tmin;
-        ++sp;
-        while (sp > 0) {
-            --sp;
-            int node = stk_node[sp];
-            R te = stk_t[sp];
-            if (found && te > closest) continue;
-            if (node >= 0) {
-                const float4 *N = S.nodes + 4 * (size_t)node;
-                float4 q0 = __ldg(N), q1 = __ldg(N + 1), q2 = __ldg(N + 2);
-                int4 q3 = __ldg(reinterpret_cast<const int4 *>(N + 3));
+        int node = 0;
+        bool done = false;
+        while (!done) {
+            // ---- descend through inner nodes ----
+            while (node >= 0) {
+                const float4 *Nd = S.nodes + 4 * (size_t)node;
+                float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
+                int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
                 bool hl, hr;
                 R tl, tr;
                 ++nvis;
                 node_test(q0, q1, q2, rp, tmin, closest, &hl, &hr, &tl, &tr);
-                int cl = q3.x, cr = q3.y;
-                if (sp + 2 > kStackSize) {
-                    atomicOr(S.err, ERR_STACK);
-                    break;
-                }
                 if (hl && hr) {
-                    if (tl <= tr) {
-                        stk_node[sp] = cr; stk_t[sp] = tr; ++sp;
-                        stk_node[sp] = cl; stk_t[sp] = tl; ++sp;
-                    } else {
-                        stk_node[sp] = cl; stk_t[sp] = tl; ++sp;
-                        stk_node[sp] = cr; stk_t[sp] = tr; ++sp;
+                    bool lnear = tl <= tr;
+                    int nearc = lnear ? q3.x : q3.y;
+                    int farc = lnear ? q3.y : q3.x;
+                    if (sp >= cap) {
+                        atomicOr(S.err, ERR_STACK);
+                        done = true;
+                        node = kEmpty;
+                        break;
                     }
+                    stk[sp * stride] = farc;
+                    ++sp;
+                    node = nearc;
                 } else if (hl) {
-                    stk_node[sp] = cl; stk_t[sp] = tl; ++sp;
+                    node = q3.x;
                 } else if (hr) {
-                    stk_node[sp] = cr; stk_t[sp] = tr; ++sp;
+                    node = q3.y;
+                } else {
+                    node = sp > 0 ? stk[--sp * stride] : kEmpty;
+                }
+            }
+            if (node == kEmpty) break;
+            // ---- leaf ----
+            int leaf = ~node;
+            int first = leaf >> 4, count = leaf & 7;
+            if ((leaf >> 3) & 1) {
+                for (int i = 0; i < count; ++i) {
+                    R t, u, v;
+                    ++ntest;
+                    ++ntri;
+                    if (tri_t(S, first + i, rp, tmin, closest, &t, &u, &v)) {
+                        if (ANY) {
+                            found = true;
+                            break;
+                        }
+                        int pi = tri_prim_index(S, first + i);
+                        if (!found || t < best->t || (t == best->t && pi < best->prim)) {
+                            best->t = t;
+                            best->u = u;
+                            best->v = v;
+                            best->prim = pi;
+                            best->code = (KIND_TRIANGLE << 28) | (first + i);
+                            closest = t;
+                            found = true;
+                        }
+                    }
                 }
             } else {
-                int leaf = ~node;
-                int first = leaf >> 3, count = leaf & 7;
                 for (int i = 0; i < count; ++i) {
                     int2 ref = __ldg(S.refs + first + i);
                     R t, u, v;
                     ++ntest;
                     ntri += (ref.y >> 28) == KIND_TRIANGLE;
-                    if (prim_hit_t(S, ref.y, rp, tmin, closest, &t, &u, &v)) {
+                    bool hit = ANY ? prim_occluded(S, ref.y, rp, tmin, tmax)
+                                   : prim_hit_t(S, ref.y, rp, tmin, closest, &t, &u, &v);
+                    if (hit) {
+                        if (ANY) {
+                            found = true;
+                            break;
+                        }
                         if (!found || t < best->t || (t == best->t && ref.x < best->prim)) {
                             best->t = t;
                             best->u = u;
@@ -554,80 +619,35 @@ MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tma
                     }
                 }
             }
+            if (ANY && found) break;
+            node = sp > 0 ? stk[--sp * stride] : kEmpty;
+            if (node == kEmpty) break;
         }
     }
     if (S.counters) {
-        count_add(&S.counters->node_visits, nvis);
-        count_add(&S.counters->prim_tests, ntest);
-        count_add(&S.counters->tri_tests, ntri);
+        if (ANY) {
+            count_add(&S.counters->any_node_visits, nvis);
+            count_add(&S.counters->any_prim_tests, ntest);
+            count_add(&S.counters->any_tri_tests, ntri);
+        } else {
+            count_add(&S.counters->node_visits, nvis);
+            count_add(&S.counters->prim_tests, ntest);
+            count_add(&S.counters->tri_tests, ntri);
+        }
     }
     return found;
 }
 
-// Any hit in [tmin, tmax] (bvh_occluded src/bvh.c:714-813 with the
-// primitive_occluded tests). The reference's last-occluder cache only
-// reorders the tests, so it is not needed for the same boolean.
+template <typename R>
+MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best)
+{
+    return traverse<R, false>(S, rp, tmin, tmax, best);
+}
+
 template <typename R> MT_D bool scene_any(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax)
 {
-    unsigned long long nvis = 0, ntest = 0, ntri = 0;
-    bool hit = false;
-    for (int i = 0; i < S.plane_count && !hit; ++i) {
-        R t;
-        ++ntest;
-        if (plane_t(S.planes + 6 * (size_t)i, rp.o, rp.d, tmin, tmax, &t)) hit = true;
-    }
-    if (!hit && S.node_count > 0) {
-        int stk[kStackSize];
-        int sp = 0;
-        stk[sp++] = 0;
-        while (sp > 0 && !hit) {
-            int node = stk[--sp];
-            if (node >= 0) {
-                const float4 *N = S.nodes + 4 * (size_t)node;
-                float4 q0 = __ldg(N), q1 = __ldg(N + 1), q2 = __ldg(N + 2);
-                int4 q3 = __ldg(reinterpret_cast<const int4 *>(N + 3));
-                bool hl, hr;
-                R tl, tr;
-                ++nvis;
-                node_test(q0, q1, q2, rp, tmin, tmax, &hl, &hr, &tl, &tr);
-                if (sp + 2 > kStackSize) {
-                    atomicOr(S.err, ERR_STACK);
-                    break;
-                }
-                if (hl && hr) {
-                    if (tl <= tr) {
-                        stk[sp++] = q3.y;
-                        stk[sp++] = q3.x;
-                    } else {
-                        stk[sp++] = q3.x;
-                        stk[sp++] = q3.y;
-                    }
-                } else if (hl) {
-                    stk[sp++] = q3.x;
-                } else if (hr) {
-                    stk[sp++] = q3.y;
-                }
-            } else {
-                int leaf = ~node;
-                int first = leaf >> 3, count = leaf & 7;
-                for (int i = 0; i < count; ++i) {
-                    int2 ref = __ldg(S.refs + first + i);
-                    ++ntest;
-                    ntri += (ref.y >> 28) == KIND_TRIANGLE;
-                    if (prim_occluded(S, ref.y, rp, tmin, tmax)) {
-                        hit = true;
-                        break;
-                    }
-                }
-            }
-        }
-    }
-    if (S.counters) {
-        count_add(&S.counters->any_node_visits, nvis);
-        count_add(&S.counters->any_prim_tests, ntest);
-        count_add(&S.counters->any_tri_tests, ntri);
-    }
-    return hit;
+    Hit<R> dummy;
+    return traverse<R, true>(S, rp, tmin, tmax, &dummy);
 }
 
 // scene_intersect / scene_occluded entry semantics: a direction that is not

@@ -135,6 +135,12 @@ __global__ void k_primary(const DevScene<R> S, const DevCamera<R> cam, int w, in
 
 static inline int grid_for(long long n, int block) { return (int)((n + block - 1) / block); }
 
+// Dynamic shared memory of a traversing kernel: one stack per thread.
+template <typename R> static inline size_t stack_smem(const DevScene<R> &S, int block)
+{
+    return (size_t)(S.stack_depth > 0 ? S.stack_depth : 1) * block * sizeof(int);
+}
+
 template <typename R>
 cudaError_t launch_render(const DevScene<R> &S, const DevCamera<R> &cam, int w, int h, int spp_total, int s0,
                           int s1, int depth, int mode, int out_kind, void *out, int block, cudaStream_t stream)
@@ -143,10 +149,10 @@ cudaError_t launch_render(const DevScene<R> &S, const DevCamera<R> &cam, int w, 
     if (block > 128) block = 128;  // __launch_bounds__(128)
     long long n = (long long)w * h;
     if (mode == RENDER_PT)
-        k_render<R, RENDER_PT><<<grid_for(n, block), block, 0, stream>>>(S, cam, w, h, spp_total, s0, s1, depth,
+        k_render<R, RENDER_PT><<<grid_for(n, block), block, stack_smem(S, block), stream>>>(S, cam, w, h, spp_total, s0, s1, depth,
                                                                          out_kind, out);
     else
-        k_render<R, RENDER_WHITTED><<<grid_for(n, block), block, 0, stream>>>(S, cam, w, h, spp_total, s0, s1,
+        k_render<R, RENDER_WHITTED><<<grid_for(n, block), block, stack_smem(S, block), stream>>>(S, cam, w, h, spp_total, s0, s1,
                                                                               depth, out_kind, out);
     return cudaGetLastError();
 }
@@ -155,7 +161,7 @@ template <typename R>
 cudaError_t launch_intersect(const DevScene<R> &S, int n, const double *o, const double *d, double tmin, double tmax,
                              int *prim, double *t, double *normal, int *front, int *mat, cudaStream_t stream)
 {
-    k_intersect<R><<<grid_for(n, 128), 128, 0, stream>>>(S, n, o, d, tmin, tmax, prim, t, normal, front, mat);
+    k_intersect<R><<<grid_for(n, 128), 128, stack_smem(S, 128), stream>>>(S, n, o, d, tmin, tmax, prim, t, normal, front, mat);
     return cudaGetLastError();
 }
 
@@ -163,7 +169,7 @@ template <typename R>
 cudaError_t launch_occluded(const DevScene<R> &S, int n, const double *o, const double *d, double tmin, double tmax,
                             int *occ, cudaStream_t stream)
 {
-    k_occluded<R><<<grid_for(n, 128), 128, 0, stream>>>(S, n, o, d, tmin, tmax, occ);
+    k_occluded<R><<<grid_for(n, 128), 128, stack_smem(S, 128), stream>>>(S, n, o, d, tmin, tmax, occ);
     return cudaGetLastError();
 }
 
@@ -171,7 +177,7 @@ template <typename R>
 cudaError_t launch_radiance(const DevScene<R> &S, int n, const double *o, const double *d, int depth,
                             const unsigned *seeds, double *out, int mode, cudaStream_t stream)
 {
-    k_radiance<R><<<grid_for(n, 64), 64, 0, stream>>>(S, n, o, d, depth, seeds, out, mode);
+    k_radiance<R><<<grid_for(n, 64), 64, stack_smem(S, 64), stream>>>(S, n, o, d, depth, seeds, out, mode);
     return cudaGetLastError();
 }
 

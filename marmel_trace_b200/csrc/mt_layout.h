@@ -124,6 +124,7 @@ template <typename R> struct DevScene {
     const R *cyls;
     const R *planes;         // point, axis
     const int *plane_prims;  // prim_index of each plane
+    const int *tri_prim;     // prim_index of each triangle slot (FP64 path)
     const int2 *prim_info;   // {code, material} per prim_index
     const DevMaterial<R> *materials;
     int node_count;
@@ -133,6 +134,7 @@ template <typename R> struct DevScene {
     int light_count;
     int water_material;
     int has_passthrough;   // some material lets shadow rays through (water, transparency > 0.8)
+    int stack_depth;       // traversal stack entries per thread (dynamic shared memory)
     R water_level;
     DevOcean<R> ocean;
     DevSky<R> sky;

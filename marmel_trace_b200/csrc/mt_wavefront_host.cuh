@@ -118,6 +118,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
     const WfParams<R> *P = (const WfParams<R> *)st->params;
     WfCounters *C = st->counters;
     const int g = st->grid;
+    const size_t smem = (size_t)(S.stack_depth > 0 ? S.stack_depth : 1) * block * sizeof(int);
     int ev = 0;
     auto tic = [&]() {
         if (prof) cudaEventRecord(st->kev[ev & 63], s);
@@ -140,7 +141,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         int which = 0;
         for (int b = 0; b <= depth; ++b) {
             tic();
-            k_wf_extend<R><<<g, block, 0, s>>>(S, rays[which], C, which, hits);
+            k_wf_extend<R><<<g, block, smem, s>>>(S, rays[which], C, which, hits);
             toc(0);
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
             WF_CK(cudaMemsetAsync(&C->shadow_count, 0, sizeof(int), s), "memset(shadow_count)");
@@ -149,7 +150,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
                                               sq);
             toc(1);
             tic();
-            k_wf_shadow<R><<<g, block, 0, s>>>(S, sq, C, nee);
+            k_wf_shadow<R><<<g, block, smem, s>>>(S, sq, C, nee);
             toc(2);
             which ^= 1;
         }
@@ -187,7 +188,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_extend<R>, block, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_extend<R>, block,
+                                                      (size_t)(S.stack_depth > 0 ? S.stack_depth : 1) * block * 4);
         if (per_sm < 1) per_sm = 1;
         st->grid = sms * per_sm;
     }
