@@ -293,6 +293,28 @@ int mt_render_accumulate_device(mt_scene *scene, const mt_camera *cam, int width
                                 int spp_begin, int spp_end, int max_depth, int mode,
                                 float *accum_dev, int accumulate, void *stream);
 
+/*
+ * Same result as mt_render_accumulate_device with the path tracer (the same
+ * wavefront stage kernels and random streams), for callers that cannot
+ * allocate device memory while they render: for example an application whose
+ * own pool allocator owns the whole device budget, or a render loop that must
+ * not pay the device-wide synchronisation of cudaMalloc / cudaFree. This
+ * entry point has no counterpart in the reference.
+ *
+ * It allocates nothing. Its queues and path state live in one fixed 12 MiB
+ * __device__ array inside the library, which every GPU that loads the library
+ * holds until the process exits. Limits: width * height <= 16384 pixels per
+ * call (MT_ERR_INVALID beyond), FP32 scenes only (MT_ERR_UNSUPPORTED). The
+ * caller passes the scene, the camera and the device output buffer
+ * `accum_dev` (width * height * 3 floats). The first call on a device looks
+ * up the array's device address; make it before capturing any stream. All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.
+ */
+int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_camera *cam, int width, int height,
+                                        int spp_begin, int spp_end, int max_depth, float *accum_dev,
+                                        int accumulate, void *stream);
+
 /* Per-launch statistics of the last render on this scene. */
 typedef struct {
     double  kernel_ms;        /* device time of the render kernels (CUDA events) */

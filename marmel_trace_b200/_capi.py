@@ -200,6 +200,7 @@ SIGNATURES = {
     "mt_render_image_ex": (I, [P, P, I, I, P, P]),
     "mt_render_linear": (I, [P, P, I, I, I, I, I, P]),
     "mt_render_accumulate_device": (I, [P, P, I, I, I, I, I, I, P, I, P]),
+    "mt_render_accumulate_device_noalloc": (I, [P, P, I, I, I, I, I, P, I, P]),
     "mt_get_stats": (I, [P, P]),
     "mt_set_counting": (I, [P, I]),
     "mt_pathtrace_radiance": (I, [P, I, P, P, I, P, P]),

@@ -34,6 +34,7 @@ UNITS = [
     ("mt_kernels_f64.cu", ["--fmad=false"]),
     ("mt_wavefront.cu", []),
     ("mt_wavefront_f64.cu", ["--fmad=false"]),
+    ("mt_noalloc.cu", []),
     ("mt_bvh.cpp", []),
 ]
 

@@ -876,3 +876,9 @@ int mt_primary_rays(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, i
 }
 
 }  // extern "C"
+
+// Accessors for entry points defined in other translation units.
+const mt::DevScene<float> *mt_scene_dev_f32(const mt_scene *sc) { return &sc->sf; }
+int mt_scene_precision(const mt_scene *sc) { return sc->opts.precision; }
+int mt_scene_device(const mt_scene *sc) { return sc->opts.device; }
+void mt_set_last_error_text(const char *msg) { g_last_error = msg; }
