@@ -376,6 +376,40 @@ int mt_occluded(mt_scene *scene, int n, const double *origins, const double *dir
 int mt_primary_rays(mt_scene *scene, const mt_camera *cam, int width, int height, int spp,
                     int mode, double *rays_out);
 
+/* ------------------------------------------------------------------ */
+/* Differentiable rendering: path-replay adjoint                        */
+/* ------------------------------------------------------------------ */
+
+/*
+ * Differentiable parameters, flat: for each material m, albedo rgb at 8m+0..2,
+ * roughness 8m+3, metallic 8m+4, emissive rgb 8m+5..7; then the sun radiance
+ * (sky sun_color) rgb at 8M+0..2. mt_scene_param_count returns 8M + 3.
+ * Setting parameters updates the device materials and sun and re-collects the
+ * emissive light list (scene_collect_emissive_lights, src/scene.c:1384-1426).
+ */
+int mt_scene_param_count(const mt_scene *scene);
+int mt_scene_get_material_params(const mt_scene *scene, double *params, int n);
+int mt_scene_set_material_params(mt_scene *scene, const double *params, int n);
+
+/*
+ * Backward of the path-traced linear image I = mt_render_linear(...) with
+ * respect to the parameters above, by path replay: each path is traced, then
+ * replayed from its own random stream to accumulate
+ *     grad[i] = sum_pixels dL_dimage[pixel] . dI[pixel] / dparam[i]
+ * with detached sampling (directions, lobe and roulette probabilities held
+ * fixed); geometry and visibility derivatives are out of scope. This is the
+ * backward half of a torch.autograd.Function whose forward is mt_render_linear.
+ * Host buffers: dL_dimage (w*h*3 floats), grad (n doubles).
+ */
+int mt_adjoint_backward(mt_scene *scene, const mt_camera *cam, int width, int height, int samples_per_pixel,
+                        int max_depth, const float *dL_dimage, double *grad, int n);
+
+/* Device-buffer form over the sample window [spp_begin, spp_end), asynchronous
+ * on `stream`; grad_dev is overwritten (accumulate = 0) or added to. */
+int mt_adjoint_backward_device(mt_scene *scene, const mt_camera *cam, int width, int height, int spp_begin,
+                               int spp_end, int max_depth, const float *dL_dimage_dev, double *grad_dev,
+                               int accumulate, void *stream);
+
 /* Library version and last error text (thread-local, never NULL). */
 const char *mt_version(void);
 const char *mt_last_error(void);

@@ -208,6 +208,11 @@ SIGNATURES = {
     "mt_intersect": (I, [P, I, P, P, D, D, P, P, P, P, P]),
     "mt_occluded": (I, [P, I, P, P, D, D, P]),
     "mt_primary_rays": (I, [P, P, I, I, I, I, P]),
+    "mt_scene_param_count": (I, [P]),
+    "mt_scene_get_material_params": (I, [P, P, I]),
+    "mt_scene_set_material_params": (I, [P, P, I]),
+    "mt_adjoint_backward": (I, [P, P, I, I, I, I, P, P, I]),
+    "mt_adjoint_backward_device": (I, [P, P, I, I, I, I, I, P, P, I, P]),
     "mt_version": (C.c_char_p, []),
     "mt_last_error": (C.c_char_p, []),
 }

@@ -22,6 +22,10 @@
 
 using namespace mt;
 
+// Adjoint parameter layout (mt_adjoint.cuh): 8 per material, then the sun.
+static constexpr int kParamsPerMaterialApi = 8;
+static constexpr int kAdjMaxMaterialsApi = 256;
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -65,6 +69,13 @@ void normalize3(const double *a, double *o)
     o[2] = a[2] * inv;
 }
 
+struct HostSphere {
+    int prim;
+    int material;
+    double center[3];
+    double radius;
+};
+
 }  // namespace
 
 struct mt_scene {
@@ -84,6 +95,11 @@ struct mt_scene {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     mt_stats stats;
     WavefrontState *wf = nullptr;
+    // host copies used by parameter updates (mt_scene_set_material_params)
+    std::vector<mt_material> h_mats;
+    mt_sky h_sky;
+    std::vector<HostSphere> h_spheres;
+    int version = 0;
 
     template <typename T> int upload(const std::vector<T> &v, const T **dst)
     {
@@ -168,6 +184,31 @@ template <typename R> void fill_sky(const mt_sky &s, DevSky<R> *o)
     o->sun_radius = (R)s.sun_radius;
     o->cloud_octaves = s.cloud_octaves;
     o->seed = s.seed;
+}
+
+// scene_collect_emissive_lights (src/scene.c:1384-1426): the first 8 emissive
+// PBR spheres with radius > 0, in file order, from the host copies.
+template <typename R> void collect_lights(mt_scene *sc, DevScene<R> *S)
+{
+    S->light_count = 0;
+    for (const HostSphere &p : sc->h_spheres) {
+        if (S->light_count >= kMaxLights) break;
+        if (p.material < 0 || p.material >= (int)sc->h_mats.size()) continue;
+        const mt_material &m = sc->h_mats[p.material];
+        if (!m.pbr) continue;
+        if (m.emissive[0] == 0.0 && m.emissive[1] == 0.0 && m.emissive[2] == 0.0) continue;
+        if (!(p.radius > 0.0)) continue;
+        DevLight<R> &L = S->lights[S->light_count];
+        for (int k = 0; k < 3; ++k) {
+            L.center[k] = (R)p.center[k];
+            L.emissive[k] = (R)m.emissive[k];
+        }
+        L.radius = (R)p.radius;
+        L.prim = p.prim;
+        sc->light_prims[S->light_count] = p.prim;
+        S->light_count++;
+    }
+    sc->light_count = S->light_count;
 }
 
 // Upload every array of the scene in arithmetic type R.
@@ -310,30 +351,18 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     S->ocean.chop_wavelength = (R)d->ocean.chop_wavelength;
     fill_sky(d->sky, &S->sky);
 
-    // scene_collect_emissive_lights (src/scene.c:1384-1426): the first 8
-    // emissive PBR spheres with radius > 0, in file order.
-    S->light_count = 0;
-    for (int i = 0; i < n && S->light_count < kMaxLights; ++i) {
-        const mt_prim &p = d->prims[i];
-        if (p.kind != MT_PRIM_SPHERE) continue;
-        if (p.material < 0 || p.material >= d->material_count) continue;
-        const mt_material &m = d->materials[p.material];
-        if (!m.pbr) continue;
-        if (m.emissive[0] == 0.0 && m.emissive[1] == 0.0 && m.emissive[2] == 0.0) continue;
-        if (!(p.v[3] > 0.0)) continue;
-        DevLight<R> &L = S->lights[S->light_count];
-        for (int k = 0; k < 3; ++k) {
-            L.center[k] = (R)p.v[k];
-            L.emissive[k] = (R)m.emissive[k];
-        }
-        L.radius = (R)p.v[3];
-        L.prim = i;
-        sc->light_prims[S->light_count] = i;
-        S->light_count++;
-    }
-    sc->light_count = S->light_count;
+    // host copies for parameter updates (materials, sun, sphere list)
+    sc->h_mats.assign(d->materials, d->materials + d->material_count);
+    sc->h_sky = d->sky;
+    sc->h_spheres.clear();
+    for (int i = 0; i < n; ++i)
+        if (d->prims[i].kind == MT_PRIM_SPHERE)
+            sc->h_spheres.push_back({i, d->prims[i].material, {d->prims[i].v[0], d->prims[i].v[1], d->prims[i].v[2]},
+                                     d->prims[i].v[3]});
+    collect_lights(sc, S);
     S->err = sc->d_err;
     S->counters = nullptr;
+    S->version = 0;
     return 0;
 }
 
@@ -873,6 +902,130 @@ int mt_primary_rays(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, i
     CK(cudaDeviceSynchronize(), "primary kernel");
     CK(cudaMemcpy(out, dR.p, 6 * n * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
     return 0;
+}
+
+int mt_scene_param_count(const mt_scene *sc)
+{
+    if (!sc) return -fail(MT_ERR_NULL, "NULL pointer");
+    return kParamsPerMaterialApi * (int)sc->h_mats.size() + 3;
+}
+
+int mt_scene_get_material_params(const mt_scene *sc, double *params, int n)
+{
+    if (!sc || !params) return fail(MT_ERR_NULL, "NULL pointer");
+    const int M = (int)sc->h_mats.size();
+    if (n != kParamsPerMaterialApi * M + 3) return fail(MT_ERR_INVALID, "expected %d parameters, got %d",
+                                                        kParamsPerMaterialApi * M + 3, n);
+    for (int m = 0; m < M; ++m) {
+        const mt_material &mt = sc->h_mats[m];
+        double *p = params + kParamsPerMaterialApi * m;
+        for (int k = 0; k < 3; ++k) {
+            p[k] = mt.albedo[k];
+            p[5 + k] = mt.emissive[k];
+        }
+        p[3] = mt.roughness;
+        p[4] = mt.metallic;
+    }
+    for (int k = 0; k < 3; ++k) params[kParamsPerMaterialApi * M + k] = sc->h_sky.sun_color[k];
+    return 0;
+}
+
+}  // extern "C"
+
+namespace {
+template <typename R> int apply_params(mt_scene *sc, DevScene<R> *S)
+{
+    std::vector<DevMaterial<R>> mats(sc->h_mats.size());
+    for (size_t i = 0; i < mats.size(); ++i) fill_material(sc->h_mats[i], &mats[i]);
+    if (!mats.empty())
+        CK(cudaMemcpy((void *)S->materials, mats.data(), mats.size() * sizeof(DevMaterial<R>), cudaMemcpyHostToDevice),
+           "cudaMemcpy(materials)");
+    for (int k = 0; k < 3; ++k) S->sky.sun_color[k] = (R)sc->h_sky.sun_color[k];
+    collect_lights(sc, S);  // a material that gains or loses emission changes the light list
+    S->version = sc->version;
+    return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int mt_scene_set_material_params(mt_scene *sc, const double *params, int n)
+{
+    if (!sc || !params) return fail(MT_ERR_NULL, "NULL pointer");
+    const int M = (int)sc->h_mats.size();
+    if (n != kParamsPerMaterialApi * M + 3) return fail(MT_ERR_INVALID, "expected %d parameters, got %d",
+                                                        kParamsPerMaterialApi * M + 3, n);
+    for (int m = 0; m < M; ++m) {
+        mt_material &mt = sc->h_mats[m];
+        const double *p = params + kParamsPerMaterialApi * m;
+        for (int k = 0; k < 3; ++k) {
+            mt.albedo[k] = p[k];
+            mt.emissive[k] = p[5 + k];
+        }
+        mt.roughness = p[3];
+        mt.metallic = p[4];
+    }
+    for (int k = 0; k < 3; ++k) sc->h_sky.sun_color[k] = params[kParamsPerMaterialApi * M + k];
+    sc->version++;
+    int rc = set_device(sc);
+    if (rc) return rc;
+    if (sc->opts.precision == MT_PRECISION_FP64) return apply_params(sc, &sc->sd);
+    return apply_params(sc, &sc->sf);
+}
+
+int mt_adjoint_backward_device(mt_scene *sc, const mt_camera *cam, int w, int h, int s0, int s1, int depth,
+                               const float *dL_dimage_dev, double *grad_dev, int accumulate, void *stream)
+{
+    int rc = render_args(sc, cam, dL_dimage_dev, w, h, s1 - s0, depth);
+    if (rc) return rc;
+    if (!grad_dev) return fail(MT_ERR_NULL, "NULL gradient buffer");
+    if (s0 < 0) return fail(MT_ERR_COUNTS, "negative first sample");
+    const int M = (int)sc->h_mats.size();
+    if (M > kAdjMaxMaterialsApi) return fail(MT_ERR_UNSUPPORTED, "the adjoint supports at most %d materials",
+                                             kAdjMaxMaterialsApi);
+    if ((rc = set_device(sc))) return rc;
+    const int np = kParamsPerMaterialApi * M + 3;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!accumulate) CK(cudaMemsetAsync(grad_dev, 0, np * sizeof(double), s), "cudaMemsetAsync(grad)");
+    const double scale = 1.0 / (double)(s1 - s0);
+    if (sc->opts.precision == MT_PRECISION_FP64) {
+        DevCamera<double> dc;
+        fill_camera(cam, &dc);
+        CK(launch_adjoint<double>(sc->sd, dc, w, h, s0, s1, depth, dL_dimage_dev, scale, grad_dev, np, s),
+           "adjoint launch");
+    } else {
+        DevCamera<float> dc;
+        fill_camera(cam, &dc);
+        CK(launch_adjoint<float>(sc->sf, dc, w, h, s0, s1, depth, dL_dimage_dev, scale, grad_dev, np, s),
+           "adjoint launch");
+    }
+    return 0;
+}
+
+int mt_adjoint_backward(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, int depth, const float *dL_dimage,
+                        double *grad, int n)
+{
+    int rc = render_args(sc, cam, dL_dimage, w, h, spp, depth);
+    if (rc) return rc;
+    if (!grad) return fail(MT_ERR_NULL, "NULL gradient buffer");
+    const int np = kParamsPerMaterialApi * (int)sc->h_mats.size() + 3;
+    if (n != np) return fail(MT_ERR_INVALID, "expected %d parameters, got %d", np, n);
+    if ((rc = set_device(sc))) return rc;
+    DevBuf<float> dA;
+    DevBuf<double> dG;
+    size_t npix = (size_t)w * h * 3;
+    CK(dA.alloc(npix), "cudaMalloc");
+    CK(dG.alloc((size_t)np), "cudaMalloc");
+    CK(cudaMemcpy(dA.p, dL_dimage, npix * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
+    CK(cudaEventRecord(sc->ev0, 0), "cudaEventRecord");
+    if ((rc = mt_adjoint_backward_device(sc, cam, w, h, 0, spp, depth, dA.p, dG.p, 0, nullptr))) return rc;
+    CK(cudaEventRecord(sc->ev1, 0), "cudaEventRecord");
+    CK(cudaDeviceSynchronize(), "adjoint kernel");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
+    sc->stats.kernel_ms = ms;
+    CK(cudaMemcpy(grad, dG.p, np * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return check_err_word(sc);
 }
 
 }  // extern "C"

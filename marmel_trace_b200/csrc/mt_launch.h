@@ -42,7 +42,10 @@ template <typename R>
 cudaError_t launch_primary(const DevScene<R> &S, const DevCamera<R> &cam, int w, int h, int spp, int mode,
                            double *out, cudaStream_t stream);
 
-// Name of the render kernel (for profiles) and its register footprint.
-template <typename R> const char *render_kernel_name(int mode);
+// Path-replay adjoint over samples [s0, s1): grad += adj_scale * sum over
+// pixels and samples of adj_img[pixel] . dL_sample/dtheta (mt_adjoint.cuh).
+template <typename R>
+cudaError_t launch_adjoint(const DevScene<R> &S, const DevCamera<R> &cam, int w, int h, int s0, int s1, int depth,
+                           const float *adj_img, double adj_scale, double *grad, int n_params, cudaStream_t stream);
 
 }  // namespace mt

@@ -135,6 +135,7 @@ template <typename R> struct DevScene {
     int water_material;
     int has_passthrough;   // some material lets shadow rays through (water, transparency > 0.8)
     int stack_depth;       // traversal stack entries per thread (dynamic shared memory)
+    int version;           // bumped whenever material / sun parameters change
     R water_level;
     DevOcean<R> ocean;
     DevSky<R> sky;

@@ -218,8 +218,10 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     int kernels_per_window = n_batches * (3 * (depth + 1) + 3);
     if (use_graph) {
         char key[256];
-        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p", (int)sizeof(R), w, h, batch_spp, n_batches, depth,
-                 (const void *)S.nodes);
+        // the scene travels by value in the captured kernel parameters, so
+        // its identity, counters and parameter version are part of the key
+        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d", (int)sizeof(R), w, h, batch_spp, n_batches, depth,
+                 (const void *)S.nodes, (const void *)S.counters, S.version);
         if (!st->exec || st->key != key) {
             if (st->exec) cudaGraphExecDestroy(st->exec);
             st->exec = nullptr;

@@ -180,6 +180,60 @@ def torus_field_scene(seed: int = 2, n_instances: int = 4096, n_materials: int =
 
 
 # ---------------------------------------------------------------------
+# C4: inverse-rendering scene, 128 spheres + plane sharing 32 PBR materials
+# ---------------------------------------------------------------------
+PARAMS_PER_MATERIAL = 8  # albedo rgb, roughness, metallic, emissive rgb
+
+
+def adjoint_scene(seed: int = 4, n_spheres: int = 128, n_materials: int = 32, n_emissive: int = 4) -> SceneDesc:
+    """Spheres and a ground plane sharing `n_materials` PBR materials with the
+    hidden true parameters of the inverse-rendering configuration: albedo
+    U(0.1, 0.9)^3, roughness U(0.05, 0.8), metallic U(0, 1), emissive 0 except
+    for `n_emissive` materials with emissive U(1, 10)^3."""
+    rng = np.random.default_rng(seed)
+    mats = []
+    emissive_ids = set(rng.choice(n_materials, n_emissive, replace=False).tolist())
+    for i in range(n_materials):
+        em = tuple(rng.uniform(1.0, 10.0, 3)) if i in emissive_ids else (0.0, 0.0, 0.0)
+        mats.append(material(albedo=tuple(rng.uniform(0.1, 0.9, 3)), roughness=float(rng.uniform(0.05, 0.8)),
+                             metallic=float(rng.uniform(0.0, 1.0)), emissive=em, pbr=1))
+    centers = np.stack([rng.uniform(-10, 10, n_spheres), rng.uniform(0.2, 2.5, n_spheres),
+                        rng.uniform(-10, 10, n_spheres)], axis=1)
+    radii = rng.uniform(0.2, 0.9, n_spheres)
+    mat_of = rng.integers(0, n_materials, n_spheres)
+    prims = prims_array(1 + n_spheres)
+    set_plane(prims[0], (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), int(rng.integers(0, n_materials)))
+    for i in range(n_spheres):
+        set_sphere(prims[1 + i], centers[i], radii[i], int(mat_of[i]))
+    return SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=default_sky(),
+                     camera=dict(eye=(0.0, 6.0, -18.0), target=(0.0, 0.5, 0.0), up=(0.0, 1.0, 0.0), vfov=50.0))
+
+
+def material_params(desc: SceneDesc) -> np.ndarray:
+    """Flat parameter vector of the adjoint: per material albedo rgb,
+    roughness, metallic, emissive rgb; then the sun radiance rgb."""
+    m = desc.materials
+    per = np.concatenate([m["albedo"], m["roughness"][:, None], m["metallic"][:, None], m["emissive"]], axis=1)
+    return np.concatenate([per.ravel(), np.asarray(desc.sky["sun_color"], np.float64)])
+
+
+def with_params(desc: SceneDesc, params: np.ndarray) -> SceneDesc:
+    """A copy of `desc` whose materials and sun radiance take `params`."""
+    n = len(desc.materials)
+    p = np.asarray(params, np.float64)
+    per = p[: PARAMS_PER_MATERIAL * n].reshape(n, PARAMS_PER_MATERIAL)
+    mats = desc.materials.copy()
+    mats["albedo"] = per[:, 0:3]
+    mats["roughness"] = per[:, 3]
+    mats["metallic"] = per[:, 4]
+    mats["emissive"] = per[:, 5:8]
+    sky = dict(desc.sky)
+    sky["sun_color"] = tuple(float(x) for x in p[PARAMS_PER_MATERIAL * n: PARAMS_PER_MATERIAL * n + 3])
+    return SceneDesc(prims=desc.prims, materials=mats, sky=sky, water_level=desc.water_level,
+                     water_material=desc.water_material, fog_density=desc.fog_density, camera=desc.camera)
+
+
+# ---------------------------------------------------------------------
 # Reference scene text
 # ---------------------------------------------------------------------
 def _f(x) -> str:
