@@ -251,6 +251,12 @@ def run_ours(args):
         gm.release()
         del fm
 
+    # adjoint (inverse-rendering configuration: 512x512, 32 spp, depth 6,
+    # 128 spheres + plane sharing 32 PBR materials, 259 parameters)
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_bench(torch, local, flush)
+
     # time to RMSE 1e-3
     ttr = None
     if len(means) >= 3:
@@ -304,6 +310,7 @@ def run_ours(args):
         "mrays_per_s": round(value * rays_per_sample, 2),
         "rays_per_sample": round(rays_per_sample, 3),
         "time_to_rmse": ttr,
+        "adjoint": adjoint,
         "stage_ms": stage,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -324,6 +331,43 @@ def run_ours(args):
     g.release()
     if dist:
         dist.destroy_process_group()
+
+
+def adjoint_bench(torch, device: int, flush, steps: int = 3):
+    """Forward + path-replay backward of the inverse-rendering configuration;
+    a gradient is the full 259-parameter vector of an L2 image loss."""
+    from marmel_trace_b200 import scenes
+    from marmel_trace_b200.adjoint import DiffRenderer
+
+    aw, ah, aspp, adepth = 512, 512, 32, 6
+    d = scenes.adjoint_scene()
+    r = DiffRenderer(d, aw, ah, aspp, adepth, precision="fp32", integrator="wavefront", device=device)
+    target = r.render(s0=1_000_000)
+    img = r.render()
+    dl = 2.0 * (img - target)
+    r.backward(dl)  # warm-up
+    torch.cuda.synchronize()
+    fw, bw = [], []
+    stream = torch.cuda.current_stream()
+    for k in range(steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        flush.zero_()
+        e[0].record(stream)
+        img = r.render(s0=aspp * (k + 1))
+        e[1].record(stream)
+        r.backward(2.0 * (img - target), s0=aspp * (k + 1))
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        fw.append(e[0].elapsed_time(e[1]))
+        bw.append(e[1].elapsed_time(e[2]))
+    r.release()
+    b = statistics.median(bw) / 1e3
+    f = statistics.median(fw) / 1e3
+    return {"workload": "inverse rendering 512x512, 32 spp, depth 6, 128 spheres + plane, 32 PBR materials (seed 4)",
+            "params": r.n_params, "grads_per_s": round(1.0 / b, 3), "backward_ms": round(1e3 * b, 2),
+            "forward_ms": round(1e3 * f, 2), "backward_msamples_s": round(aw * ah * aspp / b / 1e6, 2),
+            "forward_msamples_s": round(aw * ah * aspp / f / 1e6, 2),
+            "method": "path replay: each sample traced then replayed from its random stream (megakernel form)"}
 
 
 def cpu_baseline(desc, cam, spp: int):
@@ -399,6 +443,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
