@@ -149,6 +149,14 @@ template <typename R> MT_D V3<R> sky_dsun(V3<R> dir, const DevSky<R> &sky)
     return d;
 }
 
+// The sky seen along `dir` with weight `coeff` (adj * throughput): its sun
+// radiance term.
+template <typename R> MT_D void sky_sun_grad(const AdjCtx &ctx, V3<R> dir, const DevSky<R> &sky, V3<R> coeff)
+{
+    V3<R> ds = sky_dsun(dir, sky);
+    for (int ch = 0; ch < 3; ++ch) gadd(ctx, ctx.sun + ch, (float)(comp3(coeff, ch) * comp3(ds, ch)));
+}
+
 // pt_sample_pbr / pt_sample_legacy plus what the weight derivative needs.
 template <typename R> struct LobeInfo {
     int kind;       // 0 none, 1 pbr specular, 2 pbr diffuse, 3 legacy diffuse, 4 delta lobe
@@ -269,6 +277,89 @@ template <typename R> MT_D V3<R> safe_div(V3<R> a, V3<R> b)
     return v3(b.x != R(0) ? a.x / b.x : R(0), b.y != R(0) ? a.y / b.y : R(0), b.z != R(0) ? a.z / b.z : R(0));
 }
 
+// A surface vertex of a replayed path, held until its NEE visibility and the
+// radiance the path gathers after it are known. Everything else the
+// vertex's gradient needs is re-drawn from the path's random stream.
+template <typename R> struct AdjVertex {
+    R p[3], n[3], v[3];
+    R beta[3];     // throughput arriving at the vertex (the NEE weight)
+    int mat;       // material index; -1: no vertex pending
+    int b;         // bounce index
+    int flags;     // kVertFront | kVertSun
+    int pad;
+};
+static constexpr int kVertFront = 1;  // front-face hit (legacy glass sampling)
+static constexpr int kVertSun = 2;    // the vertex draws a sun NEE sample
+
+// Gradient terms of one vertex: NEE to every sphere light and to the sun,
+// given each connection's transmittance att[3*slot] (zero where it was not
+// made, occluded or dark: such a connection adds nothing), and the BSDF
+// weight term against `remaining` = L - radiance through this vertex.
+// Light sampling follows pt_nee_emissive / pt_nee_sun (src/pathtrace.c:534-606)
+// and the BSDF sample pt_sample_* (src/pathtrace.c:961-1000), from the same
+// random channels as the primal pass.
+template <typename R>
+MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *att, uint32_t seed_key,
+                         V3<R> remaining, V3<R> adj, const AdjCtx &ctx)
+{
+    const int mi = vx.mat;
+    const DevMaterial<R> &mm = S.materials[mi];
+    const V3<R> P = v3(vx.p[0], vx.p[1], vx.p[2]);
+    const V3<R> N = v3(vx.n[0], vx.n[1], vx.n[2]);
+    const V3<R> V = v3(vx.v[0], vx.v[1], vx.v[2]);
+    const V3<R> nee_w = mul(adj, v3(vx.beta[0], vx.beta[1], vx.beta[2]));
+    const int b = vx.b;
+    const V3<R> one = v3(R(1), R(1), R(1));
+    for (int li = 0; li < S.light_count; ++li) {
+        const V3<R> a = v3(att[3 * li], att[3 * li + 1], att[3 * li + 2]);
+        if (a.x == R(0) && a.y == R(0) && a.z == R(0)) continue;
+        const DevLight<R> &lt = S.lights[li];
+        V3<R> to_c = sub(mat3(lt.center), P);
+        R dc2 = length_sq(to_c);
+        R dc = msqrt(dc2);
+        R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
+        R Omega = R(2) * R(3.14159265358979323846) * (R(1) - cos_mx);
+        V3<R> w = scale(to_c, R(1) / dc);
+        R u1 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
+        R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
+        V3<R> wi = light_sphere_sample_dir(w, cos_mx, u1, u2);
+        V3<R> coeff = scale(nee_w, Omega);
+        shade_grad(mm, mi, N, wi, V, mul(mat3(lt.emissive), a), coeff, ctx);
+        V3<R> s1 = shade(mm, N, wi, V, one);
+        int lmat = __ldg(S.prim_info + lt.prim).y;
+        if (lmat >= 0 && lmat < S.material_count)
+            for (int ch = 0; ch < 3; ++ch)
+                gadd(ctx, kParamsPerMaterial * lmat + 5 + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
+    }
+    if (vx.flags & kVertSun) {
+        const R *as = att + 3 * kMaxLights;
+        const V3<R> a = v3(as[0], as[1], as[2]);
+        if (a.x != R(0) || a.y != R(0) || a.z != R(0)) {
+            R r1 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_A);
+            R r2 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_B);
+            V3<R> Ls = sun_disk_dir(mat3(S.sky.sun_dir), S.sky.sun_radius, r1, r2);
+            R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
+            R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
+            V3<R> coeff = scale(nee_w, Omega);
+            shade_grad(mm, mi, N, Ls, V, mul(mat3(S.sky.sun_color), a), coeff, ctx);
+            V3<R> s1 = shade(mm, N, Ls, V, one);
+            for (int ch = 0; ch < 3; ++ch)
+                gadd(ctx, ctx.sun + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
+        }
+    }
+    uint32_t kb = hash3(seed_key ^ PT_KEY, (uint32_t)b, 0u);
+    R u1 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_A);
+    R u2 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_B);
+    R u_lobe = rand01<R>(kb, (uint32_t)b, PT_CH_LOBE);
+    R u_glass = rand01<R>(kb, (uint32_t)b, PT_CH_GLASS);
+    V3<R> wi, w;
+    int refracted = 0, sampled_specular = 0;
+    LobeInfo<R> info;
+    if (sample_with_info(mm, N, neg(V), V, (vx.flags & kVertFront) ? 1 : 0, u1, u2, u_lobe, u_glass, &wi, &w,
+                         &refracted, &sampled_specular, &info))
+        weight_grad(mm, mi, info, N, V, wi, mul(adj, safe_div(remaining, w)), ctx);
+}
+
 // Replay of pathtrace_radiance (src/pathtrace.c:800-1028) that accumulates
 // adj . dL/dtheta, given the path's value L from the first pass.
 template <typename R>
@@ -295,16 +386,12 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
                 pt_apply_medium(S.materials[medium], R(5.0), &throughput, &radiance);
                 medium = -1;
             }
-            V3<R> ds = sky_dsun(r.d, S.sky);
-            for (int ch = 0; ch < 3; ++ch)
-                gadd(ctx, ctx.sun + ch, (float)(comp3(adj, ch) * comp3(throughput, ch) * comp3(ds, ch)));
+            sky_sun_grad(ctx, r.d, S.sky, mul(adj, throughput));
             return;
         }
         if (medium >= 0) pt_apply_medium(S.materials[medium], h.t, &throughput, &radiance);
         if (h.material < 0 || h.material >= S.material_count) {
-            V3<R> ds = sky_dsun(r.d, S.sky);
-            for (int ch = 0; ch < 3; ++ch)
-                gadd(ctx, ctx.sun + ch, (float)(comp3(adj, ch) * comp3(throughput, ch) * comp3(ds, ch)));
+            sky_sun_grad(ctx, r.d, S.sky, mul(adj, throughput));
             return;
         }
         const int mi = h.material;
@@ -328,6 +415,18 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
         }
         if (b == 0 && length_sq(mat3(mm.atmosphere_glow)) > R(1e-6))
             radiance = add(radiance, mul(throughput, atmosphere_term(mm, N, V, mat3(S.sky.sun_dir))));
+        AdjVertex<R> vx;
+        vx.p[0] = P.x; vx.p[1] = P.y; vx.p[2] = P.z;
+        vx.n[0] = N.x; vx.n[1] = N.y; vx.n[2] = N.z;
+        vx.v[0] = V.x; vx.v[1] = V.y; vx.v[2] = V.z;
+        vx.beta[0] = throughput.x; vx.beta[1] = throughput.y; vx.beta[2] = throughput.z;
+        vx.mat = mi;
+        vx.b = b;
+        vx.flags = (h.front_face ? kVertFront : 0) |
+                   ((b == 0 || (b == 1 && medium >= 0 && last_bounce_specular)) ? kVertSun : 0);
+        vx.pad = 0;
+        R att[kNeeSlots * 3];
+        for (int k = 0; k < kNeeSlots * 3; ++k) att[k] = R(0);
         // ---- emissive-sphere NEE (pt_nee_emissive, src/pathtrace.c:576-606) ----
         if (S.light_count > 0) {
             V3<R> sum = v3(R(0), R(0), R(0));
@@ -351,17 +450,11 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
                 if (!light_sphere_t(S, lt.prim, so, wi, R(1e-3), R(1e30), &lt_t)) continue;
                 V3<R> atten;
                 if (pt_occluded_segment(S, so, wi, R(1e-3), lt_t - R(1e-3), &atten)) continue;
-                V3<R> emit_col = mul(mat3(lt.emissive), atten);
-                V3<R> lit = shade(mm, N, wi, V, emit_col);
+                V3<R> lit = shade(mm, N, wi, V, mul(mat3(lt.emissive), atten));
                 sum = add(sum, mul(throughput, scale(lit, Omega)));
-                V3<R> coeff = scale(mul(adj, throughput), Omega);
-                shade_grad(mm, mi, N, wi, V, emit_col, coeff, ctx);
-                V3<R> s1 = shade(mm, N, wi, V, v3(R(1), R(1), R(1)));
-                int lmat = __ldg(S.prim_info + lt.prim).y;
-                if (lmat >= 0 && lmat < S.material_count)
-                    for (int ch = 0; ch < 3; ++ch)
-                        gadd(ctx, kParamsPerMaterial * lmat + 5 + ch,
-                             (float)(comp3(coeff, ch) * comp3(atten, ch) * comp3(s1, ch)));
+                att[3 * li] = atten.x;
+                att[3 * li + 1] = atten.y;
+                att[3 * li + 2] = atten.z;
             }
             radiance = add(radiance, sum);
         }
@@ -378,19 +471,18 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
                     if (!(atten.x < R(1e-4) && atten.y < R(1e-4) && atten.z < R(1e-4))) {
                         R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
                         R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
-                        V3<R> sun_col = mul(mat3(S.sky.sun_color), atten);
-                        V3<R> lit = shade(mm, N, Ls, V, sun_col);
+                        V3<R> lit = shade(mm, N, Ls, V, mul(mat3(S.sky.sun_color), atten));
                         radiance = add(radiance, mul(throughput, scale(lit, Omega)));
-                        V3<R> coeff = scale(mul(adj, throughput), Omega);
-                        shade_grad(mm, mi, N, Ls, V, sun_col, coeff, ctx);
-                        V3<R> s1 = shade(mm, N, Ls, V, v3(R(1), R(1), R(1)));
-                        for (int ch = 0; ch < 3; ++ch)
-                            gadd(ctx, ctx.sun + ch, (float)(comp3(coeff, ch) * comp3(atten, ch) * comp3(s1, ch)));
+                        att[3 * kMaxLights] = atten.x;
+                        att[3 * kMaxLights + 1] = atten.y;
+                        att[3 * kMaxLights + 2] = atten.z;
                     }
                 }
             }
         }
-        // ---- BSDF sample, weight derivative against the remaining radiance ----
+        // ---- this vertex's gradient; L - radiance is what the path adds after it ----
+        vertex_adjoint(S, vx, att, seed_key, sub(L, radiance), adj, ctx);
+        // ---- BSDF sample (pt_sample_*), continue the path ----
         uint32_t kb = hash3(seed_key ^ PT_KEY, (uint32_t)b, 0u);
         R u1 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_A);
         R u2 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_B);
@@ -398,14 +490,11 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
         R u_glass = rand01<R>(kb, (uint32_t)b, PT_CH_GLASS);
         V3<R> wi, w;
         int refracted = 0, sampled_specular = 0;
-        LobeInfo<R> info;
-        if (!sample_with_info(mm, N, d, V, h.front_face, u1, u2, u_lobe, u_glass, &wi, &w, &refracted, &sampled_specular,
-                              &info))
-            return;
+        bool ok = mm.pbr ? pt_sample_pbr(mm, N, d, V, u1, u2, u_lobe, &wi, &w, &sampled_specular)
+                         : pt_sample_legacy(mm, N, d, V, h.front_face, u1, u2, u_lobe, u_glass, &wi, &w, &refracted,
+                                            &sampled_specular);
+        if (!ok) return;
         last_bounce_specular = sampled_specular;
-        // everything the path adds after this vertex
-        V3<R> remaining = sub(L, radiance);
-        weight_grad(mm, mi, info, N, V, wi, mul(adj, safe_div(remaining, w)), ctx);
         throughput = mul(throughput, w);
         if (!finite3(throughput) || !(pt_max_component(throughput) > R(0))) return;
         if (refracted && (m.is_water || m.beer_lambert)) medium = h.front_face ? mi : -1;

@@ -455,6 +455,27 @@ int render_dev(mt_scene *sc, const mt_camera *cam, int w, int h, int spp_total, 
     return 0;
 }
 
+// The path-replay adjoint with the scene's integrator: the wavefront form
+// (primal and replay passes as stage kernels over compacted queues) or one
+// thread per pixel running both passes.
+template <typename R>
+int adjoint_dev(mt_scene *sc, const mt_camera *cam, int w, int h, int s0, int s1, int depth, const float *adj_img,
+                double scale, double *grad, int n_params, cudaStream_t stream)
+{
+    DevCamera<R> dc;
+    fill_camera(cam, &dc);
+    DevScene<R> S = dev_scene<R>(sc);
+    S.counters = sc->counting ? sc->d_counters : nullptr;
+    if (sc->opts.integrator == MT_INTEGRATOR_WAVEFRONT) {
+        WfAdjointCall a{adj_img, scale, grad, n_params};
+        int rc = wavefront_adjoint(sc->wf, S, dc, w, h, s0, s1, depth, a, stream, &sc->opts);
+        if (rc) return fail(rc, "wavefront adjoint failed: %s", wavefront_last_error());
+        return 0;
+    }
+    CK(launch_adjoint<R>(S, dc, w, h, s0, s1, depth, adj_img, scale, grad, n_params, stream), "adjoint launch");
+    return 0;
+}
+
 int render_args(const mt_scene *sc, const mt_camera *cam, const void *out, int w, int h, int spp, int depth)
 {
     if (sc == nullptr || cam == nullptr || out == nullptr) return fail(MT_ERR_NULL, "NULL pointer");
@@ -988,18 +1009,9 @@ int mt_adjoint_backward_device(mt_scene *sc, const mt_camera *cam, int w, int h,
     cudaStream_t s = (cudaStream_t)stream;
     if (!accumulate) CK(cudaMemsetAsync(grad_dev, 0, np * sizeof(double), s), "cudaMemsetAsync(grad)");
     const double scale = 1.0 / (double)(s1 - s0);
-    if (sc->opts.precision == MT_PRECISION_FP64) {
-        DevCamera<double> dc;
-        fill_camera(cam, &dc);
-        CK(launch_adjoint<double>(sc->sd, dc, w, h, s0, s1, depth, dL_dimage_dev, scale, grad_dev, np, s),
-           "adjoint launch");
-    } else {
-        DevCamera<float> dc;
-        fill_camera(cam, &dc);
-        CK(launch_adjoint<float>(sc->sf, dc, w, h, s0, s1, depth, dL_dimage_dev, scale, grad_dev, np, s),
-           "adjoint launch");
-    }
-    return 0;
+    if (sc->opts.precision == MT_PRECISION_FP64) return adjoint_dev<double>(sc, cam, w, h, s0, s1, depth,
+                                                                           dL_dimage_dev, scale, grad_dev, np, s);
+    return adjoint_dev<float>(sc, cam, w, h, s0, s1, depth, dL_dimage_dev, scale, grad_dev, np, s);
 }
 
 int mt_adjoint_backward(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, int depth, const float *dL_dimage,

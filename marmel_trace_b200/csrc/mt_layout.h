@@ -31,6 +31,7 @@ namespace mt {
 enum : int { KIND_SPHERE = 0, KIND_PLANE = 1, KIND_BOX = 2, KIND_TRIANGLE = 3, KIND_CYLINDER = 4 };
 
 static constexpr int kMaxLights = 8;       // SCENE_MAX_EMISSIVE_LIGHTS, src/scene.h:63
+static constexpr int kNeeSlots = kMaxLights + 1;  // NEE connections per path vertex: the lights, then the sun
 static constexpr int kStackSize = 64;      // traversal stack entries per ray
 static constexpr int kWhittedFrames = 16;  // Whitted recursion frames per sample (max depth 14)
 

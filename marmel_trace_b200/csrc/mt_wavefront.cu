@@ -12,6 +12,13 @@ int wavefront_render(WavefrontState *&st, const DevScene<float> &S, const DevCam
                                         launches);
 }
 
+int wavefront_adjoint(WavefrontState *&st, const DevScene<float> &S, const DevCamera<float> &cam, int w, int h,
+                      int s0, int s1, int depth, const WfAdjointCall &a, cudaStream_t stream, const mt_options *opts)
+{
+    return wavefront_render_impl<float>(st, S, cam, w, h, s0, s1, depth, OUT_SUM_F32, nullptr, stream, opts, nullptr,
+                                        nullptr, nullptr, &a);
+}
+
 void wavefront_stage_times(const WavefrontState *st, double ms[4], long long launches[4])
 {
     for (int i = 0; i < 4; ++i) {

@@ -17,12 +17,10 @@
 // pixel accumulator in sample order, as pt_render_pixel sums it.
 #pragma once
 
-#include "mt_integrate.cuh"
+#include "mt_adjoint.cuh"
 #include "mt_launch.h"
 
 namespace mt {
-
-static constexpr int kNeeSlots = kMaxLights + 1;  // 8 sphere lights + the sun
 
 template <typename R> struct WfRay {
     R o[3];
@@ -64,7 +62,42 @@ template <typename R> struct WfParams {
     int s0;            // first sample of the window
     int spp_window;    // samples in the window
     int out_kind;
+    // adjoint pass: dL/dimage (h, w, 3), its scale, the gradient (float64)
+    const float *adj_img;
+    double *grad;
+    double adj_scale;
+    int n_params;
 };
+
+// Buffers of the adjoint replay pass.
+template <typename R> struct WfAdj {
+    AdjVertex<R> *verts;  // the vertex each path holds until its NEE is resolved
+    R *att;               // per path: kNeeSlots x rgb transmittance of visible NEE connections
+    const R *L;           // per-sample radiance of the primal pass
+    const WfParams<R> *P;
+};
+
+// Block-local gradient accumulator: zeroed at kernel start, flushed to the
+// float64 gradient with one atomic per nonzero parameter at kernel end.
+template <typename R> MT_D void adj_block_begin(float *g, const WfParams<R> *P)
+{
+    for (int i = threadIdx.x; i < P->n_params; i += blockDim.x) g[i] = 0.0f;
+    __syncthreads();
+}
+template <typename R> MT_D void adj_block_end(const float *g, const WfParams<R> *P)
+{
+    __syncthreads();
+    for (int i = threadIdx.x; i < P->n_params; i += blockDim.x)
+        if (g[i] != 0.0f) atomicAdd(&P->grad[i], (double)g[i]);
+}
+
+template <typename R> MT_D V3<R> adj_of_path(const WfParams<R> *P, int slot)
+{
+    const int pix = slot % P->wh;
+    const float *a = P->adj_img + 3 * (size_t)pix;
+    const double sc = P->adj_scale;
+    return v3<R>((R)(a[0] * sc), (R)(a[1] * sc), (R)(a[2] * sc));
+}
 
 struct WfCounters {
     int ray_count[2];
@@ -93,7 +126,7 @@ MT_D int warp_append(int *counter, bool want)
 // ------------------------------------------------------------------
 template <typename R>
 __global__ void k_wf_generate(const DevScene<R> S, const WfParams<R> *P, int batch, int batch_spp, int n_paths,
-                              WfPath<R> *paths, WfRay<R> *rays, WfCounters *C, R *nee)
+                              WfPath<R> *paths, WfRay<R> *rays, WfCounters *C, R *nee, WfAdj<R> A)
 {
     const WfParams<R> p = *P;
     const int n_round = (n_paths + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x) * (gridDim.x * blockDim.x);
@@ -122,6 +155,10 @@ __global__ void k_wf_generate(const DevScene<R> S, const WfParams<R> *P, int bat
         }
         V3<R> d = normalize(ray.d);
         for (int k = 0; k < kNeeSlots * 3; ++k) nee[(size_t)q * kNeeSlots * 3 + k] = R(0);
+        if (A.verts) {  // adjoint replay: no vertex pending, no NEE transmittance yet
+            A.verts[q].mat = -1;
+            for (int k = 0; k < kNeeSlots * 3; ++k) A.att[(size_t)q * kNeeSlots * 3 + k] = R(0);
+        }
         paths[q] = st;
         bool live = length_sq(d) > R(0);  // degenerate primary ray: zero radiance
         int at = warp_append(&C->ray_count[0], live);
@@ -200,11 +237,20 @@ MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> 
 // ------------------------------------------------------------------
 // shade: one bounce of pathtrace_radiance (src/pathtrace.c:835-1018)
 // ------------------------------------------------------------------
-template <typename R>
+//
+// ADJ: the replay pass of the adjoint. The path's previous vertex (held in
+// A.verts) gets its gradient terms once its NEE results are gathered, with
+// the remaining radiance L - radiance; emission and sky terms are taken
+// where they occur. The radiance bookkeeping is the primal pass's, so the
+// replay reproduces it exactly.
+template <typename R, bool ADJ>
 __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
                                                   WfCounters *C, int which, int b, int max_depth, WfPath<R> *paths,
-                                                  R *nee, WfRay<R> *rays_out, WfShadow<R> *sq)
+                                                  R *nee, WfRay<R> *rays_out, WfShadow<R> *sq, WfAdj<R> A)
 {
+    __shared__ float adj_g[ADJ ? kAdjMaxParams : 1];
+    const AdjCtx ctx{adj_g, kParamsPerMaterial * S.material_count};
+    if constexpr (ADJ) adj_block_begin(adj_g, A.P);
     const int n = C->ray_count[which];
     const int stride = gridDim.x * blockDim.x;
     // Every lane of a warp walks the same number of iterations, so the
@@ -219,7 +265,7 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfR
         V3<R> beta = zero;       // throughput before the BSDF update: NEE weight
         V3<R> P = zero, N = zero, V = zero;
         V3<R> next_o = zero, next_d = zero;
-        int mat = -1;
+        int mat = -1, vflags = 0;
         bool shade_hit = false, do_sun = false, cont = false;
         if (active) {
             const WfRay<R> r = rays_in[q];
@@ -230,6 +276,17 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfR
             throughput = v3(st.throughput[0], st.throughput[1], st.throughput[2]);
             radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
             if (b > 0) gather_nee(S, nee + (size_t)slot * kNeeSlots * 3, &radiance);
+            V3<R> adj = zero;
+            if constexpr (ADJ) {
+                adj = adj_of_path(A.P, slot);
+                const AdjVertex<R> pv = A.verts[slot];
+                if (pv.mat >= 0) {
+                    const R *Lq = A.L + 3 * (size_t)slot;
+                    R *att = A.att + (size_t)slot * kNeeSlots * 3;
+                    vertex_adjoint(S, pv, att, st.seed_key, sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj, ctx);
+                    for (int k = 0; k < kNeeSlots * 3; ++k) att[k] = R(0);
+                }
+            }
             const V3<R> ro = v3(r.o[0], r.o[1], r.o[2]);
             const V3<R> d = v3(r.d[0], r.d[1], r.d[2]);
             if (hh.prim < 0) {
@@ -239,6 +296,7 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfR
                     st.medium = -1;
                 }
                 radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
+                if constexpr (ADJ) sky_sun_grad(ctx, d, S.sky, mul(adj, throughput));
             } else {
                 Hit<R> th;
                 th.t = hh.t;
@@ -251,6 +309,7 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfR
                 if (st.medium >= 0) pt_apply_medium(S.materials[st.medium], h.t, &throughput, &radiance);
                 if (h.material < 0 || h.material >= S.material_count) {
                     radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
+                    if constexpr (ADJ) sky_sun_grad(ctx, d, S.sky, mul(adj, throughput));
                 } else {
                     const DevMaterial<R> &m = S.materials[h.material];
                     P = h.point;
@@ -266,10 +325,17 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfR
                         mat = h.material;
                         shade_hit = true;
                         beta = throughput;
-                        if (b == 0 || st.last_specular) radiance = add(radiance, mul(throughput, mat3(m.emissive)));
+                        if (b == 0 || st.last_specular) {
+                            radiance = add(radiance, mul(throughput, mat3(m.emissive)));
+                            if constexpr (ADJ)
+                                for (int ch = 0; ch < 3; ++ch)
+                                    gadd(ctx, kParamsPerMaterial * mat + 5 + ch,
+                                         (float)(comp3(adj, ch) * comp3(throughput, ch)));
+                        }
                         if (b == 0 && length_sq(mat3(m.atmosphere_glow)) > R(1e-6))
                             radiance = add(radiance, mul(throughput, atmosphere_term(m, N, V, mat3(S.sky.sun_dir))));
                         do_sun = (b == 0 || (b == 1 && st.medium >= 0 && st.last_specular));
+                        vflags = (h.front_face ? kVertFront : 0) | (do_sun ? kVertSun : 0);
                         // BSDF sample, throughput update, medium, roulette, advance
                         uint32_t kb = hash3(st.seed_key ^ PT_KEY, (uint32_t)b, 0u);
                         R u1 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_A);
@@ -387,16 +453,31 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfR
             st.radiance[1] = radiance.y;
             st.radiance[2] = radiance.z;
             paths[slot] = st;
+            if constexpr (ADJ) {
+                AdjVertex<R> vx;
+                vx.p[0] = P.x; vx.p[1] = P.y; vx.p[2] = P.z;
+                vx.n[0] = N.x; vx.n[1] = N.y; vx.n[2] = N.z;
+                vx.v[0] = V.x; vx.v[1] = V.y; vx.v[2] = V.z;
+                vx.beta[0] = beta.x; vx.beta[1] = beta.y; vx.beta[2] = beta.z;
+                vx.mat = shade_hit ? mat : -1;
+                vx.b = b;
+                vx.flags = vflags;
+                vx.pad = 0;
+                A.verts[slot] = vx;
+            }
         }
     }
+    if constexpr (ADJ) adj_block_end(adj_g, A.P);
 }
 
 // ------------------------------------------------------------------
 // shadow: pt_occluded_segment (src/pathtrace.c:504-532) per NEE connection
 // ------------------------------------------------------------------
-template <typename R>
+// ADJ: also keep the connection's transmittance (zero when it adds no light)
+// for the replay's gradient terms.
+template <typename R, bool ADJ>
 __global__ void __launch_bounds__(128) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
-                                                   R *nee)
+                                                   R *nee, R *att)
 {
     const int n = C->shadow_count;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -415,14 +496,24 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const DevScene<R> S, const Wf
             occ = scene_any(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
         }
         V3<R> res = v3(R(0), R(0), R(0));
+        bool lit = false;
         if (!occ) {
             bool dark = s.li == kMaxLights && atten.x < R(1e-4) && atten.y < R(1e-4) && atten.z < R(1e-4);
-            if (!dark) res = mul(v3(s.contrib[0], s.contrib[1], s.contrib[2]), atten);
+            if (!dark) {
+                res = mul(v3(s.contrib[0], s.contrib[1], s.contrib[2]), atten);
+                lit = true;
+            }
         }
-        R *slot = nee + ((size_t)s.slot * kNeeSlots + s.li) * 3;
+        const size_t at = ((size_t)s.slot * kNeeSlots + s.li) * 3;
+        R *slot = nee + at;
         slot[0] = res.x;
         slot[1] = res.y;
         slot[2] = res.z;
+        if constexpr (ADJ) {
+            att[at] = lit ? atten.x : R(0);
+            att[at + 1] = lit ? atten.y : R(0);
+            att[at + 2] = lit ? atten.z : R(0);
+        }
     }
 }
 
@@ -445,6 +536,27 @@ __global__ void k_wf_finalize(const DevScene<R> S, int n_paths, const WfPath<R> 
         sample_buf[3 * (size_t)q + 1] = radiance.y;
         sample_buf[3 * (size_t)q + 2] = radiance.z;
     }
+}
+
+// Adjoint replay: the vertex each path still holds (its last) takes its
+// gradient terms against the radiance the path ends with.
+template <typename R>
+__global__ void k_wf_finalize_adj(const DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
+{
+    __shared__ float adj_g[kAdjMaxParams];
+    const AdjCtx ctx{adj_g, kParamsPerMaterial * S.material_count};
+    adj_block_begin(adj_g, A.P);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_paths; q += gridDim.x * blockDim.x) {
+        const AdjVertex<R> pv = A.verts[q];
+        if (pv.mat < 0) continue;
+        const WfPath<R> st = paths[q];
+        V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
+        gather_nee(S, nee + (size_t)q * kNeeSlots * 3, &radiance);
+        const R *Lq = A.L + 3 * (size_t)q;
+        vertex_adjoint(S, pv, A.att + (size_t)q * kNeeSlots * 3, st.seed_key,
+                       sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj_of_path(A.P, q), ctx);
+    }
+    adj_block_end(adj_g, A.P);
 }
 
 template <typename R>

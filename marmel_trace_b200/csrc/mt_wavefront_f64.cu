@@ -12,4 +12,11 @@ int wavefront_render(WavefrontState *&st, const DevScene<double> &S, const DevCa
                                          launches);
 }
 
+int wavefront_adjoint(WavefrontState *&st, const DevScene<double> &S, const DevCamera<double> &cam, int w, int h,
+                      int s0, int s1, int depth, const WfAdjointCall &a, cudaStream_t stream, const mt_options *opts)
+{
+    return wavefront_render_impl<double>(st, S, cam, w, h, s0, s1, depth, OUT_SUM_F32, nullptr, stream, opts,
+                                         nullptr, nullptr, nullptr, &a);
+}
+
 }  // namespace mt

@@ -31,6 +31,11 @@ struct WavefrontState {
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::string key;
+    // adjoint replay: pending vertex and NEE transmittance per path slot, and
+    // the graph of the primal + replay window
+    void *adj_verts = nullptr, *adj_att = nullptr;
+    cudaGraphExec_t adj_exec = nullptr;
+    std::string adj_key;
     int grid = 0;              // persistent grid (blocks) of the stage kernels
     cudaEvent_t kev[64];       // per-kernel timing events (profiling mode)
     bool kev_init = false;
@@ -60,8 +65,8 @@ inline int fail(int code, const char *what, cudaError_t e)
 
 inline void wf_free(WavefrontState *st)
 {
-    void **bufs[] = {&st->paths, &st->rays[0], &st->rays[1], &st->hits, &st->nee, &st->shadow, &st->sample_buf,
-                     &st->acc, &st->params};
+    void **bufs[] = {&st->paths, &st->rays[0], &st->rays[1], &st->hits,      &st->nee,      &st->shadow,
+                     &st->sample_buf, &st->acc, &st->params, &st->adj_verts, &st->adj_att};
     for (void **b : bufs) {
         if (*b) cudaFree(*b);
         *b = nullptr;
@@ -71,9 +76,15 @@ inline void wf_free(WavefrontState *st)
     if (st->exec) cudaGraphExecDestroy(st->exec);
     st->exec = nullptr;
     st->key.clear();
+    if (st->adj_exec) cudaGraphExecDestroy(st->adj_exec);
+    st->adj_exec = nullptr;
+    st->adj_key.clear();
     st->cap_paths = 0;
     st->acc_pixels = 0;
 }
+
+// the pinned host staging block of the parameters is 256 bytes
+static_assert(sizeof(WfParams<double>) <= 256 && sizeof(WfParams<float>) <= 256, "parameter block size");
 
 // Grow the buffers to hold `n_paths` path slots and `wh` pixels.
 template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t wh, int light_count)
@@ -100,11 +111,23 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
     return 0;
 }
 
+// The adjoint replay's per-path buffers, sized to the reserved path slots.
+template <typename R> int wf_reserve_adj(WavefrontState *st)
+{
+    if (st->adj_verts) return 0;
+    WF_CK(cudaMalloc(&st->adj_verts, st->cap_paths * sizeof(AdjVertex<R>)), "cudaMalloc(adjoint vertices)");
+    WF_CK(cudaMalloc(&st->adj_att, st->cap_paths * kNeeSlots * 3 * sizeof(R)), "cudaMalloc(adjoint nee)");
+    return 0;
+}
+
 // Enqueue one frame window. In profiling mode (`prof`), every stage kernel is
 // bracketed by CUDA events and its time is added to st->kernel_ms.
+// `adjoint`: per batch, the primal pass leaves every sample's radiance in
+// sample_buf, then the replay pass re-traces the same paths and accumulates
+// the parameter gradient (no image is written).
 template <typename R>
 int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch_spp, int n_batches, int depth,
-               cudaStream_t s, bool prof, int block)
+               cudaStream_t s, bool prof, int block, bool adjoint = false)
 {
     const int wh = w * h;
     const int n_paths = wh * batch_spp;
@@ -133,10 +156,15 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         st->kernel_launches[kind] += 1;
         ev += 2;
     };
-    for (int batch = 0; batch < n_batches; ++batch) {
+    const WfAdj<R> none{nullptr, nullptr, nullptr, P};
+    const WfAdj<R> A{(AdjVertex<R> *)st->adj_verts, (R *)st->adj_att, sample_buf, P};
+    // generate -> (extend, shade, shadow) x (depth + 1); the replay pass uses
+    // the ADJ stage kernels
+    auto bounces = [&](int batch, bool replay) -> int {
         WF_CK(cudaMemsetAsync(C, 0, sizeof(WfCounters), s), "memset(counters)");
         tic();
-        k_wf_generate<R><<<g, block, 0, s>>>(S, P, batch, batch_spp, n_paths, paths, rays[0], C, nee);
+        k_wf_generate<R><<<g, block, 0, s>>>(S, P, batch, batch_spp, n_paths, paths, rays[0], C, nee,
+                                             replay ? A : none);
         toc(3);
         int which = 0;
         for (int b = 0; b <= depth; ++b) {
@@ -146,18 +174,38 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
             WF_CK(cudaMemsetAsync(&C->shadow_count, 0, sizeof(int), s), "memset(shadow_count)");
             tic();
-            k_wf_shade<R><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee, rays[which ^ 1],
-                                              sq);
+            if (replay) {
+                k_wf_shade<R, true><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
+                                                        rays[which ^ 1], sq, A);
+            } else {
+                k_wf_shade<R, false><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
+                                                         rays[which ^ 1], sq, none);
+            }
             toc(1);
             tic();
-            k_wf_shadow<R><<<g, block, smem, s>>>(S, sq, C, nee);
+            if (replay)
+                k_wf_shadow<R, true><<<g, block, smem, s>>>(S, sq, C, nee, A.att);
+            else
+                k_wf_shadow<R, false><<<g, block, smem, s>>>(S, sq, C, nee, nullptr);
             toc(2);
             which ^= 1;
         }
+        return 0;
+    };
+    for (int batch = 0; batch < n_batches; ++batch) {
+        int rc = bounces(batch, false);
+        if (rc) return rc;
         tic();
         k_wf_finalize<R><<<g, block, 0, s>>>(S, n_paths, paths, nee, sample_buf);
-        k_wf_reduce<R><<<g, block, 0, s>>>(P, batch_spp, batch == 0, batch == n_batches - 1, sample_buf, acc);
+        if (!adjoint)
+            k_wf_reduce<R><<<g, block, 0, s>>>(P, batch_spp, batch == 0, batch == n_batches - 1, sample_buf, acc);
         toc(3);
+        if (adjoint) {
+            if ((rc = bounces(batch, true))) return rc;
+            tic();
+            k_wf_finalize_adj<R><<<g, block, 0, s>>>(S, n_paths, paths, nee, A);
+            toc(3);
+        }
     }
     WF_CK(cudaGetLastError(), "wavefront launch");
     return 0;
@@ -166,7 +214,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
 template <typename R>
 int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCamera<R> &cam, int w, int h, int s0,
                           int s1, int depth, int out_kind, void *out, cudaStream_t stream, const mt_options *opts,
-                          cudaEvent_t ev0, cudaEvent_t ev1, int32_t *launches)
+                          cudaEvent_t ev0, cudaEvent_t ev1, int32_t *launches, const WfAdjointCall *adj = nullptr)
 {
     if (!st) st = new WavefrontState();
     const int wh = w * h;
@@ -183,6 +231,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     int n_batches = spp / batch_spp;
     int rc = wf_reserve<R>(st, (size_t)wh * batch_spp, (size_t)wh, S.light_count);
     if (rc) return rc;
+    const bool adjoint = adj != nullptr;
+    if (adjoint && (rc = wf_reserve_adj<R>(st))) return rc;
     int block = 128;
     if (!st->grid) {
         int dev = 0, sms = 0, per_sm = 0;
@@ -204,6 +254,12 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     hp.s0 = s0;
     hp.spp_window = spp;
     hp.out_kind = out_kind;
+    if (adjoint) {
+        hp.adj_img = adj->adj_img;
+        hp.grad = adj->grad;
+        hp.adj_scale = adj->scale;
+        hp.n_params = adj->n_params;
+    }
     bool prof = opts && opts->use_graph < 0;   // profiling mode: no graph, per-kernel events
     bool use_graph = !prof && (!opts || opts->use_graph != 0);
     if (prof && !st->kev_init) {
@@ -215,19 +271,21 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     cudaStreamSynchronize(stream);  // the pinned block may still be in use by a previous copy
     memcpy(st->h_params, &hp, sizeof hp);
     WF_CK(cudaMemcpyAsync(st->params, st->h_params, sizeof hp, cudaMemcpyHostToDevice, stream), "params copy");
-    int kernels_per_window = n_batches * (3 * (depth + 1) + 3);
+    int kernels_per_window = adjoint ? n_batches * 2 * (3 * (depth + 1) + 2) : n_batches * (3 * (depth + 1) + 3);
+    cudaGraphExec_t &exec = adjoint ? st->adj_exec : st->exec;
+    std::string &exec_key = adjoint ? st->adj_key : st->key;
     if (use_graph) {
         char key[256];
         // the scene travels by value in the captured kernel parameters, so
         // its identity, counters and parameter version are part of the key
         snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d", (int)sizeof(R), w, h, batch_spp, n_batches, depth,
                  (const void *)S.nodes, (const void *)S.counters, S.version);
-        if (!st->exec || st->key != key) {
-            if (st->exec) cudaGraphExecDestroy(st->exec);
-            st->exec = nullptr;
+        if (!exec || exec_key != key) {
+            if (exec) cudaGraphExecDestroy(exec);
+            exec = nullptr;
             if (!st->cap_stream) WF_CK(cudaStreamCreateWithFlags(&st->cap_stream, cudaStreamNonBlocking), "stream");
             WF_CK(cudaStreamBeginCapture(st->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-            int erc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, st->cap_stream, false, block);
+            int erc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, st->cap_stream, false, block, adjoint);
             cudaGraph_t graph = nullptr;
             cudaError_t ce = cudaStreamEndCapture(st->cap_stream, &graph);
             if (erc) {
@@ -235,14 +293,14 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
                 return erc;
             }
             WF_CK(ce, "end capture");
-            cudaError_t ie = cudaGraphInstantiate(&st->exec, graph, 0);
+            cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
             cudaGraphDestroy(graph);
             WF_CK(ie, "graph instantiate");
-            st->key = key;
+            exec_key = key;
         }
-        WF_CK(cudaGraphLaunch(st->exec, stream), "graph launch");
+        WF_CK(cudaGraphLaunch(exec, stream), "graph launch");
     } else {
-        rc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, stream, prof, block);
+        rc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, stream, prof, block, adjoint);
         if (rc) return rc;
     }
     if (ev1) WF_CK(cudaEventRecord(ev1, stream), "cudaEventRecord");

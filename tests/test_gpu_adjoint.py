@@ -120,3 +120,28 @@ def test_autograd_function_and_fp32_fp64_agree(mtlib):
     g32, g64 = grads
     big = np.abs(g64) > 1e-3 * np.abs(g64).max()
     assert np.allclose(g32[big], g64[big], rtol=2e-3, atol=1e-6)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("which", ["pbr", "legacy"])
+def test_wavefront_adjoint_matches_megakernel(mtlib, prec, which):
+    """The wavefront replay (stage kernels, each vertex's gradient deferred
+    until its NEE is resolved) and the one-thread-per-pixel replay evaluate
+    the same estimator on the same random streams; only the order of the
+    float gradient sums differs."""
+    if which == "pbr":
+        d = scenes.adjoint_scene(n_spheres=24, n_materials=8, n_emissive=2)
+    else:
+        d = scenes.spheres_scene()  # Lambert, metal and glass: shadow rays pass through glass
+    W, H, SPP, DEPTH = 40, 30, 6, 5
+    wts = _loss_weights(H, W, 3)
+    g = {}
+    for integ in ("wavefront", "megakernel"):
+        r = DiffRenderer(d, W, H, SPP, DEPTH, precision=prec, integrator=integ)
+        g[integ] = r.backward(wts, s0=17).cpu().numpy()
+        r.release()
+    gw, gm = g["wavefront"], g["megakernel"]
+    scale = np.abs(gm).max()
+    assert scale > 0
+    tol = 1e-5 if prec == "fp64" else 2e-3
+    assert np.allclose(gw, gm, rtol=tol, atol=tol * scale), np.c_[gw, gm][np.abs(gw - gm) > tol * scale]
