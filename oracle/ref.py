@@ -53,6 +53,8 @@ _SIG = {
     "mtref_whitted_linear": (I, [P, I, I, I, I, P, I]),
     "mtref_bvh_export": (I, [P, P, P, P, P, P, P, P, P]),
     "mtref_bvh_count": (I, [P, I, P, P, D, D, P, P, P]),
+    "mtdual_param_count": (I, [P]),
+    "mtdual_pathtrace_grad": (I, [P, I, I, I, I, I, P, D, P, I, P, P]),
 }
 
 _lib = None
@@ -210,6 +212,23 @@ class RefScene:
         nt = threads or os.cpu_count() or 1
         self.lib.mtref_pathtrace_linear(self.h, w, h, s0, spp, depth, _p(out), nt)
         return out / spp
+
+    def dual_grad(self, w, h, s0, s1, depth, adj, idx=None, scale=None):
+        """Forward-mode (dual-number) gradient of sum(adj * mean image) over
+        samples [s0, s1) with respect to the adjoint's parameters `idx`
+        (default: all). Returns (grad, value_sum, mismatches): value_sum is the
+        per-pixel sum of sample values; mismatches counts samples whose value
+        or BSDF weight differs from the reference's own (must be 0)."""
+        n = self.lib.mtdual_param_count(self.h)
+        idx = np.arange(n, dtype=np.int32) if idx is None else np.ascontiguousarray(idx, dtype=np.int32)
+        a = np.ascontiguousarray(adj, dtype=np.float32).reshape(h, w, 3)
+        g = np.zeros(len(idx), np.float64)
+        vs = np.zeros((h, w, 3), np.float64)
+        sc = 1.0 / (s1 - s0) if scale is None else scale
+        rc = self.lib.mtdual_pathtrace_grad(self.h, w, h, s0, s1, depth, _p(a), sc, _p(idx), len(idx), _p(g), _p(vs))
+        if rc < 0:
+            raise RuntimeError("the dual-number oracle does not cover this scene")
+        return g, vs, rc
 
     def whitted_render(self, w, h, spp, depth):
         out = np.zeros((h, w, 3), np.uint8)

@@ -145,3 +145,47 @@ def test_wavefront_adjoint_matches_megakernel(mtlib, prec, which):
     assert scale > 0
     tol = 1e-5 if prec == "fp64" else 2e-3
     assert np.allclose(gw, gm, rtol=tol, atol=tol * scale), np.c_[gw, gm][np.abs(gw - gm) > tol * scale]
+
+
+@pytest.mark.parametrize("integ", ["wavefront", "megakernel"])
+@pytest.mark.parametrize("which", ["pbr", "legacy"])
+def test_adjoint_matches_dual_number_oracle(mtlib, oracle, which, integ):
+    """Every parameter's gradient (albedo, roughness, metallic, emissive per
+    material, sun radiance) against forward-mode differentiation of the
+    reference path tracer (oracle/ref_dual.cpp) on the same samples. FP64
+    kernels: the only differences are the float gradient sums and last-ulp
+    transcendentals."""
+    if which == "pbr":
+        d = scenes.adjoint_scene(n_spheres=24, n_materials=8, n_emissive=2)
+    else:
+        d = scenes.spheres_scene(n_spheres=24)  # Lambert, metal and glass
+    W, H, SPP, DEPTH = 24, 16, 4, 5
+    adj = np.random.default_rng(5).uniform(0.5, 1.5, (H, W, 3)).astype(np.float32)
+    r = DiffRenderer(d, W, H, SPP, DEPTH, precision="fp64", integrator=integ)
+    g = r.backward(torch.tensor(adj, device="cuda"), s0=3).cpu().numpy()
+    r.release()
+    ref = oracle.RefScene.from_desc(d, d.make_camera(W, H))
+    gd, _, mismatches = ref.dual_grad(W, H, 3, 3 + SPP, DEPTH, adj)
+    ref.free()
+    assert mismatches == 0
+    scale = np.abs(gd).max()
+    assert (np.abs(gd) > 1e-3 * scale).sum() >= 10
+    bad = ~np.isclose(g, gd, rtol=1e-4, atol=1e-6 * scale)
+    assert not bad.any(), np.c_[np.nonzero(bad)[0], g[bad], gd[bad]]
+
+
+def test_fp32_adjoint_close_to_dual_number_oracle(mtlib, oracle):
+    d = scenes.adjoint_scene(n_spheres=24, n_materials=8, n_emissive=2)
+    W, H, SPP, DEPTH = 32, 24, 8, 6
+    adj = np.random.default_rng(6).uniform(0.5, 1.5, (H, W, 3)).astype(np.float32)
+    r = DiffRenderer(d, W, H, SPP, DEPTH, precision="fp32")
+    g = r.backward(torch.tensor(adj, device="cuda")).cpu().numpy()
+    r.release()
+    ref = oracle.RefScene.from_desc(d, d.make_camera(W, H))
+    gd, _, mismatches = ref.dual_grad(W, H, 0, SPP, DEPTH, adj)
+    ref.free()
+    assert mismatches == 0
+    big = np.abs(gd) > 1e-2 * np.abs(gd).max()
+    rel = np.abs(g[big] - gd[big]) / np.abs(gd[big])
+    # FP32 rounding can flip an occasional roulette or lobe decision
+    assert np.median(rel) < 1e-3 and np.quantile(rel, 0.9) < 2e-2, rel
