@@ -186,7 +186,8 @@ def run_ours(args):
     desc = build_scene()
     cam = desc.make_camera(W, H)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
-    g = mt.GpuScene(desc, precision="fp32", integrator=args.integrator, device=local)
+    qopt = {"queue_capacity": args.queue_capacity} if args.queue_capacity else {}
+    g = mt.GpuScene(desc, precision="fp32", integrator=args.integrator, device=local, **qopt)
     fr = Frames(g, cam, SPP, torch)
 
     # counting pass (untimed): rays, node pairs and primitive tests per sample
@@ -227,7 +228,7 @@ def run_ours(args):
     # dominant-kernel duration: one frame with every stage bracketed by events
     stage = None
     if args.integrator == "wavefront":
-        gp = mt.GpuScene(desc, precision="fp32", integrator="wavefront", use_graph=-1, device=local)
+        gp = mt.GpuScene(desc, precision="fp32", integrator="wavefront", use_graph=-1, device=local, **qopt)
         fp = Frames(gp, cam, SPP, torch)
         fp.render(0, base=30_000)
         gp.set_counting(False)  # resets the stage timers
@@ -305,6 +306,7 @@ def run_ours(args):
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": SPP, "depth": DEPTH,
                    "integrator": args.integrator, "parallelism": f"replicas x{world}",
+                   "queue_capacity": args.queue_capacity or 8 << 20,
                    "l2": "flushed between timed steps (256 MB write); the 90 MB scene fits in L2"},
         "plain_gpu_msamples_s": round(plain, 3) if plain else None,
         "mrays_per_s": round(value * rays_per_sample, 2),
@@ -367,7 +369,9 @@ def adjoint_bench(torch, device: int, flush, steps: int = 3):
             "params": r.n_params, "grads_per_s": round(1.0 / b, 3), "backward_ms": round(1e3 * b, 2),
             "forward_ms": round(1e3 * f, 2), "backward_msamples_s": round(aw * ah * aspp / b / 1e6, 2),
             "forward_msamples_s": round(aw * ah * aspp / f / 1e6, 2),
-            "method": "path replay: each sample traced then replayed from its random stream (megakernel form)"}
+            "method": "path replay, wavefront form: per batch a primal pass records each sample's radiance, "
+                      "then a replay pass re-traces the same paths from their random streams with the stage "
+                      "kernels and accumulates the gradient"}
 
 
 def cpu_baseline(desc, cam, spp: int):
@@ -444,6 +448,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--queue-capacity", type=int, default=0,
+                    help="path slots per wavefront batch (0: the library default, 8M)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -198,7 +198,14 @@ typedef struct {
     int32_t use_graph;       /* wavefront: 1 = capture the sample window in a CUDA graph,
                                 0 = plain launches, -1 = plain launches timed per stage */
     int32_t device;          /* CUDA device ordinal                             */
+    int32_t traversal;       /* wavefront traversal kernels: MT_TRAVERSAL_*     */
 } mt_options;
+
+/* Wavefront traversal kernels (extend and shadow stages). */
+#define MT_TRAVERSAL_DEFAULT 0   /* library default (grid-stride)                    */
+#define MT_TRAVERSAL_STATIC  1   /* grid-stride loop: one ray per lane per pass      */
+#define MT_TRAVERSAL_DYNAMIC 2   /* persistent lanes that refill from the queue as   */
+                                 /* their rays finish                                 */
 
 /* Fill `o` with the library defaults (FP32, megakernel, BVH2, device 0). */
 void mt_options_default(mt_options *o);

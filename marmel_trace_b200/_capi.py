@@ -148,6 +148,7 @@ class MtOptions(C.Structure):
         ("sort_threshold", C.c_int32),
         ("use_graph", C.c_int32),
         ("device", C.c_int32),
+        ("traversal", C.c_int32),
     ]
 
 

@@ -545,6 +545,7 @@ void mt_options_default(mt_options *o)
     o->sort_threshold = 0;
     o->use_graph = 1;
     o->device = 0;
+    o->traversal = MT_TRAVERSAL_DEFAULT;
 }
 
 const char *mt_version(void) { return "mtgpu 0.1 (sm_100a)"; }

@@ -495,6 +495,36 @@ MT_D void count_add(unsigned long long *p, unsigned long long v)
     if (v) atomicAdd(p, v);
 }
 
+// Traversal work counters of one thread (flushed once per ray batch).
+struct TravCount {
+    unsigned long long nvis = 0, ntest = 0, ntri = 0;
+};
+
+template <typename R, bool ANY> MT_D void trav_count_flush(const DevScene<R> &S, TravCount &c)
+{
+    if (!S.counters) return;
+    if (ANY) {
+        count_add(&S.counters->any_node_visits, c.nvis);
+        count_add(&S.counters->any_prim_tests, c.ntest);
+        count_add(&S.counters->any_tri_tests, c.ntri);
+    } else {
+        count_add(&S.counters->node_visits, c.nvis);
+        count_add(&S.counters->prim_tests, c.ntest);
+        count_add(&S.counters->tri_tests, c.ntri);
+    }
+    c = TravCount();
+}
+
+// Resumable traversal of one ray: the walk advances one leaf at a time
+// (trav_step), so a kernel can interleave rays on a lane.
+template <typename R> struct Trav {
+    RayPre<R> rp;
+    R tmin, closest;
+    int node;   // next node to visit, kEmpty when the walk is over
+    int sp;     // stack entries in use
+    bool found;
+};
+
 // Nearest hit (ANY = false) or any hit (ANY = true) in [tmin, tmax].
 // Nearest hit keeps the reference's semantics exactly: planes first
 // (src/bvh.c:579-591), then the tree; each primitive is tested against
@@ -502,140 +532,159 @@ MT_D void count_add(unsigned long long *p, unsigned long long v)
 // (src/bvh.c:641-646). Node order and culling only change the amount of
 // work, never the result. Any hit is bvh_occluded's boolean
 // (src/bvh.c:714-813); the last-occluder cache there only reorders tests.
+//
+// trav_init tests the planes and sets the walk at the root.
 template <typename R, bool ANY>
-MT_D bool traverse(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best)
+MT_D void trav_init(const DevScene<R> &S, Trav<R> &tv, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best,
+                    TravCount &c)
 {
-    bool found = false;
-    R closest = tmax;
-    unsigned long long nvis = 0, ntest = 0, ntri = 0;
-
+    tv.rp = rp;
+    tv.tmin = tmin;
+    tv.closest = tmax;
+    tv.found = false;
+    tv.sp = 0;
     for (int i = 0; i < S.plane_count; ++i) {
         R t;
-        ++ntest;
-        if (plane_t(S.planes + 6 * (size_t)i, rp.o, rp.d, tmin, closest, &t)) {
+        ++c.ntest;
+        if (plane_t(S.planes + 6 * (size_t)i, rp.o, rp.d, tmin, tv.closest, &t)) {
             int pi = S.plane_prims[i];
             if (ANY) {
-                found = true;
+                tv.found = true;
                 break;
             }
-            if (!found || t < best->t || (t == best->t && pi < best->prim)) {
+            if (!tv.found || t < best->t || (t == best->t && pi < best->prim)) {
                 best->t = t;
                 best->u = R(0);
                 best->v = R(0);
                 best->prim = pi;
                 best->code = (KIND_PLANE << 28) | i;
-                closest = t;
-                found = true;
+                tv.closest = t;
+                tv.found = true;
             }
         }
     }
+    tv.node = (S.node_count > 0 && !(ANY && tv.found)) ? 0 : kEmpty;
+}
 
-    if (S.node_count > 0 && !(ANY && found)) {
-        int *stk = mt_stack_smem + threadIdx.x;
-        const int stride = blockDim.x;
-        const int cap = S.stack_depth;
-        int sp = 0;
-        int node = 0;
-        bool done = false;
-        while (!done) {
-            // ---- descend through inner nodes ----
-            while (node >= 0) {
-                const float4 *Nd = S.nodes + 4 * (size_t)node;
-                float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
-                int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
-                bool hl, hr;
-                R tl, tr;
-                ++nvis;
-                node_test(q0, q1, q2, rp, tmin, closest, &hl, &hr, &tl, &tr);
-                if (hl && hr) {
-                    bool lnear = tl <= tr;
-                    int nearc = lnear ? q3.x : q3.y;
-                    int farc = lnear ? q3.y : q3.x;
-                    if (sp >= cap) {
-                        atomicOr(S.err, ERR_STACK);
-                        done = true;
-                        node = kEmpty;
-                        break;
-                    }
-                    stk[sp * stride] = farc;
-                    ++sp;
-                    node = nearc;
-                } else if (hl) {
-                    node = q3.x;
-                } else if (hr) {
-                    node = q3.y;
-                } else {
-                    node = sp > 0 ? stk[--sp * stride] : kEmpty;
-                }
+// One while-while step: descend through inner nodes (nearer child in a
+// register, farther child pushed) to a leaf, test the leaf, pop the next
+// node. Returns false once the walk is over. `stk` is this thread's stack
+// (entry k at stk[k * stride]).
+template <typename R, bool ANY>
+MT_D bool trav_step(const DevScene<R> &S, Trav<R> &tv, int *stk, int stride, Hit<R> *best, TravCount &c)
+{
+    const RayPre<R> &rp = tv.rp;
+    const R tmin = tv.tmin;
+    const int cap = S.stack_depth;
+    int node = tv.node;
+    int sp = tv.sp;
+    // ---- descend through inner nodes ----
+    while (node >= 0) {
+        const float4 *Nd = S.nodes + 4 * (size_t)node;
+        float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
+        int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
+        bool hl, hr;
+        R tl, tr;
+        ++c.nvis;
+        node_test(q0, q1, q2, rp, tmin, tv.closest, &hl, &hr, &tl, &tr);
+        if (hl && hr) {
+            bool lnear = tl <= tr;
+            int nearc = lnear ? q3.x : q3.y;
+            int farc = lnear ? q3.y : q3.x;
+            if (sp >= cap) {
+                atomicOr(S.err, ERR_STACK);
+                tv.node = kEmpty;
+                return false;
             }
-            if (node == kEmpty) break;
-            // ---- leaf ----
-            int leaf = ~node;
-            int first = leaf >> 4, count = leaf & 7;
-            if ((leaf >> 3) & 1) {
-                for (int i = 0; i < count; ++i) {
-                    R t, u, v;
-                    ++ntest;
-                    ++ntri;
-                    if (tri_t(S, first + i, rp, tmin, closest, &t, &u, &v)) {
-                        if (ANY) {
-                            found = true;
-                            break;
-                        }
-                        int pi = tri_prim_index(S, first + i);
-                        if (!found || t < best->t || (t == best->t && pi < best->prim)) {
-                            best->t = t;
-                            best->u = u;
-                            best->v = v;
-                            best->prim = pi;
-                            best->code = (KIND_TRIANGLE << 28) | (first + i);
-                            closest = t;
-                            found = true;
-                        }
-                    }
-                }
-            } else {
-                for (int i = 0; i < count; ++i) {
-                    int2 ref = __ldg(S.refs + first + i);
-                    R t, u, v;
-                    ++ntest;
-                    ntri += (ref.y >> 28) == KIND_TRIANGLE;
-                    bool hit = ANY ? prim_occluded(S, ref.y, rp, tmin, tmax)
-                                   : prim_hit_t(S, ref.y, rp, tmin, closest, &t, &u, &v);
-                    if (hit) {
-                        if (ANY) {
-                            found = true;
-                            break;
-                        }
-                        if (!found || t < best->t || (t == best->t && ref.x < best->prim)) {
-                            best->t = t;
-                            best->u = u;
-                            best->v = v;
-                            best->prim = ref.x;
-                            best->code = ref.y;
-                            closest = t;
-                            found = true;
-                        }
-                    }
-                }
-            }
-            if (ANY && found) break;
-            node = sp > 0 ? stk[--sp * stride] : kEmpty;
-            if (node == kEmpty) break;
-        }
-    }
-    if (S.counters) {
-        if (ANY) {
-            count_add(&S.counters->any_node_visits, nvis);
-            count_add(&S.counters->any_prim_tests, ntest);
-            count_add(&S.counters->any_tri_tests, ntri);
+            stk[sp * stride] = farc;
+            ++sp;
+            node = nearc;
+        } else if (hl) {
+            node = q3.x;
+        } else if (hr) {
+            node = q3.y;
         } else {
-            count_add(&S.counters->node_visits, nvis);
-            count_add(&S.counters->prim_tests, ntest);
-            count_add(&S.counters->tri_tests, ntri);
+            node = sp > 0 ? stk[--sp * stride] : kEmpty;
         }
     }
-    return found;
+    if (node == kEmpty) {
+        tv.node = kEmpty;
+        return false;
+    }
+    // ---- leaf ----
+    int leaf = ~node;
+    int first = leaf >> 4, count = leaf & 7;
+    if ((leaf >> 3) & 1) {
+        for (int i = 0; i < count; ++i) {
+            R t, u, v;
+            ++c.ntest;
+            ++c.ntri;
+            if (tri_t(S, first + i, rp, tmin, tv.closest, &t, &u, &v)) {
+                if (ANY) {
+                    tv.found = true;
+                    break;
+                }
+                int pi = tri_prim_index(S, first + i);
+                if (!tv.found || t < best->t || (t == best->t && pi < best->prim)) {
+                    best->t = t;
+                    best->u = u;
+                    best->v = v;
+                    best->prim = pi;
+                    best->code = (KIND_TRIANGLE << 28) | (first + i);
+                    tv.closest = t;
+                    tv.found = true;
+                }
+            }
+        }
+    } else {
+        for (int i = 0; i < count; ++i) {
+            int2 ref = __ldg(S.refs + first + i);
+            R t, u, v;
+            ++c.ntest;
+            c.ntri += (ref.y >> 28) == KIND_TRIANGLE;
+            bool hit = ANY ? prim_occluded(S, ref.y, rp, tmin, tv.closest)
+                           : prim_hit_t(S, ref.y, rp, tmin, tv.closest, &t, &u, &v);
+            if (hit) {
+                if (ANY) {
+                    tv.found = true;
+                    break;
+                }
+                if (!tv.found || t < best->t || (t == best->t && ref.x < best->prim)) {
+                    best->t = t;
+                    best->u = u;
+                    best->v = v;
+                    best->prim = ref.x;
+                    best->code = ref.y;
+                    tv.closest = t;
+                    tv.found = true;
+                }
+            }
+        }
+    }
+    if (ANY && tv.found) {
+        tv.node = kEmpty;
+        return false;
+    }
+    node = sp > 0 ? stk[--sp * stride] : kEmpty;
+    tv.node = node;
+    tv.sp = sp;
+    return node != kEmpty;
+}
+
+// The whole walk of one ray.
+template <typename R, bool ANY>
+MT_D bool traverse(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best)
+{
+    TravCount c;
+    Trav<R> tv;
+    trav_init<R, ANY>(S, tv, rp, tmin, tmax, best, c);
+    if (tv.node != kEmpty) {
+        int *stk = mt_stack_smem + threadIdx.x;
+        while (trav_step<R, ANY>(S, tv, stk, blockDim.x, best, c)) {
+        }
+    }
+    trav_count_flush<R, ANY>(S, c);
+    return tv.found;
 }
 
 template <typename R>

@@ -102,7 +102,9 @@ template <typename R> MT_D V3<R> adj_of_path(const WfParams<R> *P, int slot)
 struct WfCounters {
     int ray_count[2];
     int shadow_count;
-    int pad;
+    int shadow_fetch;  // next shadow ray handed out by the dynamic-fetch kernel
+    int ray_fetch;     // next ray handed out by the dynamic-fetch extend kernel
+    int pad[3];
 };
 
 // Warp-aggregated queue append: one atomicAdd per warp, lanes get
@@ -515,6 +517,119 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const DevScene<R> S, const Wf
             att[at + 2] = lit ? atten.z : R(0);
         }
     }
+}
+
+// ------------------------------------------------------------------
+// Dynamic ray fetch (persistent threads with per-lane refill; Aila and
+// Laine, HPG 2009): every lane walks its ray one leaf at a time (trav_step)
+// and, once it is done, takes the next ray of the queue, so lanes whose rays
+// end early do not idle until the warp's longest walk is over. Refills are
+// warp-aggregated: one atomicAdd hands out consecutive rays to every idle
+// lane, once at least kFetchMin lanes are idle or no lane is busy. Results
+// are those of the grid-stride kernels above; only the ray-to-lane schedule
+// differs.
+// ------------------------------------------------------------------
+static constexpr int kFetchMin = 8;
+
+// One refill round. Returns the ray this lane takes (-1: none this round);
+// sets *more = false once the queue of `n` rays is drained for this lane.
+MT_D int fetch_round(int *counter, int n, bool idle, bool busy_lane, bool *more)
+{
+    const unsigned want = __ballot_sync(0xffffffffu, idle);
+    const unsigned busy = __ballot_sync(0xffffffffu, busy_lane);
+    if (!want || (busy && __popc(want) < kFetchMin)) return -1;
+    const int leader = __ffs(want) - 1;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(want));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!idle) return -1;
+    const int mine = base + __popc(want & ((1u << lane) - 1u));
+    if (mine >= n) {
+        *more = false;
+        return -1;
+    }
+    return mine;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_wf_extend_dyn(const DevScene<R> S, const WfRay<R> *rays, WfCounters *C,
+                                                       int which, WfHit<R> *hits)
+{
+    const int n = C->ray_count[which];
+    int *stk = mt_stack_smem + threadIdx.x;
+    const int stride = blockDim.x;
+    int q = -1;
+    bool more = true;
+    Trav<R> tv;
+    Hit<R> best;
+    TravCount cnt;
+    while (__any_sync(0xffffffffu, q >= 0 || more)) {
+        const int f = fetch_round(&C->ray_fetch, n, q < 0 && more, q >= 0, &more);
+        if (f >= 0) {
+            q = f;
+            const WfRay<R> r = rays[q];
+            V3<R> d = unit_dir(v3(r.d[0], r.d[1], r.d[2]));
+            trav_init<R, false>(S, tv, ray_pre(v3(r.o[0], r.o[1], r.o[2]), d), R(1e-4), R(1e30), &best, cnt);
+        }
+        if (q >= 0) {
+            if (tv.node == kEmpty || !trav_step<R, false>(S, tv, stk, stride, &best, cnt)) {
+                WfHit<R> out;
+                out.t = tv.found ? best.t : R(0);
+                out.u = tv.found ? best.u : R(0);
+                out.v = tv.found ? best.v : R(0);
+                out.prim = tv.found ? best.prim : -1;
+                out.code = tv.found ? best.code : 0;
+                hits[q] = out;
+                q = -1;
+            }
+        }
+    }
+    trav_count_flush<R, false>(S, cnt);
+    if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->extension_rays, (unsigned long long)n);
+}
+
+// Shadow rays of a scene without pass-through materials: a pure any-hit
+// query per connection (see k_wf_shadow).
+template <typename R, bool ADJ>
+__global__ void __launch_bounds__(128) k_wf_shadow_dyn(const DevScene<R> S, const WfShadow<R> *sq, WfCounters *C,
+                                                       R *nee, R *att)
+{
+    const int n = C->shadow_count;
+    int *stk = mt_stack_smem + threadIdx.x;
+    const int stride = blockDim.x;
+    int q = -1;
+    bool more = true;
+    Trav<R> tv;
+    Hit<R> unused;
+    TravCount cnt;
+    while (__any_sync(0xffffffffu, q >= 0 || more)) {
+        const int f = fetch_round(&C->shadow_fetch, n, q < 0 && more, q >= 0, &more);
+        if (f >= 0) {
+            q = f;
+            const WfShadow<R> s = sq[q];
+            V3<R> d = unit_dir(v3(s.d[0], s.d[1], s.d[2]));
+            trav_init<R, true>(S, tv, ray_pre(v3(s.o[0], s.o[1], s.o[2]), d), R(1e-3), s.tmax, &unused, cnt);
+        }
+        if (q >= 0) {
+            if (tv.node == kEmpty || !trav_step<R, true>(S, tv, stk, stride, &unused, cnt)) {
+                const WfShadow<R> &s = sq[q];
+                const bool lit = !tv.found;
+                const size_t at = ((size_t)s.slot * kNeeSlots + s.li) * 3;
+                nee[at] = lit ? s.contrib[0] : R(0);
+                nee[at + 1] = lit ? s.contrib[1] : R(0);
+                nee[at + 2] = lit ? s.contrib[2] : R(0);
+                if constexpr (ADJ) {
+                    att[at] = lit ? R(1) : R(0);
+                    att[at + 1] = lit ? R(1) : R(0);
+                    att[at + 2] = lit ? R(1) : R(0);
+                }
+                q = -1;
+            }
+        }
+    }
+    trav_count_flush<R, true>(S, cnt);
+    if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->shadow_rays, (unsigned long long)n);
 }
 
 // ------------------------------------------------------------------

@@ -125,9 +125,12 @@ template <typename R> int wf_reserve_adj(WavefrontState *st)
 // `adjoint`: per batch, the primal pass leaves every sample's radiance in
 // sample_buf, then the replay pass re-traces the same paths and accumulates
 // the parameter gradient (no image is written).
+//
+// `dyn`: the extend stage, and the shadow stage of scenes without
+// pass-through materials, use the dynamic-fetch traversal kernels.
 template <typename R>
 int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch_spp, int n_batches, int depth,
-               cudaStream_t s, bool prof, int block, bool adjoint = false)
+               cudaStream_t s, bool prof, int block, bool adjoint = false, bool dyn = false)
 {
     const int wh = w * h;
     const int n_paths = wh * batch_spp;
@@ -169,10 +172,14 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         int which = 0;
         for (int b = 0; b <= depth; ++b) {
             tic();
-            k_wf_extend<R><<<g, block, smem, s>>>(S, rays[which], C, which, hits);
+            if (dyn)
+                k_wf_extend_dyn<R><<<g, block, smem, s>>>(S, rays[which], C, which, hits);
+            else
+                k_wf_extend<R><<<g, block, smem, s>>>(S, rays[which], C, which, hits);
             toc(0);
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
-            WF_CK(cudaMemsetAsync(&C->shadow_count, 0, sizeof(int), s), "memset(shadow_count)");
+            // shadow_count, shadow_fetch and ray_fetch (the next extend's)
+            WF_CK(cudaMemsetAsync(&C->shadow_count, 0, 3 * sizeof(int), s), "memset(shadow_count)");
             tic();
             if (replay) {
                 k_wf_shade<R, true><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
@@ -183,8 +190,13 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             }
             toc(1);
             tic();
-            if (replay)
+            const bool dyn_shadow = dyn && !S.has_passthrough;
+            if (replay && dyn_shadow)
+                k_wf_shadow_dyn<R, true><<<g, block, smem, s>>>(S, sq, C, nee, A.att);
+            else if (replay)
                 k_wf_shadow<R, true><<<g, block, smem, s>>>(S, sq, C, nee, A.att);
+            else if (dyn_shadow)
+                k_wf_shadow_dyn<R, false><<<g, block, smem, s>>>(S, sq, C, nee, nullptr);
             else
                 k_wf_shadow<R, false><<<g, block, smem, s>>>(S, sq, C, nee, nullptr);
             toc(2);
@@ -273,19 +285,24 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     WF_CK(cudaMemcpyAsync(st->params, st->h_params, sizeof hp, cudaMemcpyHostToDevice, stream), "params copy");
     int kernels_per_window = adjoint ? n_batches * 2 * (3 * (depth + 1) + 2) : n_batches * (3 * (depth + 1) + 3);
     cudaGraphExec_t &exec = adjoint ? st->adj_exec : st->exec;
+    // dynamic fetch reorders rays across lanes: on coherent queues (primary
+    // rays, NEE rays grouped by light) the grid-stride kernels are faster, so
+    // they are the default and dynamic fetch is a tuning candidate
+    const bool dyn = opts && opts->traversal == MT_TRAVERSAL_DYNAMIC;
     std::string &exec_key = adjoint ? st->adj_key : st->key;
     if (use_graph) {
         char key[256];
         // the scene travels by value in the captured kernel parameters, so
         // its identity, counters and parameter version are part of the key
-        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d", (int)sizeof(R), w, h, batch_spp, n_batches, depth,
-                 (const void *)S.nodes, (const void *)S.counters, S.version);
+        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d", (int)sizeof(R), w, h, batch_spp, n_batches, depth,
+                 (const void *)S.nodes, (const void *)S.counters, S.version, (int)dyn);
         if (!exec || exec_key != key) {
             if (exec) cudaGraphExecDestroy(exec);
             exec = nullptr;
             if (!st->cap_stream) WF_CK(cudaStreamCreateWithFlags(&st->cap_stream, cudaStreamNonBlocking), "stream");
             WF_CK(cudaStreamBeginCapture(st->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-            int erc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, st->cap_stream, false, block, adjoint);
+            int erc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, st->cap_stream, false, block, adjoint,
+                                    dyn);
             cudaGraph_t graph = nullptr;
             cudaError_t ce = cudaStreamEndCapture(st->cap_stream, &graph);
             if (erc) {
@@ -300,7 +317,7 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         }
         WF_CK(cudaGraphLaunch(exec, stream), "graph launch");
     } else {
-        rc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, stream, prof, block, adjoint);
+        rc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, stream, prof, block, adjoint, dyn);
         if (rc) return rc;
     }
     if (ev1) WF_CK(cudaEventRecord(ev1, stream), "cudaEventRecord");
