@@ -329,6 +329,20 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
 
     S->node_count = fb.node_count;
     S->stack_depth = fb.depth + 1;  // pushes happen only on the way down
+    S->bvh_width = 2;
+    S->wide_stack_depth = 0;
+    const int W = sc->opts.bvh_width;
+    if (sizeof(R) == 4 && (W == 4 || W == 8) && fb.node_count > 0) {
+        std::vector<float> n2(nodes.size() * 4), wide;
+        memcpy(n2.data(), nodes.data(), n2.size() * sizeof(float));
+        int bound = 0;
+        if (collapse_bvh(n2, fb.node_count, W, &wide, &bound)) return fail(MT_ERR_INVALID, "wide BVH collapse");
+        std::vector<float4> wn(wide.size() / 4);
+        memcpy(wn.data(), wide.data(), wide.size() * sizeof(float));
+        if ((rc = sc->upload(wn, &S->wnodes))) return rc;
+        S->bvh_width = W;
+        S->wide_stack_depth = bound + 1;
+    }
     S->plane_count = (int)plane_prims.size();
     S->prim_count = n;
     S->material_count = d->material_count;
@@ -565,6 +579,12 @@ int mt_scene_create(const mt_scene_desc *desc, const mt_options *opts, mt_scene 
     if (opts) sc->opts = *opts;
     else mt_options_default(&sc->opts);
     if (sc->opts.block_size <= 0) sc->opts.block_size = 128;
+    if (sc->opts.bvh_width == 0) sc->opts.bvh_width = 2;
+    if (sc->opts.bvh_width != 2 && sc->opts.bvh_width != 4 && sc->opts.bvh_width != 8) {
+        int wd = sc->opts.bvh_width;
+        delete sc;
+        return fail(MT_ERR_INVALID, "bvh_width %d (2, 4 or 8)", wd);
+    }
     if (sc->opts.device < 0 || sc->opts.device >= ndev) {
         delete sc;
         return fail(MT_ERR_INVALID, "device %d out of range", sc->opts.device);

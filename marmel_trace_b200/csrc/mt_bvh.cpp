@@ -408,4 +408,98 @@ int flatten_bvh(const HostBvh &b, FlatBvh *out)
     return 0;
 }
 
+namespace {
+
+struct Slot {
+    float mn[3], mx[3];
+    int code;
+};
+
+struct Collapser {
+    const std::vector<float> &n2;
+    int W;
+    std::vector<float> *out;
+    int words;
+
+    // child `side` (0 left, 1 right) of binary node `i`
+    Slot child(int i, int side) const
+    {
+        const float *q = n2.data() + 16 * (size_t)i;
+        Slot s;
+        if (side == 0) {
+            s.mn[0] = q[0], s.mx[0] = q[1], s.mn[1] = q[2], s.mx[1] = q[3], s.mn[2] = q[8], s.mx[2] = q[9];
+        } else {
+            s.mn[0] = q[4], s.mx[0] = q[5], s.mn[1] = q[6], s.mx[1] = q[7], s.mn[2] = q[10], s.mx[2] = q[11];
+        }
+        memcpy(&s.code, q + 12 + side, sizeof(int));
+        return s;
+    }
+    static double area(const Slot &s)
+    {
+        double dx = (double)s.mx[0] - s.mn[0], dy = (double)s.mx[1] - s.mn[1], dz = (double)s.mx[2] - s.mn[2];
+        return 2.0 * (dx * dy + dy * dz + dz * dx);
+    }
+    static bool empty_leaf(int code) { return code < 0 && ((~code) & 7) == 0; }
+
+    // Emit the wide node for binary node i; returns its index and the stack
+    // bound of its subtree.
+    int emit(int i, int *bound)
+    {
+        std::vector<Slot> slots = {child(i, 0), child(i, 1)};
+        while ((int)slots.size() < W) {
+            int best = -1;
+            double ba = -1.0;
+            for (int k = 0; k < (int)slots.size(); ++k)
+                if (slots[k].code >= 0 && area(slots[k]) > ba) {
+                    ba = area(slots[k]);
+                    best = k;
+                }
+            if (best < 0) break;
+            int inner = slots[best].code;
+            slots[best] = child(inner, 0);
+            slots.insert(slots.begin() + best + 1, child(inner, 1));
+        }
+        std::vector<Slot> used;
+        for (const Slot &s : slots)
+            if (!empty_leaf(s.code)) used.push_back(s);
+        const int idx = (int)(out->size() / (size_t)words);
+        out->resize(out->size() + (size_t)words, 0.0f);
+        int sub = 0;
+        std::vector<int> codes(W, (int)0x80000000);
+        for (int k = 0; k < (int)used.size(); ++k) {
+            int code = used[k].code;
+            if (code >= 0) {
+                int b = 0;
+                code = emit(code, &b);
+                sub = std::max(sub, b);
+            }
+            codes[k] = code;
+        }
+        float *rec = out->data() + (size_t)idx * words;
+        for (int k = 0; k < W; ++k) {
+            bool on = k < (int)used.size();
+            for (int a = 0; a < 3; ++a) {
+                rec[(2 * a) * W + k] = on ? used[k].mn[a] : 0.0f;
+                rec[(2 * a + 1) * W + k] = on ? used[k].mx[a] : 0.0f;
+            }
+            memcpy(rec + 6 * W + k, &codes[k], sizeof(int));
+        }
+        *bound = std::max(0, (int)used.size() - 1) + sub;
+        return idx;
+    }
+};
+
+}  // namespace
+
+int collapse_bvh(const std::vector<float> &nodes2, int node_count, int W, std::vector<float> *out, int *stack_bound)
+{
+    out->clear();
+    *stack_bound = 0;
+    if (W != 4 && W != 8) return -1;
+    if (node_count <= 0) return 0;
+    Collapser c{nodes2, W, out, W == 4 ? 32 : 64};
+    c.emit(0, stack_bound);
+    return 0;
+}
+
 }  // namespace mt

@@ -44,4 +44,17 @@ struct FlatBvh {
 // the tree shape.
 int flatten_bvh(const HostBvh &b, FlatBvh *out);
 
+// Wide tree for the traversal kernels: every node holds up to W (4 or 8)
+// children, made by collapsing the device binary tree `nodes2` (16 floats per
+// node, its final child codes in the last 4) from the root down: a node's
+// child slots start as the two binary children and the inner slot with the
+// largest box surface area is replaced by its two children until W slots are
+// filled or only leaves are left. Leaf codes are kept, so both trees share
+// the leaves. Record (float words): lo_x, hi_x, lo_y, hi_y, lo_z, hi_z (W
+// each), the W child codes, padding to 32 (W = 4) or 64 (W = 8) words. An
+// unused slot has child code INT_MIN. *stack_bound is the most entries a
+// walk can hold: the sum over a root-to-leaf path of (children - 1).
+int collapse_bvh(const std::vector<float> &nodes2, int node_count, int W, std::vector<float> *out,
+                 int *stack_bound);
+
 }  // namespace mt

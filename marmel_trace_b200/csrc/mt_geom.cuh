@@ -566,52 +566,12 @@ MT_D void trav_init(const DevScene<R> &S, Trav<R> &tv, const RayPre<R> &rp, R tm
     tv.node = (S.node_count > 0 && !(ANY && tv.found)) ? 0 : kEmpty;
 }
 
-// One while-while step: descend through inner nodes (nearer child in a
-// register, farther child pushed) to a leaf, test the leaf, pop the next
-// node. Returns false once the walk is over. `stk` is this thread's stack
-// (entry k at stk[k * stride]).
+// Primitive tests of one leaf (code < 0, see leaf_code).
 template <typename R, bool ANY>
-MT_D bool trav_step(const DevScene<R> &S, Trav<R> &tv, int *stk, int stride, Hit<R> *best, TravCount &c)
+MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, TravCount &c)
 {
     const RayPre<R> &rp = tv.rp;
     const R tmin = tv.tmin;
-    const int cap = S.stack_depth;
-    int node = tv.node;
-    int sp = tv.sp;
-    // ---- descend through inner nodes ----
-    while (node >= 0) {
-        const float4 *Nd = S.nodes + 4 * (size_t)node;
-        float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
-        int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
-        bool hl, hr;
-        R tl, tr;
-        ++c.nvis;
-        node_test(q0, q1, q2, rp, tmin, tv.closest, &hl, &hr, &tl, &tr);
-        if (hl && hr) {
-            bool lnear = tl <= tr;
-            int nearc = lnear ? q3.x : q3.y;
-            int farc = lnear ? q3.y : q3.x;
-            if (sp >= cap) {
-                atomicOr(S.err, ERR_STACK);
-                tv.node = kEmpty;
-                return false;
-            }
-            stk[sp * stride] = farc;
-            ++sp;
-            node = nearc;
-        } else if (hl) {
-            node = q3.x;
-        } else if (hr) {
-            node = q3.y;
-        } else {
-            node = sp > 0 ? stk[--sp * stride] : kEmpty;
-        }
-    }
-    if (node == kEmpty) {
-        tv.node = kEmpty;
-        return false;
-    }
-    // ---- leaf ----
     int leaf = ~node;
     int first = leaf >> 4, count = leaf & 7;
     if ((leaf >> 3) & 1) {
@@ -661,6 +621,150 @@ MT_D bool trav_step(const DevScene<R> &S, Trav<R> &tv, int *stk, int stride, Hit
             }
         }
     }
+}
+
+// Descend the binary tree from `node` (nearer child in a register, farther
+// child pushed) to the next leaf; kEmpty when the walk is over or the stack
+// would overflow (error word set).
+template <typename R>
+MT_D int descend2(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp, int *stk, int stride, TravCount &c)
+{
+    const int cap = S.stack_depth;
+    while (node >= 0) {
+        const float4 *Nd = S.nodes + 4 * (size_t)node;
+        float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
+        int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
+        bool hl, hr;
+        R tl, tr;
+        ++c.nvis;
+        node_test(q0, q1, q2, tv.rp, tv.tmin, tv.closest, &hl, &hr, &tl, &tr);
+        if (hl && hr) {
+            bool lnear = tl <= tr;
+            int nearc = lnear ? q3.x : q3.y;
+            int farc = lnear ? q3.y : q3.x;
+            if (sp >= cap) {
+                atomicOr(S.err, ERR_STACK);
+                return kEmpty;
+            }
+            stk[sp * stride] = farc;
+            ++sp;
+            node = nearc;
+        } else if (hl) {
+            node = q3.x;
+        } else if (hr) {
+            node = q3.y;
+        } else {
+            node = sp > 0 ? stk[--sp * stride] : kEmpty;
+        }
+    }
+    return node;
+}
+
+// Slab test of one child box (the arithmetic of node_test).
+template <typename R>
+MT_D bool box_hit(float lx, float hx, float ly, float hy, float lz, float hz, const RayPre<R> &rp, R tmin, R tmax,
+                  R *enter)
+{
+    R x0 = (R(lx) - rp.o.x) * rp.inv.x, x1 = (R(hx) - rp.o.x) * rp.inv.x;
+    R y0 = (R(ly) - rp.o.y) * rp.inv.y, y1 = (R(hy) - rp.o.y) * rp.inv.y;
+    R z0 = (R(lz) - rp.o.z) * rp.inv.z, z1 = (R(hz) - rp.o.z) * rp.inv.z;
+    R en = mfmax(mfmax(mfmin(x0, x1), mfmin(y0, y1)), mfmin(z0, z1));
+    R ex = mfmin(mfmin(mfmax(x0, x1), mfmax(y0, y1)), mfmax(z0, z1));
+    *enter = en < tmin ? tmin : en;
+    return ex >= en && ex >= tmin && en <= tmax;
+}
+
+// Descend the wide tree (W = 4 or 8 children per node): test every child box,
+// continue with the nearest hit child and push the other hit children
+// farthest first, so they pop nearest first.
+template <typename R, int W>
+MT_D int descend_wide(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp, int *stk, int stride,
+                      TravCount &c)
+{
+    constexpr int G = W / 4;  // float4 words per coordinate row
+    const int cap = S.wide_stack_depth;
+    while (node >= 0) {
+        const float4 *Nd = S.wnodes + (size_t)(8 * G) * node;
+        ++c.nvis;
+        R d[W];
+        int ch[W];
+        unsigned mask = 0;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const float4 lx = __ldg(Nd + 0 * G + g), hx = __ldg(Nd + 1 * G + g);
+            const float4 ly = __ldg(Nd + 2 * G + g), hy = __ldg(Nd + 3 * G + g);
+            const float4 lz = __ldg(Nd + 4 * G + g), hz = __ldg(Nd + 5 * G + g);
+            const int4 cc = __ldg(reinterpret_cast<const int4 *>(Nd + 6 * G + g));
+            const int b = 4 * g;
+            ch[b] = cc.x;
+            ch[b + 1] = cc.y;
+            ch[b + 2] = cc.z;
+            ch[b + 3] = cc.w;
+            if (cc.x != kEmpty && box_hit(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, tv.rp, tv.tmin, tv.closest, &d[b]))
+                mask |= 1u << b;
+            if (cc.y != kEmpty && box_hit(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, tv.rp, tv.tmin, tv.closest, &d[b + 1]))
+                mask |= 2u << b;
+            if (cc.z != kEmpty && box_hit(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, tv.rp, tv.tmin, tv.closest, &d[b + 2]))
+                mask |= 4u << b;
+            if (cc.w != kEmpty && box_hit(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, tv.rp, tv.tmin, tv.closest, &d[b + 3]))
+                mask |= 8u << b;
+        }
+        if (!mask) {
+            node = sp > 0 ? stk[--sp * stride] : kEmpty;
+            continue;
+        }
+        // nearest hit child
+        R bd = R(3.0e38);
+        int bi = 0, next = kEmpty;
+#pragma unroll
+        for (int i = 0; i < W; ++i)
+            if (((mask >> i) & 1u) && d[i] < bd) {
+                bd = d[i];
+                bi = i;
+                next = ch[i];
+            }
+        mask &= ~(1u << bi);
+        if (sp + __popc(mask) > cap) {
+            atomicOr(S.err, ERR_STACK);
+            return kEmpty;
+        }
+        // the others, farthest first
+        while (mask) {
+            R fd = R(-1.0);
+            int fi = 0, fc = kEmpty;
+#pragma unroll
+            for (int i = 0; i < W; ++i)
+                if (((mask >> i) & 1u) && d[i] >= fd) {
+                    fd = d[i];
+                    fi = i;
+                    fc = ch[i];
+                }
+            stk[sp * stride] = fc;
+            ++sp;
+            mask &= ~(1u << fi);
+        }
+        node = next;
+    }
+    return node;
+}
+
+// One while-while step: descend to a leaf, test it, pop the next node.
+// Returns false once the walk is over. `stk` is this thread's stack (entry k
+// at stk[k * stride]). W is the tree: 2 (binary `nodes`), 4 or 8 (`wnodes`).
+template <typename R, bool ANY, int W = 2>
+MT_D bool trav_step(const DevScene<R> &S, Trav<R> &tv, int *stk, int stride, Hit<R> *best, TravCount &c)
+{
+    int sp = tv.sp;
+    int node;
+    if constexpr (W == 2)
+        node = descend2(S, tv, tv.node, sp, stk, stride, c);
+    else
+        node = descend_wide<R, W>(S, tv, tv.node, sp, stk, stride, c);
+    if (node == kEmpty) {
+        tv.node = kEmpty;
+        return false;
+    }
+    trav_leaf<R, ANY>(S, tv, node, best, c);
     if (ANY && tv.found) {
         tv.node = kEmpty;
         return false;
@@ -672,7 +776,7 @@ MT_D bool trav_step(const DevScene<R> &S, Trav<R> &tv, int *stk, int stride, Hit
 }
 
 // The whole walk of one ray.
-template <typename R, bool ANY>
+template <typename R, bool ANY, int W = 2>
 MT_D bool traverse(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best)
 {
     TravCount c;
@@ -680,23 +784,23 @@ MT_D bool traverse(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hi
     trav_init<R, ANY>(S, tv, rp, tmin, tmax, best, c);
     if (tv.node != kEmpty) {
         int *stk = mt_stack_smem + threadIdx.x;
-        while (trav_step<R, ANY>(S, tv, stk, blockDim.x, best, c)) {
+        while (trav_step<R, ANY, W>(S, tv, stk, blockDim.x, best, c)) {
         }
     }
     trav_count_flush<R, ANY>(S, c);
     return tv.found;
 }
 
-template <typename R>
+template <typename R, int W = 2>
 MT_D bool scene_nearest(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best)
 {
-    return traverse<R, false>(S, rp, tmin, tmax, best);
+    return traverse<R, false, W>(S, rp, tmin, tmax, best);
 }
 
-template <typename R> MT_D bool scene_any(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax)
+template <typename R, int W = 2> MT_D bool scene_any(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax)
 {
     Hit<R> dummy;
-    return traverse<R, true>(S, rp, tmin, tmax, &dummy);
+    return traverse<R, true, W>(S, rp, tmin, tmax, &dummy);
 }
 
 // scene_intersect / scene_occluded entry semantics: a direction that is not

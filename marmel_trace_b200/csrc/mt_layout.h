@@ -11,6 +11,10 @@
 //                primitive references start at ~index (count in q3.z / q3.w).
 //                One node load tests two children, the GPU form of the
 //                reference's bvh_slab_2way (src/bvh.c:495-533).
+//   wnodes     : optional wide tree (bvh_width 4 or 8, FP32 path): 128 / 256 B
+//                records of W child boxes as SoA (lo_x, hi_x, lo_y, hi_y, lo_z,
+//                hi_z, W floats each) and W child codes, collapsed from `nodes`
+//                with the same leaf codes (collapse_bvh, mt_bvh.cpp).
 //   refs       : leaf-ordered primitive references, int2 {prim_index, code},
 //                code = kind << 28 | slot into the per-kind array.
 //   tri4       : FP32 triangles, 48 B = (v0.xyz, prim_index) (e1.xyz, smooth)
@@ -115,6 +119,7 @@ struct DevCounters {
 
 template <typename R> struct DevScene {
     const float4 *nodes;
+    const float4 *wnodes;    // wide tree (bvh_width 4 or 8; FP32 path), same leaves as `nodes`
     const int2 *refs;
     const float4 *tri4;      // FP32 triangle records (R = float)
     const R *tris;           // FP64 triangle records a, e1, e2 (R = double)
@@ -136,6 +141,8 @@ template <typename R> struct DevScene {
     int water_material;
     int has_passthrough;   // some material lets shadow rays through (water, transparency > 0.8)
     int stack_depth;       // traversal stack entries per thread (dynamic shared memory)
+    int bvh_width;         // 2, or 4 / 8 when `wnodes` is present
+    int wide_stack_depth;  // stack entries per thread for the wide tree
     int version;           // bumped whenever material / sun parameters change
     R water_level;
     DevOcean<R> ocean;

@@ -109,7 +109,7 @@ extern "C" int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_cam
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MT_ERR_LAUNCH;
             int sms = 0, per_sm = 0;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_extend<float>, 128,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_extend<float, 2>, 128,
                                                           (size_t)(S.stack_depth > 0 ? S.stack_depth : 1) * 128 * 4);
             g_grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
             g_scratch_ptr[dev] = (unsigned char *)p;

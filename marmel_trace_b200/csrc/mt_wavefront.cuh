@@ -179,7 +179,7 @@ __global__ void k_wf_generate(const DevScene<R> S, const WfParams<R> *P, int bat
 // ------------------------------------------------------------------
 // extend: nearest hit (scene_intersect, src/scene.c:767 -> src/bvh.c:557)
 // ------------------------------------------------------------------
-template <typename R>
+template <typename R, int W>
 __global__ void __launch_bounds__(128) k_wf_extend(const DevScene<R> S, const WfRay<R> *rays, const WfCounters *C,
                                                    int which, WfHit<R> *hits)
 {
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(128) k_wf_extend(const DevScene<R> S, const Wf
         RayPre<R> rp = ray_pre(o, d);
         Hit<R> h;
         WfHit<R> out;
-        if (scene_nearest(S, rp, R(1e-4), R(1e30), &h)) {
+        if (scene_nearest<R, W>(S, rp, R(1e-4), R(1e30), &h)) {
             out.t = h.t;
             out.u = h.u;
             out.v = h.v;
@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfR
 // ------------------------------------------------------------------
 // ADJ: also keep the connection's transmittance (zero when it adds no light)
 // for the replay's gradient terms.
-template <typename R, bool ADJ>
+template <typename R, bool ADJ, int W>
 __global__ void __launch_bounds__(128) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
                                                    R *nee, R *att)
 {
@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const DevScene<R> S, const Wf
             // walk stops at its first hit, so it equals an any-hit query.
             atten = v3(R(1), R(1), R(1));
             if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
-            occ = scene_any(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
+            occ = scene_any<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
         }
         V3<R> res = v3(R(0), R(0), R(0));
         bool lit = false;
@@ -552,7 +552,7 @@ MT_D int fetch_round(int *counter, int n, bool idle, bool busy_lane, bool *more)
     return mine;
 }
 
-template <typename R>
+template <typename R, int W>
 __global__ void __launch_bounds__(128) k_wf_extend_dyn(const DevScene<R> S, const WfRay<R> *rays, WfCounters *C,
                                                        int which, WfHit<R> *hits)
 {
@@ -573,7 +573,7 @@ __global__ void __launch_bounds__(128) k_wf_extend_dyn(const DevScene<R> S, cons
             trav_init<R, false>(S, tv, ray_pre(v3(r.o[0], r.o[1], r.o[2]), d), R(1e-4), R(1e30), &best, cnt);
         }
         if (q >= 0) {
-            if (tv.node == kEmpty || !trav_step<R, false>(S, tv, stk, stride, &best, cnt)) {
+            if (tv.node == kEmpty || !trav_step<R, false, W>(S, tv, stk, stride, &best, cnt)) {
                 WfHit<R> out;
                 out.t = tv.found ? best.t : R(0);
                 out.u = tv.found ? best.u : R(0);
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(128) k_wf_extend_dyn(const DevScene<R> S, cons
 
 // Shadow rays of a scene without pass-through materials: a pure any-hit
 // query per connection (see k_wf_shadow).
-template <typename R, bool ADJ>
+template <typename R, bool ADJ, int W>
 __global__ void __launch_bounds__(128) k_wf_shadow_dyn(const DevScene<R> S, const WfShadow<R> *sq, WfCounters *C,
                                                        R *nee, R *att)
 {
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(128) k_wf_shadow_dyn(const DevScene<R> S, cons
             trav_init<R, true>(S, tv, ray_pre(v3(s.o[0], s.o[1], s.o[2]), d), R(1e-3), s.tmax, &unused, cnt);
         }
         if (q >= 0) {
-            if (tv.node == kEmpty || !trav_step<R, true>(S, tv, stk, stride, &unused, cnt)) {
+            if (tv.node == kEmpty || !trav_step<R, true, W>(S, tv, stk, stride, &unused, cnt)) {
                 const WfShadow<R> &s = sq[q];
                 const bool lit = !tv.found;
                 const size_t at = ((size_t)s.slot * kNeeSlots + s.li) * 3;

@@ -120,6 +120,50 @@ template <typename R> int wf_reserve_adj(WavefrontState *st)
     return 0;
 }
 
+// Traversal stage launches for the tree width W (2: binary nodes; 4 / 8: the
+// wide tree, FP32 only). `smem` is the stack of that tree.
+template <typename R, int W>
+void launch_extend(bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
+                   const WfRay<R> *rays, WfCounters *C, int which, WfHit<R> *hits)
+{
+    if (dyn)
+        k_wf_extend_dyn<R, W><<<g, block, smem, s>>>(S, rays, C, which, hits);
+    else
+        k_wf_extend<R, W><<<g, block, smem, s>>>(S, rays, C, which, hits);
+}
+
+template <typename R, bool ADJ, int W>
+void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
+                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att)
+{
+    if (dyn && !S.has_passthrough)
+        k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
+    else
+        k_wf_shadow<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
+}
+
+template <typename R, bool ADJ>
+void launch_shadow_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
+                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att)
+{
+    if constexpr (sizeof(R) == 4) {
+        if (W == 4) return launch_shadow<R, ADJ, 4>(dyn, g, block, smem, s, S, sq, C, nee, att);
+        if (W == 8) return launch_shadow<R, ADJ, 8>(dyn, g, block, smem, s, S, sq, C, nee, att);
+    }
+    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att);
+}
+
+template <typename R>
+void launch_extend_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
+                     const WfRay<R> *rays, WfCounters *C, int which, WfHit<R> *hits)
+{
+    if constexpr (sizeof(R) == 4) {
+        if (W == 4) return launch_extend<R, 4>(dyn, g, block, smem, s, S, rays, C, which, hits);
+        if (W == 8) return launch_extend<R, 8>(dyn, g, block, smem, s, S, rays, C, which, hits);
+    }
+    launch_extend<R, 2>(dyn, g, block, smem, s, S, rays, C, which, hits);
+}
+
 // Enqueue one frame window. In profiling mode (`prof`), every stage kernel is
 // bracketed by CUDA events and its time is added to st->kernel_ms.
 // `adjoint`: per batch, the primal pass leaves every sample's radiance in
@@ -144,7 +188,13 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
     const WfParams<R> *P = (const WfParams<R> *)st->params;
     WfCounters *C = st->counters;
     const int g = st->grid;
+    // tree width of the traversal stages; the pass-through shadow walk
+    // (pt_occluded_segment) stays on the binary tree
+    const int W = (sizeof(R) == 4 && S.wnodes) ? S.bvh_width : 2;
     const size_t smem = (size_t)(S.stack_depth > 0 ? S.stack_depth : 1) * block * sizeof(int);
+    const size_t smem_w = W == 2 ? smem : (size_t)S.wide_stack_depth * block * sizeof(int);
+    const int Ws = S.has_passthrough ? 2 : W;
+    const size_t smem_s = Ws == 2 ? smem : smem_w;
     int ev = 0;
     auto tic = [&]() {
         if (prof) cudaEventRecord(st->kev[ev & 63], s);
@@ -172,10 +222,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         int which = 0;
         for (int b = 0; b <= depth; ++b) {
             tic();
-            if (dyn)
-                k_wf_extend_dyn<R><<<g, block, smem, s>>>(S, rays[which], C, which, hits);
-            else
-                k_wf_extend<R><<<g, block, smem, s>>>(S, rays[which], C, which, hits);
+            launch_extend_w<R>(W, dyn, g, block, smem_w, s, S, rays[which], C, which, hits);
             toc(0);
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
             // shadow_count, shadow_fetch and ray_fetch (the next extend's)
@@ -190,15 +237,10 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             }
             toc(1);
             tic();
-            const bool dyn_shadow = dyn && !S.has_passthrough;
-            if (replay && dyn_shadow)
-                k_wf_shadow_dyn<R, true><<<g, block, smem, s>>>(S, sq, C, nee, A.att);
-            else if (replay)
-                k_wf_shadow<R, true><<<g, block, smem, s>>>(S, sq, C, nee, A.att);
-            else if (dyn_shadow)
-                k_wf_shadow_dyn<R, false><<<g, block, smem, s>>>(S, sq, C, nee, nullptr);
+            if (replay)
+                launch_shadow_w<R, true>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, A.att);
             else
-                k_wf_shadow<R, false><<<g, block, smem, s>>>(S, sq, C, nee, nullptr);
+                launch_shadow_w<R, false>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, nullptr);
             toc(2);
             which ^= 1;
         }
@@ -250,7 +292,7 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_extend<R>, block,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_extend<R, 2>, block,
                                                       (size_t)(S.stack_depth > 0 ? S.stack_depth : 1) * block * 4);
         if (per_sm < 1) per_sm = 1;
         st->grid = sms * per_sm;

@@ -111,3 +111,31 @@ def test_dynamic_fetch_traversal_gives_identical_images(mtlib):
         imgs.append(acc.cpu())
         g.release()
     assert torch.equal(imgs[0], imgs[1])
+
+
+@pytest.mark.parametrize("width", [4, 8])
+def test_wide_bvh_gives_identical_images(mtlib, width):
+    """The 4- and 8-wide trees are collapsed from the binary tree with the
+    same leaves; nearest hits keep the lowest-prim tie-break, so the images
+    are bit-identical to the binary tree's (grid-stride and dynamic fetch)."""
+    import torch
+
+    d = scenes.torus_field_scene(n_instances=64)
+    W, H, SPP, DEPTH = 96, 64, 4, 6
+    cam = d.make_camera(W, H)
+    imgs = []
+    for bw, trav in ((2, 1), (width, 1), (width, 2)):
+        g = mt.GpuScene(d, precision="fp32", integrator="wavefront", traversal=trav, bvh_width=bw)
+        acc = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
+        rc = g.lib.mt_render_accumulate_device(g.h, cam.ref, W, H, 0, SPP, DEPTH, 0, acc.data_ptr(), 0,
+                                               torch.cuda.current_stream().cuda_stream)
+        assert rc == 0
+        torch.cuda.synchronize()
+        imgs.append(acc.cpu())
+        g.release()
+    assert torch.equal(imgs[0], imgs[1]) and torch.equal(imgs[0], imgs[2])
+
+
+def test_bvh_width_must_be_2_4_or_8(mtlib):
+    with pytest.raises(RuntimeError):
+        mt.GpuScene(scenes.spheres_scene(n_spheres=8), bvh_width=3)
