@@ -322,6 +322,44 @@ int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_camera *cam, i
                                         int spp_begin, int spp_end, int max_depth, float *accum_dev,
                                         int accumulate, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Batched rendering: many images in one CUDA-graph launch             */
+/* ------------------------------------------------------------------ */
+
+/*
+ * A batch context owns `lanes` sets of wavefront queues of `queue_capacity`
+ * path slots each (0 = 2M). mt_batch_render spreads the items over the lanes
+ * (longest first, by pixels x samples x bounces) and renders all of them with
+ * ONE graph launch on `stream`: each lane renders its items in turn, the lanes
+ * run concurrently. The graph is captured on the first call and reused while
+ * the item list keeps its shape (scenes, sizes, windows, depths); cameras and
+ * output pointers may change between calls. Scenes must be FP32 and on the
+ * batch's device; their integrator option does not matter (the wavefront
+ * stages are used). No counterpart in the reference, whose CLI renders one
+ * image per process.
+ */
+typedef struct mt_batch mt_batch;
+
+typedef struct {
+    mt_scene *scene;
+    const mt_camera *cam;
+    int32_t width, height;
+    int32_t s0;           /* first sample of the window                      */
+    int32_t spp;          /* samples per pixel [s0, s0 + spp)                */
+    int32_t depth;        /* max bounces                                     */
+    int32_t pad;
+    float *out_dev;       /* device, height x width x 3: mean linear RGB     */
+} mt_batch_item;
+
+int mt_batch_create(int32_t lanes, int32_t queue_capacity, int32_t device, mt_batch **out);
+void mt_batch_release(mt_batch *batch);
+
+/* item_ms (optional, n floats): each item's completion time after the
+ * launch's first node; total_ms (optional): the whole launch. Either one
+ * makes the call wait for the launch to finish. */
+int mt_batch_render(mt_batch *batch, int32_t n, const mt_batch_item *items, void *stream, float *item_ms,
+                    float *total_ms);
+
 /* Per-launch statistics of the last render on this scene. */
 typedef struct {
     double  kernel_ms;        /* device time of the render kernels (CUDA events) */

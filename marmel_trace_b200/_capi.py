@@ -152,6 +152,20 @@ class MtOptions(C.Structure):
     ]
 
 
+class MtBatchItem(C.Structure):
+    _fields_ = [
+        ("scene", C.c_void_p),
+        ("cam", C.c_void_p),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("s0", C.c_int32),
+        ("spp", C.c_int32),
+        ("depth", C.c_int32),
+        ("pad", C.c_int32),
+        ("out_dev", C.c_void_p),
+    ]
+
+
 class MtSceneInfo(C.Structure):
     _fields_ = [
         ("prim_count", C.c_int32),
@@ -202,6 +216,9 @@ SIGNATURES = {
     "mt_render_linear": (I, [P, P, I, I, I, I, I, P]),
     "mt_render_accumulate_device": (I, [P, P, I, I, I, I, I, I, P, I, P]),
     "mt_render_accumulate_device_noalloc": (I, [P, P, I, I, I, I, I, P, I, P]),
+    "mt_batch_create": (I, [I, I, I, P]),
+    "mt_batch_release": (None, [P]),
+    "mt_batch_render": (I, [P, I, P, P, P, P]),
     "mt_get_stats": (I, [P, P]),
     "mt_set_counting": (I, [P, I]),
     "mt_pathtrace_radiance": (I, [P, I, P, P, I, P, P]),

@@ -35,6 +35,7 @@ UNITS = [
     ("mt_wavefront.cu", []),
     ("mt_wavefront_f64.cu", ["--fmad=false"]),
     ("mt_noalloc.cu", []),
+    ("mt_batch.cu", []),
     ("mt_adjoint.cu", []),
     ("mt_adjoint_f64.cu", ["--fmad=false"]),
     ("mt_bvh.cpp", []),

@@ -83,6 +83,22 @@ inline void wf_free(WavefrontState *st)
     st->acc_pixels = 0;
 }
 
+// Batch size of a window of `spp` samples over `wh` pixels: the largest
+// divisor of spp whose paths fit the queue capacity (default 8M path slots,
+// at least one sample of every pixel).
+inline void wf_batch_split(int wh, int spp, long long capacity, int *batch_spp, int *n_batches)
+{
+    long long cap = capacity > 0 ? capacity : (8ll << 20);
+    if (cap < wh) cap = wh;
+    *batch_spp = 1;
+    for (int d = spp; d >= 1; --d)
+        if (spp % d == 0 && (long long)wh * d <= cap) {
+            *batch_spp = d;
+            break;
+        }
+    *n_batches = spp / *batch_spp;
+}
+
 // the pinned host staging block of the parameters is 256 bytes
 static_assert(sizeof(WfParams<double>) <= 256 && sizeof(WfParams<float>) <= 256, "parameter block size");
 
@@ -172,9 +188,13 @@ void launch_extend_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_
 //
 // `dyn`: the extend stage, and the shadow stage of scenes without
 // pass-through materials, use the dynamic-fetch traversal kernels.
+//
+// `params` (default: the state's own block) is the device parameter block the
+// kernels read, so several windows can share one state's queues.
 template <typename R>
 int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch_spp, int n_batches, int depth,
-               cudaStream_t s, bool prof, int block, bool adjoint = false, bool dyn = false)
+               cudaStream_t s, bool prof, int block, bool adjoint = false, bool dyn = false,
+               const void *params = nullptr)
 {
     const int wh = w * h;
     const int n_paths = wh * batch_spp;
@@ -185,7 +205,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
     WfShadow<R> *sq = (WfShadow<R> *)st->shadow;
     R *sample_buf = (R *)st->sample_buf;
     R *acc = (R *)st->acc;
-    const WfParams<R> *P = (const WfParams<R> *)st->params;
+    const WfParams<R> *P = (const WfParams<R> *)(params ? params : st->params);
     WfCounters *C = st->counters;
     const int g = st->grid;
     // tree width of the traversal stages; the pass-through shadow walk
@@ -273,16 +293,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     if (!st) st = new WavefrontState();
     const int wh = w * h;
     const int spp = s1 - s0;
-    // Batch size: the largest divisor of the window whose paths fit the queue.
-    long long cap = opts && opts->queue_capacity > 0 ? opts->queue_capacity : (8ll << 20);
-    if (cap < wh) cap = wh;
-    int batch_spp = 1;
-    for (int d = spp; d >= 1; --d)
-        if (spp % d == 0 && (long long)wh * d <= cap) {
-            batch_spp = d;
-            break;
-        }
-    int n_batches = spp / batch_spp;
+    int batch_spp = 1, n_batches = 1;
+    wf_batch_split(wh, spp, opts ? opts->queue_capacity : 0, &batch_spp, &n_batches);
     int rc = wf_reserve<R>(st, (size_t)wh * batch_spp, (size_t)wh, S.light_count);
     if (rc) return rc;
     const bool adjoint = adj != nullptr;

@@ -13,6 +13,9 @@ doubles.
     torus_field_scene (config "C2"): 1920x1080, 64 spp, depth 8; 4096
         instances of a 256-triangle torus (1,048,576 triangles, seed 2), PBR
         GGX materials, 8 emissive sphere lights, ground plane, sun and sky.
+    batch_workload (config "C3"): 64 mixed scenes (seed 3) of uneven
+        triangle count, resolution, spp and depth for one batched launch.
+    adjoint_scene (config "C4"): the inverse-rendering scene.
 """
 from __future__ import annotations
 
@@ -177,6 +180,79 @@ def torus_field_scene(seed: int = 2, n_instances: int = 4096, n_materials: int =
         set_sphere(prims[1 + n_instances * ntri + k], light_pos[k], 0.5, first_light_mat + k)
     return SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=default_sky(),
                      camera=dict(eye=(0.0, 14.0, -62.0), target=(0.0, 0.0, -5.0), up=(0.0, 1.0, 0.0), vfov=50.0))
+
+
+# ---------------------------------------------------------------------
+# C3: batched uneven workload, 64 scenes (seed 3)
+# ---------------------------------------------------------------------
+BATCH_RESOLUTIONS = ((256, 256), (512, 512), (768, 432), (1024, 1024))
+BATCH_SPP = (16, 64, 256)
+
+
+def mixed_scene(rng: np.random.Generator, n_triangles: int) -> SceneDesc:
+    """A random sphere/triangle mix: ~n_triangles in torus instances (256
+    triangles each), 8-40 spheres and a ground plane; Lambert, PBR GGX
+    (metal or dielectric), glass and emissive PBR sphere lights."""
+    mesh = torus_mesh()
+    ntri = len(mesh)
+    n_inst = max(2, int(round(n_triangles / ntri)))
+    area = 12.0 + 1.6 * math.sqrt(n_inst)
+    scale = rng.uniform(0.5, 2.0, n_inst)
+    rot = random_rotations(rng, n_inst)
+    pos = np.stack([rng.uniform(-area / 2, area / 2, n_inst), scale * 0.35 + rng.uniform(0.0, 1.0, n_inst),
+                    rng.uniform(-area / 2, area / 2, n_inst)], axis=1)
+    tv = np.einsum("nij,tkj->ntki", rot, mesh) * scale[:, None, None, None] + pos[:, None, None, :]
+    mats = [material(albedo=(0.5, 0.5, 0.48))]  # ground: Lambert
+    kinds = []
+    for _ in range(12):
+        k = int(rng.integers(0, 3))
+        kinds.append(k)
+        if k == 0:
+            mats.append(material(albedo=tuple(rng.uniform(0.1, 0.9, 3))))
+        elif k == 1:
+            mats.append(material(albedo=tuple(rng.uniform(0.2, 0.9, 3)), metallic=float(rng.uniform() < 0.5),
+                                 roughness=float(rng.uniform(0.05, 0.8)), pbr=1))
+        else:
+            mats.append(glass_material())
+    n_lights = int(rng.integers(1, 9))
+    first_light = len(mats)
+    for _ in range(n_lights):
+        mats.append(light_material(tuple(rng.uniform(0.6, 1.0, 3)), float(rng.uniform(5.0, 20.0))))
+    n_sph = int(rng.integers(8, 41))
+    n = 1 + n_inst * ntri + n_sph + n_lights
+    prims = prims_array(n)
+    set_plane(prims[0], (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 0)
+    tri = prims[1:1 + n_inst * ntri]
+    tri["kind"] = PRIM_TRIANGLE
+    tri["material"] = np.repeat(rng.integers(1, 13, n_inst), ntri)
+    tri["v"] = tv.reshape(-1, 9)
+    base = 1 + n_inst * ntri
+    for k in range(n_sph):
+        r = float(rng.uniform(0.3, 1.2))
+        c = (float(rng.uniform(-area / 2, area / 2)), r, float(rng.uniform(-area / 2, area / 2)))
+        set_sphere(prims[base + k], c, r, int(rng.integers(1, 13)))
+    for k in range(n_lights):
+        c = (float(rng.uniform(-area / 3, area / 3)), float(rng.uniform(2.0, 5.0)), float(rng.uniform(-area / 3, area / 3)))
+        set_sphere(prims[base + n_sph + k], c, 0.4, first_light + k)
+    eye = (0.0, 0.25 * area + 3.0, -0.75 * area - 4.0)
+    return SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=default_sky(),
+                     camera=dict(eye=eye, target=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), vfov=50.0))
+
+
+def batch_workload(seed: int = 3, n: int = 64, spp_scale: float = 1.0) -> list:
+    """The batched uneven workload: `n` scenes with triangle counts
+    log-uniform in [500, 200k], resolution from BATCH_RESOLUTIONS, spp from
+    BATCH_SPP (times spp_scale, at least 1), depth 4-10. Returns dicts with
+    desc, width, height, spp, depth."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        t = int(round(math.exp(rng.uniform(math.log(500.0), math.log(200_000.0)))))
+        w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
+        spp = max(1, int(round(BATCH_SPP[int(rng.integers(0, len(BATCH_SPP)))] * spp_scale)))
+        depth = int(rng.integers(4, 11))
+        out.append(dict(desc=mixed_scene(rng, t), width=w, height=h, spp=spp, depth=depth, triangles=t))
+    return out
 
 
 # ---------------------------------------------------------------------
