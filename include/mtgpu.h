@@ -323,6 +323,43 @@ int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_camera *cam, i
                                         int accumulate, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* Autotuner                                                           */
+/* ------------------------------------------------------------------ */
+
+#define MT_TUNE_MAX_ENTRIES 32
+
+typedef struct {
+    mt_options options;   /* a timed configuration                         */
+    float ms;             /* its probe window, best of two runs            */
+    float pad;
+} mt_tune_entry;
+
+typedef struct {
+    mt_options chosen;    /* the fastest configuration, now set on the scene */
+    float chosen_ms;
+    float default_ms;     /* the library defaults on the same probe         */
+    int32_t n_entries;
+    int32_t pad;
+    mt_tune_entry entries[MT_TUNE_MAX_ENTRIES];
+} mt_tune_report;
+
+/*
+ * Pick the wavefront integrator's configuration for this scene and view by
+ * timing a probe window of `probe_spp` samples per pixel (same samples for
+ * every candidate) on the scene's device. Coordinate descent, each stage
+ * keeping the fastest so far (library defaults first):
+ *   traversal schedule (grid-stride, dynamic fetch), block size (128, 64),
+ *   BVH width (2, 4, 8; wide trees built on first use), sort-by-material
+ *   threshold (off, 256K rays, always), queue capacity (8M, 4M, 2M, 1M).
+ * Every candidate computes the same image (the tests check this), so the
+ * choice only moves time. The scene must be FP32; on return its options are
+ * the chosen ones with the wavefront integrator. Allocates probe buffers;
+ * synchronous. No counterpart in the reference (a single CPU code path).
+ */
+int mt_autotune(mt_scene *scene, const mt_camera *cam, int width, int height, int probe_spp, int max_depth,
+                mt_tune_report *report);
+
+/* ------------------------------------------------------------------ */
 /* Batched rendering: many images in one CUDA-graph launch             */
 /* ------------------------------------------------------------------ */
 

@@ -152,6 +152,15 @@ class MtOptions(C.Structure):
     ]
 
 
+class MtTuneEntry(C.Structure):
+    _fields_ = [("options", MtOptions), ("ms", C.c_float), ("pad", C.c_float)]
+
+
+class MtTuneReport(C.Structure):
+    _fields_ = [("chosen", MtOptions), ("chosen_ms", C.c_float), ("default_ms", C.c_float),
+                ("n_entries", C.c_int32), ("pad", C.c_int32), ("entries", MtTuneEntry * 32)]
+
+
 class MtBatchItem(C.Structure):
     _fields_ = [
         ("scene", C.c_void_p),
@@ -216,6 +225,7 @@ SIGNATURES = {
     "mt_render_linear": (I, [P, P, I, I, I, I, I, P]),
     "mt_render_accumulate_device": (I, [P, P, I, I, I, I, I, I, P, I, P]),
     "mt_render_accumulate_device_noalloc": (I, [P, P, I, I, I, I, I, P, I, P]),
+    "mt_autotune": (I, [P, P, I, I, I, I, P]),
     "mt_batch_create": (I, [I, I, I, P]),
     "mt_batch_release": (None, [P]),
     "mt_batch_render": (I, [P, I, P, P, P, P]),

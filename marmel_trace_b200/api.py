@@ -232,6 +232,22 @@ class GpuScene:
         check(self.lib.mt_render_image(self.h, cam.ref, w, h, spp, depth, ptr(out)), "mt_render_image")
         return out
 
+    def autotune(self, cam: Camera, w: int, h: int, probe_spp: int, depth: int) -> dict:
+        """mt_autotune: time the wavefront configurations on a probe window
+        and keep the fastest on this scene. Returns the chosen options, the
+        probe times and every timed candidate."""
+        rep = capi.MtTuneReport()
+        check(self.lib.mt_autotune(self.h, cam.ref, w, h, probe_spp, depth, C.byref(rep)), "mt_autotune")
+
+        def opts(o):
+            return {"traversal": {0: "static", 1: "static", 2: "dynamic"}[o.traversal], "block": o.block_size,
+                    "bvh_width": o.bvh_width, "sort_threshold": o.sort_threshold,
+                    "queue_capacity": o.queue_capacity or 8 << 20}
+
+        return {"chosen": opts(rep.chosen), "chosen_ms": rep.chosen_ms, "default_ms": rep.default_ms,
+                "candidates": [dict(opts(rep.entries[i].options), ms=round(rep.entries[i].ms, 3))
+                               for i in range(rep.n_entries)]}
+
     def linear(self, cam: Camera, w: int, h: int, spp: int, depth: int, mode: str = "pathtrace") -> np.ndarray:
         out = np.zeros((h, w, 3), np.float32)
         m = capi.MODE_PATHTRACE if mode == "pathtrace" else capi.MODE_WHITTED

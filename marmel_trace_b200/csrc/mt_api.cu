@@ -100,6 +100,11 @@ struct mt_scene {
     mt_sky h_sky;
     std::vector<HostSphere> h_spheres;
     int version = 0;
+    // FP32 binary tree on the host (device layout), and the wide trees
+    // collapsed from it on first use (index 0: 4 children, 1: 8 children)
+    std::vector<float> nodes2;
+    const float4 *wide[2] = {nullptr, nullptr};
+    int wide_depth[2] = {0, 0};
 
     template <typename T> int upload(const std::vector<T> &v, const T **dst)
     {
@@ -331,17 +336,9 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     S->stack_depth = fb.depth + 1;  // pushes happen only on the way down
     S->bvh_width = 2;
     S->wide_stack_depth = 0;
-    const int W = sc->opts.bvh_width;
-    if (sizeof(R) == 4 && (W == 4 || W == 8) && fb.node_count > 0) {
-        std::vector<float> n2(nodes.size() * 4), wide;
-        memcpy(n2.data(), nodes.data(), n2.size() * sizeof(float));
-        int bound = 0;
-        if (collapse_bvh(n2, fb.node_count, W, &wide, &bound)) return fail(MT_ERR_INVALID, "wide BVH collapse");
-        std::vector<float4> wn(wide.size() / 4);
-        memcpy(wn.data(), wide.data(), wide.size() * sizeof(float));
-        if ((rc = sc->upload(wn, &S->wnodes))) return rc;
-        S->bvh_width = W;
-        S->wide_stack_depth = bound + 1;
+    if (sizeof(R) == 4) {
+        sc->nodes2.resize(nodes.size() * 4);
+        if (!nodes.empty()) memcpy(sc->nodes2.data(), nodes.data(), sc->nodes2.size() * sizeof(float));
     }
     S->plane_count = (int)plane_prims.size();
     S->prim_count = n;
@@ -439,6 +436,36 @@ int reset_counters(mt_scene *sc)
 {
     if (!sc->counting) return 0;
     CK(cudaMemset(sc->d_counters, 0, sizeof(DevCounters)), "cudaMemset(counters)");
+    return 0;
+}
+
+// The tree the FP32 traversal kernels walk: the binary tree (W = 2) or a
+// wide tree collapsed from it (W = 4 or 8), built on first use and kept for
+// the scene's lifetime. The FP64 path always walks the binary tree.
+int select_bvh_width(mt_scene *sc, int W)
+{
+    DevScene<float> &S = sc->sf;
+    if (sc->opts.precision != MT_PRECISION_FP32 || W == 2 || S.node_count == 0) {
+        S.bvh_width = 2;
+        S.wnodes = nullptr;
+        S.wide_stack_depth = 0;
+        return 0;
+    }
+    if (W != 4 && W != 8) return fail(MT_ERR_INVALID, "bvh_width %d (2, 4 or 8)", W);
+    const int k = W == 4 ? 0 : 1;
+    if (!sc->wide[k]) {
+        std::vector<float> wide;
+        int bound = 0;
+        if (collapse_bvh(sc->nodes2, S.node_count, W, &wide, &bound)) return fail(MT_ERR_INVALID, "wide BVH collapse");
+        std::vector<float4> wn(wide.size() / 4);
+        memcpy(wn.data(), wide.data(), wide.size() * sizeof(float));
+        int rc = sc->upload(wn, &sc->wide[k]);
+        if (rc) return rc;
+        sc->wide_depth[k] = bound + 1;
+    }
+    S.wnodes = sc->wide[k];
+    S.bvh_width = W;
+    S.wide_stack_depth = sc->wide_depth[k];
     return 0;
 }
 
@@ -621,6 +648,7 @@ int mt_scene_create(const mt_scene_desc *desc, const mt_options *opts, mt_scene 
 
     if (sc->opts.precision == MT_PRECISION_FP64) rc = upload_scene<double>(sc, desc, &sc->sd);
     else rc = upload_scene<float>(sc, desc, &sc->sf);
+    if (!rc) rc = select_bvh_width(sc, sc->opts.bvh_width);
     if (rc) return bail(rc);
     *out = sc;
     return 0;
@@ -797,6 +825,109 @@ int mt_render_accumulate_device(mt_scene *sc, const mt_camera *cam, int w, int h
         return render_dev<double>(sc, cam, w, h, s1, s0, s1, depth, m, out_kind, accum_dev, (cudaStream_t)stream,
                                   false);
     return render_dev<float>(sc, cam, w, h, s1, s0, s1, depth, m, out_kind, accum_dev, (cudaStream_t)stream, false);
+}
+
+int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp, int depth, mt_tune_report *rep)
+{
+    if (!rep) return fail(MT_ERR_NULL, "NULL report");
+    int rc = render_args(sc, cam, rep, w, h, probe_spp, depth);
+    if (rc) return rc;
+    if (sc->opts.precision != MT_PRECISION_FP32) return fail(MT_ERR_UNSUPPORTED, "mt_autotune: FP32 scenes only");
+    if ((rc = set_device(sc))) return rc;
+    memset(rep, 0, sizeof *rep);
+    DevBuf<float> out;
+    CK(out.alloc((size_t)w * h * 3), "cudaMalloc(probe)");
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0), "cudaEventCreate");
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(MT_ERR_LAUNCH, "cudaEventCreate");
+    }
+    const bool counting = sc->counting;
+    sc->counting = false;
+    const mt_options saved = sc->opts;
+    const int s0 = 1 << 20;  // one fixed probe window for every candidate
+    // time one configuration: a warm-up window (captures its graph), then the
+    // better of two timed windows
+    auto probe = [&](const mt_options &o, float *ms) -> int {
+        sc->opts = o;
+        int r = select_bvh_width(sc, o.bvh_width);
+        if (r) return r;
+        float best = 3.0e38f;
+        for (int k = 0; k < 3; ++k) {
+            if (k) CK(cudaEventRecord(e0, 0), "cudaEventRecord");
+            r = render_dev<float>(sc, cam, w, h, s0 + probe_spp, s0, s0 + probe_spp, depth, RENDER_PT, OUT_SUM_F32,
+                                  out.p, 0, false);
+            if (r) return r;
+            if (k) {
+                CK(cudaEventRecord(e1, 0), "cudaEventRecord");
+                CK(cudaEventSynchronize(e1), "probe");
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                best = t < best ? t : best;
+            } else {
+                CK(cudaDeviceSynchronize(), "probe");
+            }
+        }
+        *ms = best;
+        if (rep->n_entries < MT_TUNE_MAX_ENTRIES) {
+            rep->entries[rep->n_entries].options = o;
+            rep->entries[rep->n_entries].ms = best;
+            rep->n_entries++;
+        }
+        return 0;
+    };
+    mt_options cur = saved;
+    cur.integrator = MT_INTEGRATOR_WAVEFRONT;
+    cur.traversal = MT_TRAVERSAL_STATIC;
+    cur.block_size = 128;
+    cur.bvh_width = 2;
+    cur.sort_threshold = 0;
+    cur.queue_capacity = 0;
+    cur.use_graph = 1;
+    float cur_ms = 0.f;
+    rc = probe(cur, &cur_ms);
+    rep->default_ms = cur_ms;
+    // coordinate descent over the knobs, defaults first in each stage
+    for (int stage = 0; stage < 5 && !rc; ++stage) {
+        int vals[4];
+        int nv = 0;
+        switch (stage) {
+        case 0: vals[nv++] = MT_TRAVERSAL_DYNAMIC; break;
+        case 1: vals[nv++] = 64; break;
+        case 2: vals[nv++] = 4; vals[nv++] = 8; break;
+        case 3: vals[nv++] = 1 << 18; vals[nv++] = 1; break;
+        default: vals[nv++] = 4 << 20; vals[nv++] = 2 << 20; vals[nv++] = 1 << 20; break;
+        }
+        for (int i = 0; i < nv && !rc; ++i) {
+            mt_options o = cur;
+            if (stage == 0) o.traversal = vals[i];
+            else if (stage == 1) o.block_size = vals[i];
+            else if (stage == 2) o.bvh_width = vals[i];
+            else if (stage == 3) o.sort_threshold = vals[i];
+            else o.queue_capacity = vals[i];
+            if (stage == 4 && (long long)w * h >= o.queue_capacity) continue;  // one sample per batch already
+            float ms = 0.f;
+            rc = probe(o, &ms);
+            if (!rc && ms < cur_ms) {
+                cur = o;
+                cur_ms = ms;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    sc->counting = counting;
+    if (rc) {
+        sc->opts = saved;
+        select_bvh_width(sc, saved.bvh_width);
+        return rc;
+    }
+    sc->opts = cur;
+    if ((rc = select_bvh_width(sc, cur.bvh_width))) return rc;
+    rep->chosen = cur;
+    rep->chosen_ms = cur_ms;
+    return 0;
 }
 
 int mt_get_stats(const mt_scene *csc, mt_stats *out)

@@ -99,12 +99,17 @@ template <typename R> MT_D V3<R> adj_of_path(const WfParams<R> *P, int slot)
     return v3<R>((R)(a[0] * sc), (R)(a[1] * sc), (R)(a[2] * sc));
 }
 
+// Stage kernels run with 64 or 128 (default) threads per block; the register
+// allocation is tuned for the 128-thread bound.
+static constexpr int kWfMaxBlock = 128;
+
 struct WfCounters {
     int ray_count[2];
     int shadow_count;
     int shadow_fetch;  // next shadow ray handed out by the dynamic-fetch kernel
     int ray_fetch;     // next ray handed out by the dynamic-fetch extend kernel
-    int pad[3];
+    int sorted;        // this bounce's extend results were sorted by material
+    int pad[2];
 };
 
 // Warp-aggregated queue append: one atomicAdd per warp, lanes get
@@ -180,7 +185,7 @@ __global__ void k_wf_generate(const DevScene<R> S, const WfParams<R> *P, int bat
 // extend: nearest hit (scene_intersect, src/scene.c:767 -> src/bvh.c:557)
 // ------------------------------------------------------------------
 template <typename R, int W>
-__global__ void __launch_bounds__(128) k_wf_extend(const DevScene<R> S, const WfRay<R> *rays, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend(const DevScene<R> S, const WfRay<R> *rays, const WfCounters *C,
                                                    int which, WfHit<R> *hits)
 {
     const int n = C->ray_count[which];
@@ -245,11 +250,19 @@ MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> 
 // the remaining radiance L - radiance; emission and sky terms are taken
 // where they occur. The radiance bookkeeping is the primal pass's, so the
 // replay reproduces it exactly.
+//
+// When the bounce's extend results were sorted by material (C->sorted), the
+// kernel reads the sorted copies instead.
 template <typename R, bool ADJ>
-__global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
                                                   WfCounters *C, int which, int b, int max_depth, WfPath<R> *paths,
-                                                  R *nee, WfRay<R> *rays_out, WfShadow<R> *sq, WfAdj<R> A)
+                                                  R *nee, WfRay<R> *rays_out, WfShadow<R> *sq, WfAdj<R> A,
+                                                  const WfRay<R> *sorted_rays, const WfHit<R> *sorted_hits)
 {
+    if (!ADJ && sorted_rays && C->sorted) {
+        rays_in = sorted_rays;
+        hits = sorted_hits;
+    }
     __shared__ float adj_g[ADJ ? kAdjMaxParams : 1];
     const AdjCtx ctx{adj_g, kParamsPerMaterial * S.material_count};
     if constexpr (ADJ) adj_block_begin(adj_g, A.P);
@@ -473,12 +486,90 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene<R> S, const WfR
 }
 
 // ------------------------------------------------------------------
+// sort by material: a counting sort of one bounce's extend results by the
+// material hit (bucket M = no surface), so that the shade kernel's warps see
+// one material, hence one BSDF code path, at a time. It runs only when the
+// queue holds at least `threshold` rays (decided on the device). Queue order
+// never changes a path's result: every path keeps its own slot, NEE slots and
+// sample index. Lanes of a warp with the same key share one atomicAdd.
+// ------------------------------------------------------------------
+MT_D int warp_add_by_key(int *counters, int key, bool want)
+{
+    const unsigned active = __ballot_sync(0xffffffffu, want);
+    if (!want) return 0;
+    const unsigned peers = __match_any_sync(active, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&counters[key], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+template <typename R>
+__global__ void k_wf_sort_count(const DevScene<R> S, WfCounters *C, int which, const WfHit<R> *hits, int *keys,
+                                int *buckets, int threshold)
+{
+    const int n = C->ray_count[which];
+    if (blockIdx.x == 0 && threadIdx.x == 0) C->sorted = n >= threshold;
+    if (n < threshold) return;
+    const int M = S.material_count;
+    const int stride = gridDim.x * blockDim.x;
+    const int n_round = (n + stride - 1) / stride * stride;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
+        int key = M;
+        if (q < n) {
+            const int prim = hits[q].prim;
+            if (prim >= 0) {
+                const int m = __ldg(S.prim_info + prim).y;
+                if (m >= 0 && m < M) key = m;
+            }
+            keys[q] = key;
+        }
+        warp_add_by_key(buckets, key, q < n);
+    }
+}
+
+// exclusive scan of the bucket counts into the cursors (one thread: the
+// bucket count is the material count + 1)
+template <typename R> __global__ void k_wf_sort_scan(const DevScene<R> S, const WfCounters *C, int *buckets)
+{
+    if (!C->sorted || threadIdx.x != 0) return;
+    const int nb = S.material_count + 1;
+    int acc = 0;
+    for (int k = 0; k < nb; ++k) {
+        buckets[nb + k] = acc;
+        acc += buckets[k];
+    }
+}
+
+template <typename R>
+__global__ void k_wf_sort_scatter(const DevScene<R> S, const WfCounters *C, int which, const WfRay<R> *rays,
+                                  const WfHit<R> *hits, const int *keys, int *buckets, WfRay<R> *sorted_rays,
+                                  WfHit<R> *sorted_hits)
+{
+    if (!C->sorted) return;
+    const int n = C->ray_count[which];
+    int *cursors = buckets + S.material_count + 1;
+    const int stride = gridDim.x * blockDim.x;
+    const int n_round = (n + stride - 1) / stride * stride;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
+        const int key = q < n ? keys[q] : 0;
+        const int pos = warp_add_by_key(cursors, key, q < n);
+        if (q < n) {
+            sorted_rays[pos] = rays[q];
+            sorted_hits[pos] = hits[q];
+        }
+    }
+}
+
+// ------------------------------------------------------------------
 // shadow: pt_occluded_segment (src/pathtrace.c:504-532) per NEE connection
 // ------------------------------------------------------------------
 // ADJ: also keep the connection's transmittance (zero when it adds no light)
 // for the replay's gradient terms.
 template <typename R, bool ADJ, int W>
-__global__ void __launch_bounds__(128) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
                                                    R *nee, R *att)
 {
     const int n = C->shadow_count;
@@ -553,7 +644,7 @@ MT_D int fetch_round(int *counter, int n, bool idle, bool busy_lane, bool *more)
 }
 
 template <typename R, int W>
-__global__ void __launch_bounds__(128) k_wf_extend_dyn(const DevScene<R> S, const WfRay<R> *rays, WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend_dyn(const DevScene<R> S, const WfRay<R> *rays, WfCounters *C,
                                                        int which, WfHit<R> *hits)
 {
     const int n = C->ray_count[which];
@@ -592,7 +683,7 @@ __global__ void __launch_bounds__(128) k_wf_extend_dyn(const DevScene<R> S, cons
 // Shadow rays of a scene without pass-through materials: a pure any-hit
 // query per connection (see k_wf_shadow).
 template <typename R, bool ADJ, int W>
-__global__ void __launch_bounds__(128) k_wf_shadow_dyn(const DevScene<R> S, const WfShadow<R> *sq, WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_dyn(const DevScene<R> S, const WfShadow<R> *sq, WfCounters *C,
                                                        R *nee, R *att)
 {
     const int n = C->shadow_count;

@@ -36,6 +36,11 @@ struct WavefrontState {
     void *adj_verts = nullptr, *adj_att = nullptr;
     cudaGraphExec_t adj_exec = nullptr;
     std::string adj_key;
+    // sort by material: sorted copies of a bounce's rays and hits, keys, and
+    // bucket counts + cursors (2 x buckets ints)
+    void *sorted_rays = nullptr, *sorted_hits = nullptr, *sort_keys = nullptr, *sort_buckets = nullptr;
+    int sort_bucket_cap = 0;
+    int grid_block = 0;        // block size the persistent grid was sized for
     int grid = 0;              // persistent grid (blocks) of the stage kernels
     cudaEvent_t kev[64];       // per-kernel timing events (profiling mode)
     bool kev_init = false;
@@ -65,8 +70,9 @@ inline int fail(int code, const char *what, cudaError_t e)
 
 inline void wf_free(WavefrontState *st)
 {
-    void **bufs[] = {&st->paths, &st->rays[0], &st->rays[1], &st->hits,      &st->nee,      &st->shadow,
-                     &st->sample_buf, &st->acc, &st->params, &st->adj_verts, &st->adj_att};
+    void **bufs[] = {&st->paths,       &st->rays[0],    &st->rays[1],     &st->hits,        &st->nee,
+                     &st->shadow,      &st->sample_buf, &st->acc,         &st->params,      &st->adj_verts,
+                     &st->adj_att,     &st->sorted_rays, &st->sorted_hits, &st->sort_keys, &st->sort_buckets};
     for (void **b : bufs) {
         if (*b) cudaFree(*b);
         *b = nullptr;
@@ -81,6 +87,7 @@ inline void wf_free(WavefrontState *st)
     st->adj_key.clear();
     st->cap_paths = 0;
     st->acc_pixels = 0;
+    st->sort_bucket_cap = 0;
 }
 
 // Batch size of a window of `spp` samples over `wh` pixels: the largest
@@ -180,6 +187,23 @@ void launch_extend_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_
     launch_extend<R, 2>(dyn, g, block, smem, s, S, rays, C, which, hits);
 }
 
+// Buffers of the sort-by-material stage for `buckets` keys.
+template <typename R> int wf_reserve_sort(WavefrontState *st, int buckets)
+{
+    if (!st->sorted_rays) {
+        WF_CK(cudaMalloc(&st->sorted_rays, st->cap_paths * sizeof(WfRay<R>)), "cudaMalloc(sorted rays)");
+        WF_CK(cudaMalloc(&st->sorted_hits, st->cap_paths * sizeof(WfHit<R>)), "cudaMalloc(sorted hits)");
+        WF_CK(cudaMalloc(&st->sort_keys, st->cap_paths * sizeof(int)), "cudaMalloc(sort keys)");
+    }
+    if (st->sort_bucket_cap < buckets) {
+        if (st->sort_buckets) cudaFree(st->sort_buckets);
+        st->sort_buckets = nullptr;
+        WF_CK(cudaMalloc(&st->sort_buckets, 2 * (size_t)buckets * sizeof(int)), "cudaMalloc(sort buckets)");
+        st->sort_bucket_cap = buckets;
+    }
+    return 0;
+}
+
 // Enqueue one frame window. In profiling mode (`prof`), every stage kernel is
 // bracketed by CUDA events and its time is added to st->kernel_ms.
 // `adjoint`: per batch, the primal pass leaves every sample's radiance in
@@ -194,7 +218,7 @@ void launch_extend_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_
 template <typename R>
 int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch_spp, int n_batches, int depth,
                cudaStream_t s, bool prof, int block, bool adjoint = false, bool dyn = false,
-               const void *params = nullptr)
+               const void *params = nullptr, int sort_threshold = 0)
 {
     const int wh = w * h;
     const int n_paths = wh * batch_spp;
@@ -247,13 +271,28 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
             // shadow_count, shadow_fetch and ray_fetch (the next extend's)
             WF_CK(cudaMemsetAsync(&C->shadow_count, 0, 3 * sizeof(int), s), "memset(shadow_count)");
+            const bool sort = sort_threshold > 0 && !replay && st->sorted_rays;
+            if (sort) {
+                const int nb = S.material_count + 1;
+                WF_CK(cudaMemsetAsync(st->sort_buckets, 0, 2 * (size_t)nb * sizeof(int), s), "memset(buckets)");
+                tic();
+                k_wf_sort_count<R><<<g, block, 0, s>>>(S, C, which, hits, (int *)st->sort_keys,
+                                                       (int *)st->sort_buckets, sort_threshold);
+                k_wf_sort_scan<R><<<1, 32, 0, s>>>(S, C, (int *)st->sort_buckets);
+                k_wf_sort_scatter<R><<<g, block, 0, s>>>(S, C, which, rays[which], hits, (const int *)st->sort_keys,
+                                                         (int *)st->sort_buckets, (WfRay<R> *)st->sorted_rays,
+                                                         (WfHit<R> *)st->sorted_hits);
+                toc(3);
+            }
             tic();
             if (replay) {
                 k_wf_shade<R, true><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
-                                                        rays[which ^ 1], sq, A);
+                                                        rays[which ^ 1], sq, A, nullptr, nullptr);
             } else {
                 k_wf_shade<R, false><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
-                                                         rays[which ^ 1], sq, none);
+                                                         rays[which ^ 1], sq, none,
+                                                         sort ? (const WfRay<R> *)st->sorted_rays : nullptr,
+                                                         (const WfHit<R> *)st->sorted_hits);
             }
             toc(1);
             tic();
@@ -299,8 +338,11 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     if (rc) return rc;
     const bool adjoint = adj != nullptr;
     if (adjoint && (rc = wf_reserve_adj<R>(st))) return rc;
-    int block = 128;
-    if (!st->grid) {
+    const int block = (opts && opts->block_size == 64) ? 64 : 128;
+    const int sort_threshold = (!adjoint && opts && opts->sort_threshold > 0) ? opts->sort_threshold : 0;
+    if (sort_threshold && (rc = wf_reserve_sort<R>(st, S.material_count + 1))) return rc;
+    if (!st->grid || st->grid_block != block) {
+        st->grid_block = block;
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -337,7 +379,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     cudaStreamSynchronize(stream);  // the pinned block may still be in use by a previous copy
     memcpy(st->h_params, &hp, sizeof hp);
     WF_CK(cudaMemcpyAsync(st->params, st->h_params, sizeof hp, cudaMemcpyHostToDevice, stream), "params copy");
-    int kernels_per_window = adjoint ? n_batches * 2 * (3 * (depth + 1) + 2) : n_batches * (3 * (depth + 1) + 3);
+    int kernels_per_window = adjoint ? n_batches * 2 * (3 * (depth + 1) + 2)
+                                     : n_batches * ((3 + (sort_threshold ? 3 : 0)) * (depth + 1) + 3);
     cudaGraphExec_t &exec = adjoint ? st->adj_exec : st->exec;
     // dynamic fetch reorders rays across lanes: on coherent queues (primary
     // rays, NEE rays grouped by light) the grid-stride kernels are faster, so
@@ -348,15 +391,16 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         char key[256];
         // the scene travels by value in the captured kernel parameters, so
         // its identity, counters and parameter version are part of the key
-        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d", (int)sizeof(R), w, h, batch_spp, n_batches, depth,
-                 (const void *)S.nodes, (const void *)S.counters, S.version, (int)dyn);
+        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d:%d:%d:%d", (int)sizeof(R), w, h, batch_spp, n_batches,
+                 depth, (const void *)S.nodes, (const void *)S.counters, S.version, (int)dyn, block, sort_threshold,
+                 S.bvh_width);
         if (!exec || exec_key != key) {
             if (exec) cudaGraphExecDestroy(exec);
             exec = nullptr;
             if (!st->cap_stream) WF_CK(cudaStreamCreateWithFlags(&st->cap_stream, cudaStreamNonBlocking), "stream");
             WF_CK(cudaStreamBeginCapture(st->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
             int erc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, st->cap_stream, false, block, adjoint,
-                                    dyn);
+                                    dyn, nullptr, sort_threshold);
             cudaGraph_t graph = nullptr;
             cudaError_t ce = cudaStreamEndCapture(st->cap_stream, &graph);
             if (erc) {
@@ -371,7 +415,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         }
         WF_CK(cudaGraphLaunch(exec, stream), "graph launch");
     } else {
-        rc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, stream, prof, block, adjoint, dyn);
+        rc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, stream, prof, block, adjoint, dyn, nullptr,
+                           sort_threshold);
         if (rc) return rc;
     }
     if (ev1) WF_CK(cudaEventRecord(ev1, stream), "cudaEventRecord");

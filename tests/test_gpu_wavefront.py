@@ -139,3 +139,42 @@ def test_wide_bvh_gives_identical_images(mtlib, width):
 def test_bvh_width_must_be_2_4_or_8(mtlib):
     with pytest.raises(RuntimeError):
         mt.GpuScene(scenes.spheres_scene(n_spheres=8), bvh_width=3)
+
+
+def _acc_image(g, cam, W, H, SPP, DEPTH, s0=0):
+    acc = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
+    rc = g.lib.mt_render_accumulate_device(g.h, cam.ref, W, H, s0, s0 + SPP, DEPTH, 0, acc.data_ptr(), 0,
+                                           torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    return acc.cpu()
+
+
+@pytest.mark.parametrize("opts", [dict(sort_threshold=1), dict(sort_threshold=1 << 30), dict(block_size=64),
+                                  dict(sort_threshold=1, block_size=64, bvh_width=4)])
+def test_tuning_knobs_give_identical_images(mtlib, opts):
+    """Sorting by material reorders the shade queue, the block size changes
+    the persistent grid; neither changes any path's result."""
+    d = scenes.spheres_scene()  # Lambert, metal and glass: several BSDF code paths
+    W, H, SPP, DEPTH = 80, 60, 4, 6
+    cam = d.make_camera(W, H)
+    g0 = mt.GpuScene(d, integrator="wavefront")
+    ref = _acc_image(g0, cam, W, H, SPP, DEPTH)
+    g0.release()
+    g = mt.GpuScene(d, integrator="wavefront", **opts)
+    assert torch.equal(_acc_image(g, cam, W, H, SPP, DEPTH), ref)
+    g.release()
+
+
+def test_autotune_keeps_the_image(mtlib):
+    d = scenes.torus_field_scene(n_instances=256)
+    W, H, DEPTH = 160, 96, 6
+    cam = d.make_camera(W, H)
+    g = mt.GpuScene(d, integrator="wavefront")
+    ref = _acc_image(g, cam, W, H, 4, DEPTH)
+    rep = g.autotune(cam, W, H, 2, DEPTH)
+    assert rep["chosen_ms"] <= rep["default_ms"] + 1e-6
+    assert len(rep["candidates"]) >= 8
+    assert rep["chosen"]["bvh_width"] in (2, 4, 8) and rep["chosen"]["block"] in (64, 128)
+    assert torch.equal(_acc_image(g, cam, W, H, 4, DEPTH), ref)
+    g.release()
