@@ -14,10 +14,14 @@ plain_gpu    : the same frames through the megakernel (one thread per pixel,
 e2e          : the same metric through the drop-in entry point
                mt_pathtrace_render (camera from host memory, RGB8 image read
                back to host memory every step).
-roofline     : dominant kernel (nearest-hit traversal: the wavefront's extend
-               stage) against the measured HBM copy bandwidth, canonical BVH2
-               accounting per ray: 64 B per node pair, 48 B per triangle,
-               16 B per other primitive, 48 B of ray + hit record.
+roofline     : dominant kernel (any-hit traversal: the wavefront's shadow
+               stage; the extend stage beside it) against the measured HBM
+               copy bandwidth, canonical accounting per ray: one node record
+               per visit (64 B binary), 48 B per triangle, 16 B per other
+               primitive, 48 B of ray + hit record.
+autotune     : mt_autotune's choice for this scene and view (4-spp probe),
+               used by the timed frames.
+batch        : the batched uneven workload (64 scenes) in one graph launch.
 time_to_rmse : both integrators evaluate the same unbiased estimator with the
                same random streams, so linear-RGB RMSE after N samples per
                pixel is sqrt(mean sigma^2 / N); N* = mean(sigma^2) / 1e-6 and
@@ -124,13 +128,22 @@ def build_scene():
     return scenes.torus_field_scene()
 
 
-def traversal_bytes(st, kind: str) -> float:
-    """Canonical BVH2 bytes of the counted launch (nearest-hit or any-hit)."""
+# DRAM bytes (read + write) per path sample of the stage kernels, from an ncu
+# launch list of this workload (4-spp frames, 2M-slot queue; summarised under
+# profiles/): 26.54 GB (shadow) and 6.09 GB (extend) over 7 frames of
+# 4 x 2,073,600 samples.
+TRAFFIC_BYTES_PER_SAMPLE = {"shadow": 26.54e9 / (7 * 4 * 2073600), "extend": 6.09e9 / (7 * 4 * 2073600)}
+
+
+def traversal_bytes(st, kind: str, width: int = 2) -> float:
+    """Canonical bytes of the counted launch (nearest-hit or any-hit): one
+    node record per visit (64 B binary, 128 / 256 B for 4 / 8 children)."""
     if kind == "nearest":
         nodes, prims, tris, rays = st.node_visits, st.prim_tests, st.tri_tests, st.extension_rays
     else:
         nodes, prims, tris, rays = st.any_node_visits, st.any_prim_tests, st.any_tri_tests, st.shadow_rays
-    return 64.0 * nodes + 48.0 * tris + 16.0 * (prims - tris) + 48.0 * rays
+    node_bytes = {2: 64.0, 4: 128.0, 8: 256.0}[width]
+    return node_bytes * nodes + 48.0 * tris + 16.0 * (prims - tris) + 48.0 * rays
 
 
 class Frames:
@@ -189,6 +202,15 @@ def run_ours(args):
     qopt = {"queue_capacity": args.queue_capacity} if args.queue_capacity else {}
     g = mt.GpuScene(desc, precision="fp32", integrator=args.integrator, device=local, **qopt)
     fr = Frames(g, cam, SPP, torch)
+
+    # autotuner (untimed): the wavefront configuration for this scene and view,
+    # chosen on a 4-spp probe window and kept on the scene for the timed frames
+    tune = None
+    if args.integrator == "wavefront" and not args.no_autotune:
+        tune = g.autotune(cam, W, H, 4, DEPTH)
+        ch = tune["chosen"]
+        qopt = {"queue_capacity": ch["queue_capacity"], "traversal": 2 if ch["traversal"] == "dynamic" else 1,
+                "block_size": ch["block"], "bvh_width": ch["bvh_width"], "sort_threshold": ch["sort_threshold"]}
 
     # counting pass (untimed): rays, node pairs and primitive tests per sample
     g.set_counting(True)
@@ -258,6 +280,11 @@ def run_ours(args):
     if not args.no_adjoint:
         adjoint = adjoint_bench(torch, local, flush)
 
+    # batched uneven workload: 64 scenes in one graph launch
+    batch = None
+    if not args.no_batch:
+        batch = batch_bench(torch, local)
+
     # time to RMSE 1e-3
     ttr = None
     if len(means) >= 3:
@@ -274,22 +301,29 @@ def run_ours(args):
 
     peak, peak_kind = peaks()
     rays_per_sample = (cnt.extension_rays + cnt.shadow_rays) / n_counted
+    secondary = None
+    traffic = None
+    bw = qopt.get("bvh_width", 2) or 2
     if stage:
-        alg = traversal_bytes(cnt, "nearest") * (W * H * SPP) / n_counted
-        achieved = alg / (stage["extend_ms"] / 1e3) / 1e9
-        kernel = "k_wf_extend<float> (nearest-hit traversal; per-stage CUDA events over one 64-spp frame)"
-        per_launch = alg / stage["extend_launches"]
+        # dominant stage kernel: the shadow (any-hit) stage on this workload
+        dom = "shadow" if stage["shadow_ms"] >= stage["extend_ms"] else "extend"
+        other = "extend" if dom == "shadow" else "shadow"
+        kinds = {"shadow": ("any", "k_wf_shadow<float> (any-hit traversal per NEE connection)"),
+                 "extend": ("nearest", "k_wf_extend<float> (nearest-hit traversal)")}
+        alg = traversal_bytes(cnt, kinds[dom][0], bw) * (W * H * SPP) / n_counted
+        achieved = alg / (stage[f"{dom}_ms"] / 1e3) / 1e9
+        kernel = kinds[dom][1] + "; per-stage CUDA events over one frame"
+        per_launch = alg / stage[f"{dom}_launches"]
+        traffic = TRAFFIC_BYTES_PER_SAMPLE[dom] * W * H * SPP / stage[f"{dom}_launches"]
+        alg2 = traversal_bytes(cnt, kinds[other][0], bw) * (W * H * SPP) / n_counted
+        secondary = {"kernel": kinds[other][1], "achieved": round(alg2 / (stage[f"{other}_ms"] / 1e3) / 1e9, 1),
+                     "frac": round(alg2 / (stage[f"{other}_ms"] / 1e3) / 1e9 / peak, 4),
+                     "traffic": round(TRAFFIC_BYTES_PER_SAMPLE[other] * W * H * SPP / stage[f"{other}_launches"])}
     else:
         alg = (traversal_bytes(cnt, "nearest") + traversal_bytes(cnt, "any")) * (W * H * SPP) / n_counted
         achieved = alg / (sum(ms) / 1e3 / args.steps) / 1e9
         kernel = "k_render<float, PT> (megakernel)"
         per_launch = alg
-    traffic = None
-    tf = ROOT / "profiles" / "traffic_bytes_per_sample.json"
-    if tf.exists():
-        tv = json.loads(tf.read_text()).get(args.integrator)
-        if tv:
-            traffic = tv * W * H * SPP / (stage["extend_launches"] if stage else 1)
 
     out = {
         "metric": METRIC,
@@ -306,18 +340,24 @@ def run_ours(args):
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": SPP, "depth": DEPTH,
                    "integrator": args.integrator, "parallelism": f"replicas x{world}",
-                   "queue_capacity": args.queue_capacity or 8 << 20,
+                   "queue_capacity": qopt.get("queue_capacity") or 8 << 20,
+                   "tuned": tune["chosen"] if tune else None,
                    "l2": "flushed between timed steps (256 MB write); the 90 MB scene fits in L2"},
         "plain_gpu_msamples_s": round(plain, 3) if plain else None,
         "mrays_per_s": round(value * rays_per_sample, 2),
         "rays_per_sample": round(rays_per_sample, 3),
         "time_to_rmse": ttr,
         "adjoint": adjoint,
+        "autotune": tune,
+        "batch": batch,
         "stage_ms": stage,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                     "kernel": kernel, "algorithmic_bytes_per_launch": per_launch},
+                     "kernel": kernel, "algorithmic_bytes_per_launch": per_launch,
+                     "traffic_source": "ncu launch list of the stage kernels (profiles/): DRAM read + "
+                                       "write per sample x samples per launch",
+                     "second_kernel": secondary},
         "e2e": {"value": round(e2e_val, 3) if e2e_val else None, "unit": "Msamples/s", "h2d_bytes_per_step": 128,
                 "d2h_bytes_per_step": W * H * 3, "entry_point": "mt_pathtrace_render"},
         "gpu_launches": launches * args.steps,
@@ -372,6 +412,40 @@ def adjoint_bench(torch, device: int, flush, steps: int = 3):
             "method": "path replay, wavefront form: per batch a primal pass records each sample's radiance, "
                       "then a replay pass re-traces the same paths from their random streams with the stage "
                       "kernels and accumulates the gradient"}
+
+
+def batch_bench(torch, device: int, lanes: int = 16):
+    """The batched uneven workload (64 scenes, seed 3): every image rendered
+    by ONE graph launch, with `lanes` concurrent queue sets and with a single
+    lane (the images one after another, same launch shape)."""
+    from marmel_trace_b200 import scenes
+    from marmel_trace_b200.api import GpuScene
+    from marmel_trace_b200.batch import BatchRenderer
+
+    wl = scenes.batch_workload(seed=3, n=64)
+    gs = [GpuScene(it["desc"], precision="fp32", integrator="wavefront", device=device) for it in wl]
+    cams = [it["desc"].make_camera(it["width"], it["height"]) for it in wl]
+    items = [(g, c, it["width"], it["height"], it["spp"], it["depth"]) for g, c, it in zip(gs, cams, wl)]
+    samples = sum(it["width"] * it["height"] * it["spp"] for it in wl)
+    out = {"workload": "64 scenes (seed 3): 500-200k triangles (log-uniform) + 8-40 spheres, resolution from "
+                       "256^2/512^2/768x432/1024^2, spp from 16/64/256, depth 4-10, Lambert/GGX/glass/emissive",
+           "samples": samples}
+    imgs = None
+    for nl in (1, lanes):
+        br = BatchRenderer(lanes=nl, device=device)
+        imgs, _, _ = br.render(items, out=imgs)  # capture + warm-up
+        _, item_ms, total = br.render(items, out=imgs)
+        br.release()
+        item_ms = sorted(item_ms)
+        out[f"lanes_{nl}"] = {"ms": round(total, 1), "msamples_s": round(samples / total / 1e3, 2),
+                              "item_ms_median": round(statistics.median(item_ms), 1),
+                              "item_ms_p90": round(item_ms[int(0.9 * (len(item_ms) - 1))], 1),
+                              "item_ms_max": round(item_ms[-1], 1)}
+        torch.cuda.empty_cache()
+    out["speedup_lanes"] = round(out["lanes_1"]["ms"] / out[f"lanes_{lanes}"]["ms"], 3)
+    for g in gs:
+        g.release()
+    return out
 
 
 def cpu_baseline(desc, cam, spp: int):
@@ -448,6 +522,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--queue-capacity", type=int, default=0,
                     help="path slots per wavefront batch (0: the library default, 8M)")
     args = ap.parse_args()
