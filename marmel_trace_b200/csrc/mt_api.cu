@@ -795,13 +795,88 @@ int mt_render_image(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, i
     return render_host(sc, cam, w, h, spp, depth, RENDER_WHITTED, OUT_RGB8, rgb);
 }
 
+}  // extern "C"
+
+namespace {
+
+// render_image_adaptive (src/render.c:1382-1500) on the device: pass 0 over
+// every pixel, then refinement passes over the pixels the active-set kernel
+// flags, until none is flagged or the pass bound is reached; the host reads
+// only the flagged count between passes, as the reference's loop does.
+template <typename R>
+int adaptive_dev(mt_scene *sc, const mt_camera *cam, int w, int h, int n0, int nmax, double tau, int depth,
+                 unsigned char *rgb)
+{
+    DevCamera<R> dc;
+    fill_camera(cam, &dc);
+    DevScene<R> S = dev_scene<R>(sc);
+    S.counters = sc->counting ? sc->d_counters : nullptr;
+    const int wh = w * h;
+    DevBuf<double> sums;
+    DevBuf<int> nsamp, list, count;
+    DevBuf<unsigned char> drgb;
+    CK(sums.alloc((size_t)wh * 5), "cudaMalloc(adaptive sums)");
+    CK(nsamp.alloc((size_t)wh), "cudaMalloc(adaptive counts)");
+    CK(list.alloc((size_t)wh), "cudaMalloc(adaptive list)");
+    CK(count.alloc(1), "cudaMalloc(adaptive count)");
+    CK(drgb.alloc((size_t)wh * 3), "cudaMalloc(rgb)");
+    CK(cudaMemset(sums.p, 0, (size_t)wh * 5 * sizeof(double)), "cudaMemset");
+    CK(cudaMemset(nsamp.p, 0, (size_t)wh * sizeof(int)), "cudaMemset");
+    int max_passes = 1;
+    if (nmax > n0 && n0 > 0) max_passes += (nmax - n0 + n0 - 1) / n0;
+    CK(cudaEventRecord(sc->ev0, 0), "cudaEventRecord");
+    CK(launch_adaptive_pass<R>(S, dc, w, h, n0, nmax, n0, depth, nullptr, nullptr, sums.p, nsamp.p, 0),
+       "adaptive pass");
+    int passes = 1;
+    for (int pass = 1;; ++pass) {
+        CK(cudaMemsetAsync(count.p, 0, sizeof(int), 0), "cudaMemsetAsync");
+        CK(launch_adaptive_active(wh, nmax, tau, sums.p, nsamp.p, list.p, count.p, 0), "adaptive active set");
+        int remaining = 0;
+        CK(cudaMemcpy(&remaining, count.p, sizeof(int), cudaMemcpyDeviceToHost), "adaptive count");
+        if (remaining == 0 || pass >= max_passes) break;
+        CK(launch_adaptive_pass<R>(S, dc, w, h, n0, nmax, n0, depth, list.p, count.p, sums.p, nsamp.p, 0),
+           "adaptive pass");
+        ++passes;
+    }
+    CK(launch_adaptive_resolve(wh, sums.p, nsamp.p, drgb.p, 0), "adaptive resolve");
+    CK(cudaEventRecord(sc->ev1, 0), "cudaEventRecord");
+    CK(cudaMemcpy(rgb, drgb.p, (size_t)wh * 3, cudaMemcpyDeviceToHost), "cudaMemcpy(rgb)");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
+    sc->stats.kernel_ms = ms;
+    sc->stats.launches = 2 * passes + 1;
+    if (sc->counting) {
+        int rc = read_counters(sc);
+        if (rc) return rc;
+    }
+    return check_err_word(sc);
+}
+
+int render_image_adaptive_dev(mt_scene *sc, const mt_camera *cam, int w, int h, const mt_render_params *p,
+                              unsigned char *rgb)
+{
+    const int n0 = p->samples_per_pixel;
+    int nmax = p->adaptive_max_spp > 0 ? p->adaptive_max_spp : 4 * n0;  // default cap (src/render.c:1655-1658)
+    if (nmax < n0) nmax = n0;
+    const double tau = p->adaptive_tau > 0.0 ? p->adaptive_tau : 0.02;   // default tolerance
+    int rc = set_device(sc);
+    if (rc) return rc;
+    if (sc->opts.precision == MT_PRECISION_FP64)
+        return adaptive_dev<double>(sc, cam, w, h, n0, nmax, tau, p->max_depth, rgb);
+    return adaptive_dev<float>(sc, cam, w, h, n0, nmax, tau, p->max_depth, rgb);
+}
+
+}  // namespace
+
+extern "C" {
+
 int mt_render_image_ex(mt_scene *sc, const mt_camera *cam, int w, int h, const mt_render_params *p,
                        unsigned char *rgb)
 {
     if (p == nullptr) return fail(MT_ERR_NULL, "NULL params");
     int rc = render_args(sc, cam, rgb, w, h, p->samples_per_pixel, p->max_depth);
     if (rc) return rc;
-    if (p->adaptive) return mt_render_image_adaptive(sc, cam, w, h, p, rgb);
+    if (p->adaptive) return render_image_adaptive_dev(sc, cam, w, h, p, rgb);
     return render_host(sc, cam, w, h, p->samples_per_pixel, p->max_depth, RENDER_WHITTED, OUT_RGB8, rgb);
 }
 

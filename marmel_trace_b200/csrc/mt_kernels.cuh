@@ -190,7 +190,136 @@ cudaError_t launch_primary(const DevScene<R> &S, const DevCamera<R> &cam, int w,
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------
+// Adaptive Whitted refinement (render_image_adaptive, src/render.c:1128-1500).
+// Per pixel: double sums of R, G, B, luminance Y and Y^2, and the sample count.
+// Pass 0 takes samples 0..n0-1 of every pixel; each later pass takes up to
+// `batch` more samples of the pixels the active-set kernel flagged. Sample
+// index s is global per pixel, so a pixel's k-th sample is the same ray in
+// any pass, and each pass sums its samples serially before folding them in,
+// as adaptive_region does.
+// ------------------------------------------------------------------
+
+// adaptive_sample_offset (src/render.c:1156-1165): the fixed path's offsets
+// for s < n0, uniform jitter beyond; lens channels 2s+2 / 2s+3.
+template <typename R>
+MT_D Ray3<R> adaptive_primary(const DevCamera<R> &cam, int w, int h, int n0, int x, int y, int s)
+{
+    if (s < n0) return wh_primary(cam, w, h, n0, x, y, s);
+    R du = rand01<R>((uint32_t)x, (uint32_t)y, (uint32_t)(s * 2 + 0));
+    R dv = rand01<R>((uint32_t)x, (uint32_t)y, (uint32_t)(s * 2 + 1));
+    R uu = (R(x) + du) / R(w);
+    R vv = R(1) - (R(y) + dv) / R(h);
+    R lr1 = rand01<R>((uint32_t)x, (uint32_t)y, (uint32_t)(s * 2 + 2));
+    R lr2 = rand01<R>((uint32_t)x, (uint32_t)y, (uint32_t)(s * 2 + 3));
+    return camera_ray_dof(cam, uu, vv, lr1, lr2);
+}
+
+// One pass (adaptive_region, src/render.c:1174-1240). `list` holds the active
+// pixels (count on the device); NULL means every pixel (pass 0).
+template <typename R>
+__global__ void __launch_bounds__(128) k_adaptive_pass(const DevScene<R> S, const DevCamera<R> cam, int w, int h,
+                                                       int n0, int nmax, int batch, int depth, const int *list,
+                                                       const int *count, double *sums, int *nsamp)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n_active = list ? *count : w * h;
+    if (i >= n_active) return;
+    const int p = list ? list[i] : i;
+    const int x = p % w, y = p / w;
+    const int n = nsamp[p];
+    int b = batch;
+    if (b > nmax - n) b = nmax - n;
+    if (b <= 0) return;
+    double sr = 0.0, sg = 0.0, sb = 0.0, sy = 0.0, sy2 = 0.0;
+    for (int k = 0; k < b; ++k) {
+        const int s = n + k;
+        Ray3<R> ray = adaptive_primary(cam, w, h, n0, x, y, s);
+        uint32_t seed_key = hash3((uint32_t)x, (uint32_t)y, (uint32_t)s);
+        V3<R> c = whitted_trace(S, ray, depth, seed_key);
+        const double cx = (double)c.x, cy = (double)c.y, cz = (double)c.z;
+        sr += cx;
+        sg += cy;
+        sb += cz;
+        const double Y = 0.2126 * cx + 0.7152 * cy + 0.0722 * cz;
+        sy += Y;
+        sy2 += Y * Y;
+    }
+    double *q = sums + 5 * (size_t)p;
+    q[0] += sr;
+    q[1] += sg;
+    q[2] += sb;
+    q[3] += sy;
+    q[4] += sy2;
+    nsamp[p] = n + b;
+    if (S.counters) atomicAdd(&S.counters->primary_rays, (unsigned long long)b);
+}
+
+// adaptive_compute_active (src/render.c:1330-1363): refine while the relative
+// standard error of the mean luminance exceeds tau and n < nmax. Flagged
+// pixels are appended to `list`; *count is their number.
+template <int Unused = 0>
+__global__ void k_adaptive_active(int wh, int nmax, double tau, const double *sums, const int *nsamp, int *list,
+                                  int *count)
+{
+    const int stride = gridDim.x * blockDim.x;
+    const int n_round = (wh + stride - 1) / stride * stride;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_round; p += stride) {
+        bool flag = false;
+        if (p < wh) {
+            const int n = nsamp[p];
+            if (n < nmax) {
+                if (n < 2) {
+                    flag = true;
+                } else {
+                    const double nf = (double)n;
+                    const double *q = sums + 5 * (size_t)p;
+                    const double ybar = q[3] / nf;
+                    double var = (q[4] - q[3] * ybar) / (nf - 1.0);
+                    if (var < 0.0) var = 0.0;
+                    const double se = sqrt(var / nf);
+                    const double e = se / (ybar + 1e-4);
+                    flag = e > tau;
+                }
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, flag);
+        int base = 0;
+        const int lane = threadIdx.x & 31;
+        if (m && lane == __ffs(m) - 1) base = atomicAdd(count, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, __ffs(m ? m : 1u) - 1);
+        if (flag) list[base + __popc(m & ((1u << lane) - 1u))] = p;
+    }
+}
+
+// adaptive_resolve (src/render.c:1365-1375): mean, then quantise once.
+template <int Unused = 0>
+__global__ void k_adaptive_resolve(int wh, const double *sums, const int *nsamp, unsigned char *rgb)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= wh) return;
+    const double inv = 1.0 / (double)nsamp[p];
+    const double *q = sums + 5 * (size_t)p;
+    rgb[3 * (size_t)p] = to_byte<double>(q[0] * inv);
+    rgb[3 * (size_t)p + 1] = to_byte<double>(q[1] * inv);
+    rgb[3 * (size_t)p + 2] = to_byte<double>(q[2] * inv);
+}
+
+template <typename R>
+cudaError_t launch_adaptive_pass(const DevScene<R> &S, const DevCamera<R> &cam, int w, int h, int n0, int nmax,
+                                 int batch, int depth, const int *list, const int *count, double *sums, int *nsamp,
+                                 cudaStream_t stream)
+{
+    long long n = (long long)w * h;
+    k_adaptive_pass<R><<<grid_for(n, 128), 128, stack_smem(S, 128), stream>>>(S, cam, w, h, n0, nmax, batch, depth,
+                                                                              list, count, sums, nsamp);
+    return cudaGetLastError();
+}
+
 #define MT_INSTANTIATE(R)                                                                                        \
+    template cudaError_t launch_adaptive_pass<R>(const DevScene<R> &, const DevCamera<R> &, int, int, int, int,   \
+                                                 int, int, const int *, const int *, double *, int *,            \
+                                                 cudaStream_t);                                                   \
     template cudaError_t launch_render<R>(const DevScene<R> &, const DevCamera<R> &, int, int, int, int, int, int, \
                                           int, int, void *, int, cudaStream_t);                                  \
     template cudaError_t launch_intersect<R>(const DevScene<R> &, int, const double *, const double *, double,    \

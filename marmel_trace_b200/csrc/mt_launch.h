@@ -42,6 +42,18 @@ template <typename R>
 cudaError_t launch_primary(const DevScene<R> &S, const DevCamera<R> &cam, int w, int h, int spp, int mode,
                            double *out, cudaStream_t stream);
 
+// Adaptive Whitted refinement (render_image_adaptive, src/render.c:1128-1500):
+// one pass over the active pixels (list == NULL: every pixel), the active-set
+// update and the final resolve. sums: 5 doubles per pixel (R, G, B, Y, Y^2).
+template <typename R>
+cudaError_t launch_adaptive_pass(const DevScene<R> &S, const DevCamera<R> &cam, int w, int h, int n0, int nmax,
+                                 int batch, int depth, const int *list, const int *count, double *sums, int *nsamp,
+                                 cudaStream_t stream);
+cudaError_t launch_adaptive_active(int wh, int nmax, double tau, const double *sums, const int *nsamp, int *list,
+                                   int *count, cudaStream_t stream);
+cudaError_t launch_adaptive_resolve(int wh, const double *sums, const int *nsamp, unsigned char *rgb,
+                                    cudaStream_t stream);
+
 // Path-replay adjoint over samples [s0, s1): grad += adj_scale * sum over
 // pixels and samples of adj_img[pixel] . dL_sample/dtheta (mt_adjoint.cuh).
 template <typename R>

@@ -50,8 +50,3 @@ void wavefront_destroy(WavefrontState *st)
 const char *wavefront_last_error() { return wfdetail::last_error().c_str(); }
 
 }  // namespace mt
-
-int mt_render_image_adaptive(mt_scene *, const mt_camera *, int, int, const mt_render_params *, unsigned char *)
-{
-    return MT_ERR_UNSUPPORTED;
-}

@@ -53,6 +53,4 @@ const char *wavefront_last_error();
 
 }  // namespace mt
 
-// Adaptive Whitted refinement (render_image_adaptive, src/render.c:1128-1500).
-int mt_render_image_adaptive(mt_scene *sc, const mt_camera *cam, int w, int h, const mt_render_params *p,
-                             unsigned char *rgb);
+

@@ -230,6 +230,14 @@ class RefScene:
             raise RuntimeError("the dual-number oracle does not cover this scene")
         return g, vs, rc
 
+    def render_image_ex(self, w, h, spp, depth, adaptive=1, max_spp=0, tau=0.0):
+        """render_image_ex: fixed or adaptive Whitted (src/render.c:1627)."""
+        out = np.zeros((h, w, 3), np.uint8)
+        rc = self.lib.mtref_render_image_ex(self.h, w, h, spp, depth, adaptive, max_spp, tau, _p(out))
+        if rc != 0:
+            raise RuntimeError(f"render_image_ex returned {rc}")
+        return out
+
     def whitted_render(self, w, h, spp, depth):
         out = np.zeros((h, w, 3), np.uint8)
         rc = self.lib.mtref_render_image(self.h, w, h, spp, depth, _p(out))
