@@ -199,7 +199,14 @@ typedef struct {
                                 0 = plain launches, -1 = plain launches timed per stage */
     int32_t device;          /* CUDA device ordinal                             */
     int32_t traversal;       /* wavefront traversal kernels: MT_TRAVERSAL_*     */
+    int32_t bvh_builder;     /* MT_BVH_BUILDER_*                                */
 } mt_options;
+
+/* Where the scene's BVH is built. Both run the reference's binned-SAH
+ * algorithm (src/bvh.c:180-422) and give the same tree; the device build
+ * orders the primitives inside each node differently (mt_bvh_build_device). */
+#define MT_BVH_BUILDER_HOST   0  /* single host thread, the reference's node order */
+#define MT_BVH_BUILDER_DEVICE 1  /* breadth-first on the scene's device           */
 
 /* Wavefront traversal kernels (extend and shadow stages). */
 #define MT_TRAVERSAL_DEFAULT 0   /* library default (grid-stride)                    */
@@ -250,6 +257,17 @@ int mt_scene_export_bvh(const mt_scene *scene, double *bounds6, int32_t *links4,
  * arrays to query the sizes. */
 int mt_bvh_build_host(const mt_prim *prims, int32_t prim_count, double *bounds6, int32_t *links4,
                       int32_t *order, int32_t *node_count, int32_t *order_count, int32_t *depth);
+
+/* The same build on a CUDA device (bvh_build's algorithm, breadth-first):
+ * the nodes, bounds, leaves and preorder numbering of mt_bvh_build_host, with
+ * the primitives of each node in a different order (a stable partition
+ * replaces the reference's in-place swap partition). The one exception is a
+ * median split whose midpoint rounds onto the smallest centroid (centroids
+ * one ulp apart): it splits the current order at count / 2, as the reference
+ * does, and that order differs. build_ms (optional): device time of the
+ * build. Call once with NULL arrays to query the sizes (each call builds). */
+int mt_bvh_build_device(const mt_prim *prims, int32_t prim_count, int32_t device, double *bounds6, int32_t *links4,
+                        int32_t *order, int32_t *node_count, int32_t *order_count, int32_t *depth, float *build_ms);
 
 /* ------------------------------------------------------------------ */
 /* Camera                                                              */

@@ -149,6 +149,7 @@ class MtOptions(C.Structure):
         ("use_graph", C.c_int32),
         ("device", C.c_int32),
         ("traversal", C.c_int32),
+        ("bvh_builder", C.c_int32),
     ]
 
 
@@ -226,6 +227,7 @@ SIGNATURES = {
     "mt_render_accumulate_device": (I, [P, P, I, I, I, I, I, I, P, I, P]),
     "mt_render_accumulate_device_noalloc": (I, [P, P, I, I, I, I, I, P, I, P]),
     "mt_autotune": (I, [P, P, I, I, I, I, P]),
+    "mt_bvh_build_device": (I, [P, I, I, P, P, P, P, P, P, P]),
     "mt_batch_create": (I, [I, I, I, P]),
     "mt_batch_release": (None, [P]),
     "mt_batch_render": (I, [P, I, P, P, P, P]),

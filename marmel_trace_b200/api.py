@@ -156,6 +156,22 @@ def bvh_build_host(prims: np.ndarray):
     return b, l, o[: m.value], dep.value
 
 
+def bvh_build_device(prims: np.ndarray, device: int = 0):
+    """The same BVH built on a CUDA device (mt_bvh_build_device): bounds,
+    links, permutation, depth and the device build time in ms."""
+    lib = capi.load()
+    prims = np.ascontiguousarray(prims)
+    n, m, dep, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
+    check(lib.mt_bvh_build_device(ptr(prims), len(prims), device, None, None, None, C.byref(n), C.byref(m),
+                                  C.byref(dep), None), "mt_bvh_build_device")
+    b = np.zeros((n.value, 6), np.float64)
+    l = np.zeros((n.value, 4), np.int32)
+    o = np.zeros(max(m.value, 1), np.int32)
+    check(lib.mt_bvh_build_device(ptr(prims), len(prims), device, ptr(b), ptr(l), ptr(o), C.byref(n), C.byref(m),
+                                  C.byref(dep), C.byref(ms)), "mt_bvh_build_device")
+    return b, l, o[: m.value], dep.value, ms.value
+
+
 def make_options(precision: str = "fp32", integrator: str = "megakernel", **kw) -> capi.MtOptions:
     lib = capi.load()
     o = capi.MtOptions()

@@ -39,6 +39,7 @@ UNITS = [
     ("mt_adjoint.cu", []),
     ("mt_adjoint_f64.cu", ["--fmad=false"]),
     ("mt_bvh.cpp", []),
+    ("mt_bvh_gpu.cu", ["--fmad=false"]),
 ]
 
 

@@ -587,6 +587,7 @@ void mt_options_default(mt_options *o)
     o->use_graph = 1;
     o->device = 0;
     o->traversal = MT_TRAVERSAL_DEFAULT;
+    o->bvh_builder = MT_BVH_BUILDER_HOST;
 }
 
 const char *mt_version(void) { return "mtgpu 0.1 (sm_100a)"; }
@@ -624,7 +625,13 @@ int mt_scene_create(const mt_scene_desc *desc, const mt_options *opts, mt_scene 
     };
     if ((rc = set_device(sc))) return bail(rc);
 
-    build_bvh(desc->prims, desc->prim_count, &sc->bvh);
+    if (sc->opts.bvh_builder == MT_BVH_BUILDER_DEVICE) {
+        std::string err;
+        int brc = build_bvh_device(desc->prims, desc->prim_count, &sc->bvh, &err, nullptr);
+        if (brc) return bail(fail(brc, "device BVH build: %s", err.c_str()));
+    } else {
+        build_bvh(desc->prims, desc->prim_count, &sc->bvh);
+    }
     flatten_bvh(sc->bvh, &sc->flat);
     if (sc->flat.depth + 1 > kStackSize)
         return bail(fail(MT_ERR_UNSUPPORTED, "BVH depth %d exceeds the traversal stack (%d)", sc->flat.depth,
@@ -710,6 +717,40 @@ int mt_bvh_build_host(const mt_prim *prims, int32_t n, double *bounds6, int32_t 
     if (n < 0 || (n > 0 && !prims)) return fail(MT_ERR_NULL, "NULL pointer");
     HostBvh b;
     build_bvh(prims, n, &b);
+    if (node_count) *node_count = (int32_t)b.nodes.size();
+    if (order_count) *order_count = (int32_t)b.order.size();
+    if (depth) *depth = b.depth;
+    for (size_t i = 0; i < b.nodes.size(); ++i) {
+        const HostNode &nd = b.nodes[i];
+        if (bounds6)
+            for (int k = 0; k < 3; ++k) {
+                bounds6[6 * i + k] = nd.mn[k];
+                bounds6[6 * i + 3 + k] = nd.mx[k];
+            }
+        if (links4) {
+            links4[4 * i] = nd.left;
+            links4[4 * i + 1] = nd.right;
+            links4[4 * i + 2] = nd.first;
+            links4[4 * i + 3] = nd.count;
+        }
+    }
+    if (order)
+        for (size_t i = 0; i < b.order.size(); ++i) order[i] = b.order[i];
+    return 0;
+}
+
+int mt_bvh_build_device(const mt_prim *prims, int32_t n, int32_t device, double *bounds6, int32_t *links4,
+                        int32_t *order, int32_t *node_count, int32_t *order_count, int32_t *depth, float *build_ms)
+{
+    if (n < 0 || (n > 0 && !prims)) return fail(MT_ERR_NULL, "NULL pointer");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return fail(MT_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(MT_ERR_INVALID, "device %d out of range", device);
+    CK(cudaSetDevice(device), "cudaSetDevice");
+    HostBvh b;
+    std::string err;
+    int rc = build_bvh_device(prims, n, &b, &err, build_ms);
+    if (rc) return fail(rc, "device BVH build: %s", err.c_str());
     if (node_count) *node_count = (int32_t)b.nodes.size();
     if (order_count) *order_count = (int32_t)b.order.size();
     if (depth) *depth = b.depth;

@@ -3,6 +3,7 @@
 
 #include <stdint.h>
 
+#include <string>
 #include <vector>
 
 #include "../../include/mtgpu.h"
@@ -29,6 +30,11 @@ void prim_bounds(const mt_prim &p, double mn[3], double mx[3]);
 // median fallback, planes in a side list. Deterministic and identical to the
 // reference builder for the same primitive array.
 int build_bvh(const mt_prim *prims, int n, HostBvh *out);
+
+// The same build on the current CUDA device (mt_bvh_gpu.cu): the tree of
+// build_bvh with the primitives of each node in another order (see there).
+// Returns 0 or an MT_ERR_* code (message in *err); *ms: device build time.
+int build_bvh_device(const mt_prim *prims, int n, HostBvh *out, std::string *err, float *ms);
 
 // Device-ready flattened tree (see mt_layout.h for the node record).
 struct FlatBvh {
