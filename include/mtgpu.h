@@ -483,7 +483,10 @@ int mt_primary_rays(mt_scene *scene, const mt_camera *cam, int width, int height
 /*
  * Differentiable parameters, flat: for each material m, albedo rgb at 8m+0..2,
  * roughness 8m+3, metallic 8m+4, emissive rgb 8m+5..7; then the sun radiance
- * (sky sun_color) rgb at 8M+0..2. mt_scene_param_count returns 8M + 3.
+ * (sky sun_color) rgb at 8M+0..2; then for each material m the Beer-Lambert
+ * absorption rgb at 8M+3+3m+0..2 (it acts on media and on shadow segments
+ * through water / beer_lambert surfaces, src/pathtrace.c:220-233, 504-532).
+ * mt_scene_param_count returns 11M + 3.
  * Setting parameters updates the device materials and sun and re-collects the
  * emissive light list (scene_collect_emissive_lights, src/scene.c:1384-1426).
  */

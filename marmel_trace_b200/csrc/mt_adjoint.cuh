@@ -2,7 +2,10 @@
 //
 // Parameters: per material m, albedo rgb (8m + 0..2), roughness (8m + 3),
 // metallic (8m + 4), emissive rgb (8m + 5..7); then the sun radiance rgb
-// (8M + 0..2). Geometry and visibility derivatives are out of scope.
+// (8M + 0..2); then per material the Beer-Lambert absorption rgb
+// (8M + 3 + 3m + 0..2), which acts through media (pt_apply_medium) and on
+// shadow segments through water / beer_lambert surfaces. Geometry and
+// visibility derivatives are out of scope.
 //
 // Estimator. The path tracer's per-sample value is L = sum_b beta_b E_b,
 // where E_b is what vertex b adds (emission, NEE, sky) and
@@ -24,13 +27,23 @@
 namespace mt {
 
 static constexpr int kParamsPerMaterial = 8;
+static constexpr int kAbsorbPerMaterial = 3;
 static constexpr int kAdjMaxMaterials = 256;
-static constexpr int kAdjMaxParams = kParamsPerMaterial * kAdjMaxMaterials + 3;
+static constexpr int kAdjMaxParams = (kParamsPerMaterial + kAbsorbPerMaterial) * kAdjMaxMaterials + 3;
+// per NEE connection of a replayed vertex: transmittance rgb, then the
+// absorbing materials passed (as R) and their distance sums (AbsorbPath)
+static constexpr int kAttStride = 8;
 
 struct AdjCtx {
     float *g;      // gradient accumulator (shared memory)
     int sun;       // index of the sun radiance's red channel
+    int absorb;    // index of material 0's absorption red channel
 };
+
+MT_D AdjCtx make_adj_ctx(float *g, int material_count)
+{
+    return AdjCtx{g, kParamsPerMaterial * material_count, kParamsPerMaterial * material_count + 3};
+}
 
 MT_D void gadd(const AdjCtx &c, int i, float v)
 {
@@ -277,6 +290,53 @@ template <typename R> MT_D V3<R> safe_div(V3<R> a, V3<R> b)
     return v3(b.x != R(0) ? a.x / b.x : R(0), b.y != R(0) ? a.y / b.y : R(0), b.z != R(0) ? a.z / b.z : R(0));
 }
 
+// Gradient of one medium segment (pt_apply_medium, src/pathtrace.c:220-233)
+// w.r.t. the medium's absorption: the segment adds beta * deep * (1 - T) and
+// scales the throughput by T = exp(-a d) (water_transmittance); `beta` is the
+// throughput entering the segment and `after` = L - radiance once the
+// segment's own term is in, i.e. what the scaled throughput carries.
+template <typename R>
+MT_D void medium_grad(const AdjCtx &ctx, const DevMaterial<R> &m, int mi, R dist, V3<R> beta, V3<R> after, V3<R> adj)
+{
+    const R d = dist > R(0) ? dist : R(0);
+    for (int ch = 0; ch < 3; ++ch) {
+        const R a = m.absorption[ch];
+        const R T = water_transmittance(a, d);
+        // exp(-a d) clamped to [0, 1]: derivative -d T inside, 0 where clamped
+        const R dT = (a >= R(0) && T > R(0)) ? -d * T : R(0);
+        if (dT == R(0)) continue;
+        const R g = comp3(adj, ch) * (-comp3(beta, ch) * m.deep_color[ch] * dT) +
+                    comp3(adj, ch) * comp3(after, ch) * (dT / T);
+        gadd(ctx, ctx.absorb + kAbsorbPerMaterial * mi + ch, (float)g);
+    }
+}
+
+// Absorption part of one NEE connection: contribution c (adj-weighted, per
+// channel) times -(distance through each absorbing material).
+template <typename R> MT_D void nee_absorb_grad(const AdjCtx &ctx, const R *slot, V3<R> c)
+{
+    for (int k = 0; k < 2; ++k) {
+        const int am = (int)slot[5 + k];
+        const R dist = slot[3 + k];
+        if (am < 0 || dist == R(0)) continue;
+        for (int ch = 0; ch < 3; ++ch)
+            gadd(ctx, ctx.absorb + kAbsorbPerMaterial * am + ch, (float)(-dist * comp3(c, ch)));
+    }
+}
+
+// Fill one NEE connection record from a shadow walk's result.
+template <typename R> MT_D void set_att(R *slot, V3<R> atten, const AbsorbPath<R> &ab)
+{
+    slot[0] = atten.x;
+    slot[1] = atten.y;
+    slot[2] = atten.z;
+    slot[3] = ab.dist[0];
+    slot[4] = ab.dist[1];
+    slot[5] = R(ab.mat[0]);
+    slot[6] = R(ab.mat[1]);
+    slot[7] = R(0);
+}
+
 // A surface vertex of a replayed path, held until its NEE visibility and the
 // radiance the path gathers after it are known. Everything else the
 // vertex's gradient needs is re-drawn from the path's random stream.
@@ -292,9 +352,10 @@ static constexpr int kVertFront = 1;  // front-face hit (legacy glass sampling)
 static constexpr int kVertSun = 2;    // the vertex draws a sun NEE sample
 
 // Gradient terms of one vertex: NEE to every sphere light and to the sun,
-// given each connection's transmittance att[3*slot] (zero where it was not
-// made, occluded or dark: such a connection adds nothing), and the BSDF
-// weight term against `remaining` = L - radiance through this vertex.
+// given each connection's record att[kAttStride * slot] (transmittance zero
+// where it was not made, occluded or dark: such a connection adds nothing),
+// and the BSDF weight term against `remaining` = L - radiance through this
+// vertex.
 // Light sampling follows pt_nee_emissive / pt_nee_sun (src/pathtrace.c:534-606)
 // and the BSDF sample pt_sample_* (src/pathtrace.c:961-1000), from the same
 // random channels as the primal pass.
@@ -311,7 +372,8 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
     const int b = vx.b;
     const V3<R> one = v3(R(1), R(1), R(1));
     for (int li = 0; li < S.light_count; ++li) {
-        const V3<R> a = v3(att[3 * li], att[3 * li + 1], att[3 * li + 2]);
+        const R *slot = att + kAttStride * li;
+        const V3<R> a = v3(slot[0], slot[1], slot[2]);
         if (a.x == R(0) && a.y == R(0) && a.z == R(0)) continue;
         const DevLight<R> &lt = S.lights[li];
         V3<R> to_c = sub(mat3(lt.center), P);
@@ -330,9 +392,10 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
         if (lmat >= 0 && lmat < S.material_count)
             for (int ch = 0; ch < 3; ++ch)
                 gadd(ctx, kParamsPerMaterial * lmat + 5 + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
+        nee_absorb_grad(ctx, slot, mul(mul(coeff, s1), mul(mat3(lt.emissive), a)));
     }
     if (vx.flags & kVertSun) {
-        const R *as = att + 3 * kMaxLights;
+        const R *as = att + kAttStride * kMaxLights;
         const V3<R> a = v3(as[0], as[1], as[2]);
         if (a.x != R(0) || a.y != R(0) || a.z != R(0)) {
             R r1 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_A);
@@ -345,6 +408,7 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
             V3<R> s1 = shade(mm, N, Ls, V, one);
             for (int ch = 0; ch < 3; ++ch)
                 gadd(ctx, ctx.sun + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
+            nee_absorb_grad(ctx, as, mul(mul(coeff, s1), mul(mat3(S.sky.sun_color), a)));
         }
     }
     uint32_t kb = hash3(seed_key ^ PT_KEY, (uint32_t)b, 0u);
@@ -383,13 +447,19 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
         SurfaceHit<R> h;
         if (!scene_intersect(S, r.o, r.d, R(1e-4), R(1e30), &h)) {
             if (medium >= 0) {
+                const V3<R> beta_in = throughput;
                 pt_apply_medium(S.materials[medium], R(5.0), &throughput, &radiance);
+                medium_grad(ctx, S.materials[medium], medium, R(5.0), beta_in, sub(L, radiance), adj);
                 medium = -1;
             }
             sky_sun_grad(ctx, r.d, S.sky, mul(adj, throughput));
             return;
         }
-        if (medium >= 0) pt_apply_medium(S.materials[medium], h.t, &throughput, &radiance);
+        if (medium >= 0) {
+            const V3<R> beta_in = throughput;
+            pt_apply_medium(S.materials[medium], h.t, &throughput, &radiance);
+            medium_grad(ctx, S.materials[medium], medium, h.t, beta_in, sub(L, radiance), adj);
+        }
         if (h.material < 0 || h.material >= S.material_count) {
             sky_sun_grad(ctx, r.d, S.sky, mul(adj, throughput));
             return;
@@ -425,8 +495,8 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
         vx.flags = (h.front_face ? kVertFront : 0) |
                    ((b == 0 || (b == 1 && medium >= 0 && last_bounce_specular)) ? kVertSun : 0);
         vx.pad = 0;
-        R att[kNeeSlots * 3];
-        for (int k = 0; k < kNeeSlots * 3; ++k) att[k] = R(0);
+        R att[kNeeSlots * kAttStride];
+        for (int k = 0; k < kNeeSlots * kAttStride; ++k) att[k] = R(0);
         // ---- emissive-sphere NEE (pt_nee_emissive, src/pathtrace.c:576-606) ----
         if (S.light_count > 0) {
             V3<R> sum = v3(R(0), R(0), R(0));
@@ -449,12 +519,11 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
                 R lt_t;
                 if (!light_sphere_t(S, lt.prim, so, wi, R(1e-3), R(1e30), &lt_t)) continue;
                 V3<R> atten;
-                if (pt_occluded_segment(S, so, wi, R(1e-3), lt_t - R(1e-3), &atten)) continue;
+                AbsorbPath<R> ab;
+                if (pt_occluded_segment_abs(S, so, wi, R(1e-3), lt_t - R(1e-3), &atten, &ab)) continue;
                 V3<R> lit = shade(mm, N, wi, V, mul(mat3(lt.emissive), atten));
                 sum = add(sum, mul(throughput, scale(lit, Omega)));
-                att[3 * li] = atten.x;
-                att[3 * li + 1] = atten.y;
-                att[3 * li + 2] = atten.z;
+                set_att(att + kAttStride * li, atten, ab);
             }
             radiance = add(radiance, sum);
         }
@@ -467,15 +536,14 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
             if (finite3(Ls) && dot(N, Ls) > R(0)) {
                 V3<R> so = add(P, scale(N, R(1e-3)));
                 V3<R> atten;
-                if (!pt_occluded_segment(S, so, Ls, R(1e-3), R(1e30), &atten)) {
+                AbsorbPath<R> ab;
+                if (!pt_occluded_segment_abs(S, so, Ls, R(1e-3), R(1e30), &atten, &ab)) {
                     if (!(atten.x < R(1e-4) && atten.y < R(1e-4) && atten.z < R(1e-4))) {
                         R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
                         R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
                         V3<R> lit = shade(mm, N, Ls, V, mul(mat3(S.sky.sun_color), atten));
                         radiance = add(radiance, mul(throughput, scale(lit, Omega)));
-                        att[3 * kMaxLights] = atten.x;
-                        att[3 * kMaxLights + 1] = atten.y;
-                        att[3 * kMaxLights + 2] = atten.z;
+                        set_att(att + kAttStride * kMaxLights, atten, ab);
                     }
                 }
             }
@@ -523,7 +591,7 @@ __global__ void __launch_bounds__(128) k_adjoint(const DevScene<R> S, const DevC
     __shared__ float g[kAdjMaxParams];
     for (int i = threadIdx.x; i < n_params; i += blockDim.x) g[i] = 0.0f;
     __syncthreads();
-    AdjCtx ctx{g, kParamsPerMaterial * S.material_count};
+    const AdjCtx ctx = make_adj_ctx(g, S.material_count);
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
     if (pix < w * h) {
         V3<R> adj = v3<R>((R)(adj_img[3 * (size_t)pix] * adj_scale), (R)(adj_img[3 * (size_t)pix + 1] * adj_scale),

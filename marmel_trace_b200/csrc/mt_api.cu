@@ -22,9 +22,11 @@
 
 using namespace mt;
 
-// Adjoint parameter layout (mt_adjoint.cuh): 8 per material, then the sun.
+// Adjoint parameter layout (mt_adjoint.cuh): 8 per material, then the sun,
+// then 3 absorption coefficients per material.
 static constexpr int kParamsPerMaterialApi = 8;
 static constexpr int kAdjMaxMaterialsApi = 256;
+static inline int param_count(int M) { return kParamsPerMaterialApi * M + 3 + 3 * M; }
 
 namespace {
 
@@ -409,6 +411,8 @@ int check_err_word(mt_scene *sc)
         if (e & ERR_STACK) return fail(MT_ERR_OVERFLOW, "traversal stack overflow");
         if (e & ERR_QUEUE) return fail(MT_ERR_OVERFLOW, "wavefront queue overflow");
         if (e & ERR_WHITTED) return fail(MT_ERR_OVERFLOW, "Whitted frame stack overflow");
+        if (e & ERR_ABSORB)
+            return fail(MT_ERR_UNSUPPORTED, "adjoint: a shadow segment crossed more than two absorbing materials");
         if (e & ERR_WATCHDOG) return fail(MT_ERR_WATCHDOG, "a bounded device loop reached its cap");
         return fail(MT_ERR_LAUNCH, "device error word 0x%x", e);
     }
@@ -1196,15 +1200,15 @@ int mt_primary_rays(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, i
 int mt_scene_param_count(const mt_scene *sc)
 {
     if (!sc) return -fail(MT_ERR_NULL, "NULL pointer");
-    return kParamsPerMaterialApi * (int)sc->h_mats.size() + 3;
+    return param_count((int)sc->h_mats.size());
 }
 
 int mt_scene_get_material_params(const mt_scene *sc, double *params, int n)
 {
     if (!sc || !params) return fail(MT_ERR_NULL, "NULL pointer");
     const int M = (int)sc->h_mats.size();
-    if (n != kParamsPerMaterialApi * M + 3) return fail(MT_ERR_INVALID, "expected %d parameters, got %d",
-                                                        kParamsPerMaterialApi * M + 3, n);
+    if (n != param_count(M)) return fail(MT_ERR_INVALID, "expected %d parameters, got %d",
+                                                        param_count(M), n);
     for (int m = 0; m < M; ++m) {
         const mt_material &mt = sc->h_mats[m];
         double *p = params + kParamsPerMaterialApi * m;
@@ -1216,6 +1220,8 @@ int mt_scene_get_material_params(const mt_scene *sc, double *params, int n)
         p[4] = mt.metallic;
     }
     for (int k = 0; k < 3; ++k) params[kParamsPerMaterialApi * M + k] = sc->h_sky.sun_color[k];
+    for (int m = 0; m < M; ++m)
+        for (int k = 0; k < 3; ++k) params[kParamsPerMaterialApi * M + 3 + 3 * m + k] = sc->h_mats[m].absorption[k];
     return 0;
 }
 
@@ -1242,8 +1248,8 @@ int mt_scene_set_material_params(mt_scene *sc, const double *params, int n)
 {
     if (!sc || !params) return fail(MT_ERR_NULL, "NULL pointer");
     const int M = (int)sc->h_mats.size();
-    if (n != kParamsPerMaterialApi * M + 3) return fail(MT_ERR_INVALID, "expected %d parameters, got %d",
-                                                        kParamsPerMaterialApi * M + 3, n);
+    if (n != param_count(M)) return fail(MT_ERR_INVALID, "expected %d parameters, got %d",
+                                                        param_count(M), n);
     for (int m = 0; m < M; ++m) {
         mt_material &mt = sc->h_mats[m];
         const double *p = params + kParamsPerMaterialApi * m;
@@ -1255,6 +1261,8 @@ int mt_scene_set_material_params(mt_scene *sc, const double *params, int n)
         mt.metallic = p[4];
     }
     for (int k = 0; k < 3; ++k) sc->h_sky.sun_color[k] = params[kParamsPerMaterialApi * M + k];
+    for (int m = 0; m < M; ++m)
+        for (int k = 0; k < 3; ++k) sc->h_mats[m].absorption[k] = params[kParamsPerMaterialApi * M + 3 + 3 * m + k];
     sc->version++;
     int rc = set_device(sc);
     if (rc) return rc;
@@ -1273,7 +1281,7 @@ int mt_adjoint_backward_device(mt_scene *sc, const mt_camera *cam, int w, int h,
     if (M > kAdjMaxMaterialsApi) return fail(MT_ERR_UNSUPPORTED, "the adjoint supports at most %d materials",
                                              kAdjMaxMaterialsApi);
     if ((rc = set_device(sc))) return rc;
-    const int np = kParamsPerMaterialApi * M + 3;
+    const int np = param_count(M);
     cudaStream_t s = (cudaStream_t)stream;
     if (!accumulate) CK(cudaMemsetAsync(grad_dev, 0, np * sizeof(double), s), "cudaMemsetAsync(grad)");
     const double scale = 1.0 / (double)(s1 - s0);
@@ -1288,7 +1296,7 @@ int mt_adjoint_backward(mt_scene *sc, const mt_camera *cam, int w, int h, int sp
     int rc = render_args(sc, cam, dL_dimage, w, h, spp, depth);
     if (rc) return rc;
     if (!grad) return fail(MT_ERR_NULL, "NULL gradient buffer");
-    const int np = kParamsPerMaterialApi * (int)sc->h_mats.size() + 3;
+    const int np = param_count((int)sc->h_mats.size());
     if (n != np) return fail(MT_ERR_INVALID, "expected %d parameters, got %d", np, n);
     if ((rc = set_device(sc))) return rc;
     DevBuf<float> dA;

@@ -172,6 +172,59 @@ MT_D bool pt_occluded_segment(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R 
     return true;
 }
 
+// Distances a shadow segment travels through absorbing (Beer-Lambert)
+// materials, for the adjoint: up to two materials, `mat` -1 when unused.
+template <typename R> struct AbsorbPath {
+    int mat[2];
+    R dist[2];
+};
+
+// pt_occluded_segment with the same result and attenuation, also reporting
+// the absorbing materials passed and the distance factor of each one: the
+// attenuation is prod exp(-absorption * t) over the passed hits, so
+// d attenuation / d absorption_c(m) = -attenuation_c * (sum of t over m's hits).
+// A third distinct absorbing material on one segment sets ERR_ABSORB.
+template <typename R>
+MT_D bool pt_occluded_segment_abs(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax, V3<R> *attenuation,
+                                  AbsorbPath<R> *ab)
+{
+    ab->mat[0] = ab->mat[1] = -1;
+    ab->dist[0] = ab->dist[1] = R(0);
+    *attenuation = v3(R(1), R(1), R(1));
+    V3<R> cur_o = o;
+    R remaining = tmax;
+    if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
+    if (!S.has_passthrough) return scene_any(S, ray_pre(o, unit_dir(d)), tmin, tmax);
+    for (int step = 0; step < 6; ++step) {
+        SurfaceHit<R> h;
+        if (!scene_intersect(S, cur_o, d, tmin, remaining, &h)) return false;
+        if (h.material < 0 || h.material >= S.material_count) return true;
+        const DevMaterial<R> &m = S.materials[h.material];
+        if (m.is_water || m.transparency > R(0.8)) {
+            if (m.beer_lambert || m.is_water) {
+                V3<R> seg = v3(mexp(-m.absorption[0] * h.t), mexp(-m.absorption[1] * h.t),
+                               mexp(-m.absorption[2] * h.t));
+                *attenuation = mul(*attenuation, seg);
+                int k = ab->mat[0] == h.material ? 0 : ab->mat[1] == h.material ? 1 : ab->mat[0] < 0 ? 0
+                                                                                     : ab->mat[1] < 0 ? 1 : -1;
+                if (k < 0) {
+                    atomicOr(S.err, ERR_ABSORB);
+                } else {
+                    ab->mat[k] = h.material;
+                    ab->dist[k] += h.t;
+                }
+            }
+            cur_o = add(h.point, scale(d, R(1e-3)));
+            remaining -= h.t;
+            if (remaining <= R(1e-3)) return false;
+            tmin = R(1e-3);
+            continue;
+        }
+        return true;
+    }
+    return true;
+}
+
 // pt_nee_sun (src/pathtrace.c:534-556)
 template <typename R>
 MT_D V3<R> pt_nee_sun(const DevScene<R> &S, const DevMaterial<R> &mm, V3<R> P, V3<R> N, V3<R> V, V3<R> throughput,

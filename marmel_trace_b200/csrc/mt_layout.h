@@ -45,6 +45,7 @@ enum : unsigned {
     ERR_QUEUE = 2u,      // wavefront queue overflow
     ERR_WATCHDOG = 4u,   // bounded loop reached its cap
     ERR_WHITTED = 8u,    // Whitted frame stack overflow
+    ERR_ABSORB = 16u,    // adjoint: a shadow segment crossed more than two absorbing materials
 };
 
 template <typename R> struct DevMaterial {

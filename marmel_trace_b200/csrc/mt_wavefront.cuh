@@ -72,7 +72,7 @@ template <typename R> struct WfParams {
 // Buffers of the adjoint replay pass.
 template <typename R> struct WfAdj {
     AdjVertex<R> *verts;  // the vertex each path holds until its NEE is resolved
-    R *att;               // per path: kNeeSlots x rgb transmittance of visible NEE connections
+    R *att;               // per path: kNeeSlots records of kAttStride (transmittance, absorbing distances)
     const R *L;           // per-sample radiance of the primal pass
     const WfParams<R> *P;
 };
@@ -164,7 +164,7 @@ __global__ void k_wf_generate(const DevScene<R> S, const WfParams<R> *P, int bat
         for (int k = 0; k < kNeeSlots * 3; ++k) nee[(size_t)q * kNeeSlots * 3 + k] = R(0);
         if (A.verts) {  // adjoint replay: no vertex pending, no NEE transmittance yet
             A.verts[q].mat = -1;
-            for (int k = 0; k < kNeeSlots * 3; ++k) A.att[(size_t)q * kNeeSlots * 3 + k] = R(0);
+            for (int k = 0; k < kNeeSlots * kAttStride; ++k) A.att[(size_t)q * kNeeSlots * kAttStride + k] = R(0);
         }
         paths[q] = st;
         bool live = length_sq(d) > R(0);  // degenerate primary ray: zero radiance
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
         hits = sorted_hits;
     }
     __shared__ float adj_g[ADJ ? kAdjMaxParams : 1];
-    const AdjCtx ctx{adj_g, kParamsPerMaterial * S.material_count};
+    const AdjCtx ctx = make_adj_ctx(adj_g, S.material_count);
     if constexpr (ADJ) adj_block_begin(adj_g, A.P);
     const int n = C->ray_count[which];
     const int stride = gridDim.x * blockDim.x;
@@ -291,15 +291,16 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
             throughput = v3(st.throughput[0], st.throughput[1], st.throughput[2]);
             radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
             if (b > 0) gather_nee(S, nee + (size_t)slot * kNeeSlots * 3, &radiance);
-            V3<R> adj = zero;
+            V3<R> adj = zero, Lp = zero;
             if constexpr (ADJ) {
                 adj = adj_of_path(A.P, slot);
+                const R *Lq = A.L + 3 * (size_t)slot;
+                Lp = v3(Lq[0], Lq[1], Lq[2]);
                 const AdjVertex<R> pv = A.verts[slot];
                 if (pv.mat >= 0) {
-                    const R *Lq = A.L + 3 * (size_t)slot;
-                    R *att = A.att + (size_t)slot * kNeeSlots * 3;
-                    vertex_adjoint(S, pv, att, st.seed_key, sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj, ctx);
-                    for (int k = 0; k < kNeeSlots * 3; ++k) att[k] = R(0);
+                    R *att = A.att + (size_t)slot * kNeeSlots * kAttStride;
+                    vertex_adjoint(S, pv, att, st.seed_key, sub(Lp, radiance), adj, ctx);
+                    for (int k = 0; k < kNeeSlots * kAttStride; ++k) att[k] = R(0);
                 }
             }
             const V3<R> ro = v3(r.o[0], r.o[1], r.o[2]);
@@ -307,7 +308,10 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
             if (hh.prim < 0) {
                 // escaped: medium fallback depth then the sky (src/pathtrace.c:837-857)
                 if (st.medium >= 0) {
+                    const V3<R> beta_in = throughput;
                     pt_apply_medium(S.materials[st.medium], R(5.0), &throughput, &radiance);
+                    if constexpr (ADJ)
+                        medium_grad(ctx, S.materials[st.medium], st.medium, R(5.0), beta_in, sub(Lp, radiance), adj);
                     st.medium = -1;
                 }
                 radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
@@ -321,7 +325,12 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
                 th.code = hh.code;
                 SurfaceHit<R> h;
                 finish_hit(S, ro, unit_dir(d), th, &h);
-                if (st.medium >= 0) pt_apply_medium(S.materials[st.medium], h.t, &throughput, &radiance);
+                if (st.medium >= 0) {
+                    const V3<R> beta_in = throughput;
+                    pt_apply_medium(S.materials[st.medium], h.t, &throughput, &radiance);
+                    if constexpr (ADJ)
+                        medium_grad(ctx, S.materials[st.medium], st.medium, h.t, beta_in, sub(Lp, radiance), adj);
+                }
                 if (h.material < 0 || h.material >= S.material_count) {
                     radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
                     if constexpr (ADJ) sky_sun_grad(ctx, d, S.sky, mul(adj, throughput));
@@ -578,9 +587,13 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, 
         V3<R> o = v3(s.o[0], s.o[1], s.o[2]);
         V3<R> d = v3(s.d[0], s.d[1], s.d[2]);
         V3<R> atten;
+        AbsorbPath<R> ab;
+        ab.mat[0] = ab.mat[1] = -1;
+        ab.dist[0] = ab.dist[1] = R(0);
         bool occ;
         if (S.has_passthrough) {
-            occ = pt_occluded_segment(S, o, d, R(1e-3), s.tmax, &atten);
+            occ = ADJ ? pt_occluded_segment_abs(S, o, d, R(1e-3), s.tmax, &atten, &ab)
+                      : pt_occluded_segment(S, o, d, R(1e-3), s.tmax, &atten);
         } else {
             // No material lets a shadow ray through: the chained nearest-hit
             // walk stops at its first hit, so it equals an any-hit query.
@@ -603,9 +616,12 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, 
         slot[1] = res.y;
         slot[2] = res.z;
         if constexpr (ADJ) {
-            att[at] = lit ? atten.x : R(0);
-            att[at + 1] = lit ? atten.y : R(0);
-            att[at + 2] = lit ? atten.z : R(0);
+            R *rec = att + ((size_t)s.slot * kNeeSlots + s.li) * kAttStride;
+            if (lit) {
+                set_att(rec, atten, ab);
+            } else {
+                for (int k = 0; k < kAttStride; ++k) rec[k] = R(0);
+            }
         }
     }
 }
@@ -711,9 +727,10 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_dyn(const DevScene<R>
                 nee[at + 1] = lit ? s.contrib[1] : R(0);
                 nee[at + 2] = lit ? s.contrib[2] : R(0);
                 if constexpr (ADJ) {
-                    att[at] = lit ? R(1) : R(0);
-                    att[at + 1] = lit ? R(1) : R(0);
-                    att[at + 2] = lit ? R(1) : R(0);
+                    R *rec = att + ((size_t)s.slot * kNeeSlots + s.li) * kAttStride;
+                    for (int k = 0; k < kAttStride; ++k) rec[k] = R(0);
+                    if (lit) rec[0] = rec[1] = rec[2] = R(1);
+                    rec[5] = rec[6] = R(-1);
                 }
                 q = -1;
             }
@@ -750,7 +767,7 @@ template <typename R>
 __global__ void k_wf_finalize_adj(const DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
 {
     __shared__ float adj_g[kAdjMaxParams];
-    const AdjCtx ctx{adj_g, kParamsPerMaterial * S.material_count};
+    const AdjCtx ctx = make_adj_ctx(adj_g, S.material_count);
     adj_block_begin(adj_g, A.P);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_paths; q += gridDim.x * blockDim.x) {
         const AdjVertex<R> pv = A.verts[q];
@@ -759,7 +776,7 @@ __global__ void k_wf_finalize_adj(const DevScene<R> S, int n_paths, const WfPath
         V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
         gather_nee(S, nee + (size_t)q * kNeeSlots * 3, &radiance);
         const R *Lq = A.L + 3 * (size_t)q;
-        vertex_adjoint(S, pv, A.att + (size_t)q * kNeeSlots * 3, st.seed_key,
+        vertex_adjoint(S, pv, A.att + (size_t)q * kNeeSlots * kAttStride, st.seed_key,
                        sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj_of_path(A.P, q), ctx);
     }
     adj_block_end(adj_g, A.P);

@@ -139,7 +139,7 @@ template <typename R> int wf_reserve_adj(WavefrontState *st)
 {
     if (st->adj_verts) return 0;
     WF_CK(cudaMalloc(&st->adj_verts, st->cap_paths * sizeof(AdjVertex<R>)), "cudaMalloc(adjoint vertices)");
-    WF_CK(cudaMalloc(&st->adj_att, st->cap_paths * kNeeSlots * 3 * sizeof(R)), "cudaMalloc(adjoint nee)");
+    WF_CK(cudaMalloc(&st->adj_att, st->cap_paths * kNeeSlots * kAttStride * sizeof(R)), "cudaMalloc(adjoint nee)");
     return 0;
 }
 

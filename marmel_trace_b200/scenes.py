@@ -285,12 +285,45 @@ def adjoint_scene(seed: int = 4, n_spheres: int = 128, n_materials: int = 32, n_
                      camera=dict(eye=(0.0, 6.0, -18.0), target=(0.0, 0.5, 0.0), up=(0.0, 1.0, 0.0), vfov=50.0))
 
 
+def water_scene(seed: int = 6, n_spheres: int = 16) -> SceneDesc:
+    """A water surface (two triangles at y = 0, the water preset with
+    Beer-Lambert absorption) over a sandy ground at y = -3, spheres above and
+    below the surface, one emissive sphere light, sun and sky. Paths refract
+    into the water (medium segments) and shadow rays from under water cross
+    the surface: both absorption terms of the adjoint are exercised."""
+    rng = np.random.default_rng(seed)
+    water = water_material()
+    mats = [material(albedo=(0.76, 0.70, 0.50)),  # ground: Lambert sand
+            water,
+            light_material((1.0, 0.9, 0.8), 12.0)]
+    for _ in range(6):
+        mats.append(material(albedo=tuple(rng.uniform(0.2, 0.9, 3)), roughness=float(rng.uniform(0.1, 0.7)),
+                             metallic=float(rng.uniform(0.0, 1.0)), pbr=1))
+    S = 12.0
+    prims = prims_array(3 + n_spheres + 1)
+    set_plane(prims[0], (0.0, -3.0, 0.0), (0.0, 1.0, 0.0), 0)
+    for k, tri in enumerate((((-S, 0.0, -S), (S, 0.0, -S), (S, 0.0, S)), ((-S, 0.0, -S), (S, 0.0, S), (-S, 0.0, S)))):
+        p = prims[1 + k]
+        p["kind"] = PRIM_TRIANGLE
+        p["material"] = 1
+        p["v"] = np.array(tri, np.float64).ravel()
+    for i in range(n_spheres):
+        r = float(rng.uniform(0.4, 1.2))
+        y = float(rng.uniform(-2.6, 1.5))
+        set_sphere(prims[3 + i], (float(rng.uniform(-6, 6)), y, float(rng.uniform(-6, 6))), r, 3 + int(rng.integers(0, 6)))
+    set_sphere(prims[3 + n_spheres], (2.0, 4.0, -1.0), 0.6, 2)
+    return SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=default_sky(),
+                     camera=dict(eye=(0.0, 5.0, -14.0), target=(0.0, -1.5, 0.0), up=(0.0, 1.0, 0.0), vfov=50.0))
+
+
 def material_params(desc: SceneDesc) -> np.ndarray:
     """Flat parameter vector of the adjoint: per material albedo rgb,
-    roughness, metallic, emissive rgb; then the sun radiance rgb."""
+    roughness, metallic, emissive rgb; then the sun radiance rgb; then per
+    material the absorption rgb."""
     m = desc.materials
     per = np.concatenate([m["albedo"], m["roughness"][:, None], m["metallic"][:, None], m["emissive"]], axis=1)
-    return np.concatenate([per.ravel(), np.asarray(desc.sky["sun_color"], np.float64)])
+    return np.concatenate([per.ravel(), np.asarray(desc.sky["sun_color"], np.float64),
+                           np.asarray(m["absorption"], np.float64).ravel()])
 
 
 def with_params(desc: SceneDesc, params: np.ndarray) -> SceneDesc:
@@ -303,6 +336,9 @@ def with_params(desc: SceneDesc, params: np.ndarray) -> SceneDesc:
     mats["roughness"] = per[:, 3]
     mats["metallic"] = per[:, 4]
     mats["emissive"] = per[:, 5:8]
+    base = PARAMS_PER_MATERIAL * n + 3
+    if len(p) >= base + 3 * n:
+        mats["absorption"] = p[base: base + 3 * n].reshape(n, 3)
     sky = dict(desc.sky)
     sky["sun_color"] = tuple(float(x) for x in p[PARAMS_PER_MATERIAL * n: PARAMS_PER_MATERIAL * n + 3])
     return SceneDesc(prims=desc.prims, materials=mats, sky=sky, water_level=desc.water_level,

@@ -7,7 +7,7 @@
  * ray generation, random streams, BVH queries, shadow segments and BSDF
  * direction sampling are the reference's code. What depends on the
  * differentiated parameters -- per-material albedo, roughness, metallic and
- * emissive, and the sun radiance -- is restated below on a dual number
+ * emissive, absorption, and the sun radiance -- is restated below on a dual number
  * (value, tangent), following the reference line by line:
  *   pathtrace_radiance          src/pathtrace.c:800-1028
  *   pt_nee_sun / pt_nee_emissive src/pathtrace.c:534-606
@@ -136,9 +136,26 @@ inline double pow_nonneg(double b, double e) { return b <= 0.0 ? 0.0 : pow(b, e)
 
 // ---------------------------------------------------------------- parameters
 struct DMat {
-    DV3 albedo, emissive;
+    DV3 albedo, emissive, absorption;
     D roughness, metallic;
 };
+
+inline D dexp(D a)
+{
+    double e = exp(a.v);
+    return {e, e * a.d};
+}
+
+// water_transmittance (src/material.c:1223-1236) with a tangent. The
+// reference returns 1 for a zero coefficient; exp(-0 * d) is that same 1, and
+// the derivative there is the limit -d (what finite differences see).
+inline D water_transmittance_d(D a, double depth)
+{
+    D t = dexp(-1.0 * a * depth);
+    if (!(t.v > 0.0)) return dc(0.0);
+    if (t.v > 1.0) return dc(1.0);
+    return t;
+}
 
 struct Params {
     const Scene *scene;
@@ -259,6 +276,37 @@ DV3 sky_sample_d(Vec3 dir, const SkyParams *sky, const DV3 &sun_color)
     return base;
 }
 
+// pt_occluded_segment (src/pathtrace.c:504-532) with the transmittance of
+// water / beer_lambert surfaces carrying the absorption tangents
+bool occluded_segment_d(const Params &pr, Ray r, double tmin, double tmax, DV3 *attenuation)
+{
+    const Scene *scene = pr.scene;
+    *attenuation = dv(vec3(1.0, 1.0, 1.0));
+    Ray cur = r;
+    double remaining = tmax;
+    for (int step = 0; step < 6; ++step) {
+        Hit h;
+        if (!scene_intersect(scene, cur, tmin, remaining, &h)) return false;
+        const Material *m = scene_material(scene, h.material_index);
+        if (m == NULL) return true;
+        if (m->is_water || m->transparency > 0.8) {
+            if (m->beer_lambert || m->is_water) {
+                const DMat &p = pr.mats[h.material_index];
+                DV3 seg = {dexp(-1.0 * p.absorption.x * h.t), dexp(-1.0 * p.absorption.y * h.t),
+                           dexp(-1.0 * p.absorption.z * h.t)};
+                *attenuation = mul(*attenuation, seg);
+            }
+            cur.origin = vec3_add(h.point, vec3_scale(cur.dir, 1e-3));
+            remaining -= h.t;
+            if (remaining <= 1e-3) return false;
+            tmin = 1e-3;
+            continue;
+        }
+        return true;
+    }
+    return true;
+}
+
 // pt_nee_sun (src/pathtrace.c:534-556)
 DV3 nee_sun_d(const Params &pr, const Material *mm, const DMat &p, Vec3 P, Vec3 N, Vec3 V, const DV3 &throughput,
               unsigned seed_key, int bounce)
@@ -273,11 +321,11 @@ DV3 nee_sun_d(const Params &pr, const Material *mm, const DMat &p, Vec3 P, Vec3 
     Ray sr;
     sr.origin = vec3_add(P, vec3_scale(N, 1e-3));
     sr.dir = L;
-    Vec3 atten;
-    if (refpt::pt_occluded_segment(scene, sr, 1e-3, 1e30, &atten)) return zero;
+    DV3 atten;
+    if (occluded_segment_d(pr, sr, 1e-3, 1e30, &atten)) return zero;
     Vec3 cloud_trans = sky_cloud_transmittance(&scene->sky, sr.origin, sr.dir);
-    atten = vec3_mul(atten, cloud_trans);
-    if (atten.x < 1e-4 && atten.y < 1e-4 && atten.z < 1e-4) return zero;
+    atten = mul(atten, cloud_trans);
+    if (atten.x.v < 1e-4 && atten.y.v < 1e-4 && atten.z.v < 1e-4) return zero;
     double rad = scene->sky.sun_radius * 3.14159265358979323846 / 180.0;
     double Omega = (scene->sky.sun_radius > 0.0) ? 2.0 * 3.14159265358979323846 * (1.0 - cos(rad)) : 1.0;
     DV3 sun_col = mul(pr.sun_color, atten);
@@ -312,8 +360,8 @@ DV3 nee_emissive_d(const Params &pr, const Material *mm, const DMat &p, Vec3 P, 
         sr.dir = wi;
         Hit lh;
         if (!primitive_intersect(&scene->geo.prims[lt->prim_index], sr, 1e-3, 1e30, &lh)) continue;
-        Vec3 atten;
-        if (refpt::pt_occluded_segment(scene, sr, 1e-3, lh.t - 1e-3, &atten)) continue;
+        DV3 atten;
+        if (occluded_segment_d(pr, sr, 1e-3, lh.t - 1e-3, &atten)) continue;
         int lmat = scene->geo.prims[lt->prim_index].material_index;
         DV3 le = (lmat >= 0 && lmat < scene->material_count) ? pr.mats[lmat].emissive : dv(lt->emissive);
         DV3 emit_col = mul(le, atten);
@@ -380,12 +428,27 @@ DV3 sample_weight_d(const Material *m, const DMat &p, Vec3 N, Vec3 d, Vec3 V, do
 
 inline bool finite_d(const DV3 &a) { return isfinite(a.x.v) && isfinite(a.y.v) && isfinite(a.z.v); }
 
-// pt_apply_medium (src/pathtrace.c:220-233)
-void apply_medium_d(const Material *m, double dist, DV3 *beta, DV3 *radiance)
+// water_attenuate (src/material.c:1238-1267) with the medium's dual absorption
+DV3 water_attenuate_d(const Material *m, const DMat &p, Vec3 inner, double depth)
 {
-    Vec3 white = water_attenuate(m, vec3(1.0, 1.0, 1.0), dist);
-    Vec3 deep = water_attenuate(m, vec3(0.0, 0.0, 0.0), dist);
-    Vec3 transmittance = vec3_sub(white, deep);
+    double d = depth > 0.0 ? depth : 0.0;
+    DV3 tr = {water_transmittance_d(p.absorption.x, d), water_transmittance_d(p.absorption.y, d),
+              water_transmittance_d(p.absorption.z, d)};
+    DV3 out = {inner.x * tr.x + m->deep_color.x * (1.0 - tr.x), inner.y * tr.y + m->deep_color.y * (1.0 - tr.y),
+               inner.z * tr.z + m->deep_color.z * (1.0 - tr.z)};
+    if (!(out.x.v >= 0.0)) out.x = dc(0.0);
+    if (!(out.y.v >= 0.0)) out.y = dc(0.0);
+    if (!(out.z.v >= 0.0)) out.z = dc(0.0);
+    return out;
+}
+
+// pt_apply_medium (src/pathtrace.c:220-233)
+void apply_medium_d(const Params &pr, const Material *m, double dist, DV3 *beta, DV3 *radiance)
+{
+    const DMat &p = pr.mats[m - pr.scene->materials];
+    DV3 white = water_attenuate_d(m, p, vec3(1.0, 1.0, 1.0), dist);
+    DV3 deep = water_attenuate_d(m, p, vec3(0.0, 0.0, 0.0), dist);
+    DV3 transmittance = sub(white, deep);
     *radiance = add(*radiance, mul(*beta, deep));
     *beta = mul(*beta, transmittance);
 }
@@ -411,13 +474,13 @@ DV3 radiance_d(const Params &pr, Ray primary, int max_depth, unsigned seed_key, 
         Hit h;
         if (!scene_intersect(scene, r, PT_RAY_EPS, PT_RAY_MAX, &h)) {
             if (medium != NULL) {
-                apply_medium_d(medium, PT_MEDIUM_FALLBACK_DEPTH, &throughput, &radiance);
+                apply_medium_d(pr, medium, PT_MEDIUM_FALLBACK_DEPTH, &throughput, &radiance);
                 medium = NULL;
             }
             radiance = add(radiance, mul(throughput, sky_sample_d(r.dir, &scene->sky, pr.sun_color)));
             break;
         }
-        if (medium != NULL) apply_medium_d(medium, h.t, &throughput, &radiance);
+        if (medium != NULL) apply_medium_d(pr, medium, h.t, &throughput, &radiance);
         const Material *m = scene_material(scene, h.material_index);
         if (m == NULL) {
             radiance = add(radiance, mul(throughput, sky_sample_d(r.dir, &scene->sky, pr.sun_color)));
@@ -537,7 +600,7 @@ extern "C" {
 /* Parameter count of the adjoint layout: 8 per material, then the sun rgb. */
 int mtdual_param_count(void *hp)
 {
-    return 8 * ((MtRefHandle *)hp)->scene.material_count + 3;
+    return 11 * ((MtRefHandle *)hp)->scene.material_count + 3;
 }
 
 /*
@@ -569,6 +632,9 @@ int mtdual_pathtrace_grad(void *hp, int w, int h, int s0, int s1, int depth, con
             mats[m].metallic = {src->metallic, k == b + 4 ? 1.0 : 0.0};
             mats[m].emissive = {{src->emissive.x, k == b + 5 ? 1.0 : 0.0}, {src->emissive.y, k == b + 6 ? 1.0 : 0.0},
                                 {src->emissive.z, k == b + 7 ? 1.0 : 0.0}};
+            const int ab = 8 * M + 3 + 3 * m;  // absorption block after the sun
+            mats[m].absorption = {{src->absorption.x, k == ab ? 1.0 : 0.0}, {src->absorption.y, k == ab + 1 ? 1.0 : 0.0},
+                                  {src->absorption.z, k == ab + 2 ? 1.0 : 0.0}};
         }
         const int sb = 8 * M;
         Params pr{scene, mats,

@@ -85,3 +85,21 @@ def test_dual_matches_fd_for_lambert_albedo(oracle):
     fd = _fd(oracle, d, idx, W, H, SPP, DEPTH, adj)
     assert (np.abs(fd) > 1e-6).sum() >= 6
     assert np.allclose(g, fd, rtol=1e-7, atol=1e-10), np.c_[g, fd]
+
+
+def test_dual_matches_fd_for_absorption(oracle):
+    """Beer-Lambert absorption of the water: media on refracted paths and
+    shadow rays through the surface. Depth 2 keeps roulette out, so the
+    detached derivative is the exact one."""
+    d = scenes.water_scene()
+    W, H, SPP, DEPTH = 16, 12, 4, 2
+    adj = _adj(H, W, 3)
+    M = len(d.materials)
+    idx = [8 * M + 3 + 3 * 1 + c for c in range(3)]  # the water material's absorption
+    r = _ref_scene(oracle, d, W, H)
+    g, _, mm = r.dual_grad(W, H, 0, SPP, DEPTH, adj, idx=idx)
+    r.free()
+    assert mm == 0
+    fd = _fd(oracle, d, idx, W, H, SPP, DEPTH, adj, rel=1e-4)
+    assert np.all(np.abs(fd) > 1e-6)
+    assert np.allclose(g, fd, rtol=1e-5, atol=1e-9), np.c_[g, fd]
