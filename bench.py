@@ -285,6 +285,8 @@ def run_ours(args):
     if not args.no_batch:
         batch = batch_bench(torch, local)
 
+    large = large_bench(torch, local) if args.large else None
+
     # time to RMSE 1e-3
     ttr = None
     if len(means) >= 3:
@@ -350,6 +352,7 @@ def run_ours(args):
         "adjoint": adjoint,
         "autotune": tune,
         "batch": batch,
+        "large": large,
         "stage_ms": stage,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -448,6 +451,67 @@ def batch_bench(torch, device: int, lanes: int = 16):
     return out
 
 
+def large_bench(torch, device: int, spp: int = 8, adj_spp: int = 4):
+    """Config 5: the 10M-triangle scene (2048^2 water heightfield + 2M-triangle
+    trees + 200 spheres + 8 emitters, soft sun; seed 5) at 3840x2160, depth
+    12: BVH built on the device, autotuned, one window of `spp` samples timed;
+    then the path-replay adjoint (albedos, absorption, ...) over `adj_spp`."""
+    from marmel_trace_b200 import _capi, scenes
+    from marmel_trace_b200.adjoint import DiffRenderer
+    from marmel_trace_b200.api import GpuScene
+
+    LW, LH, LD = 3840, 2160, 12
+    t0 = time.perf_counter()
+    d = scenes.large_scene()
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    g = GpuScene(d, precision="fp32", integrator="wavefront", bvh_builder=1, device=device)
+    create_s = time.perf_counter() - t0
+    tune = g.autotune(d.make_camera(960, 540), 960, 540, 2, LD)
+    cam = d.make_camera(LW, LH)
+    acc = torch.zeros((LH, LW, 3), device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def window(s0, n):
+        _capi.check(g.lib.mt_render_accumulate_device(g.h, cam.ref, LW, LH, s0, s0 + n, LD, 0, acc.data_ptr(), 0,
+                                                      stream.cuda_stream), "mt_render_accumulate_device")
+
+    window(0, 2)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e[0].record(stream)
+    window(1000, spp)
+    e[1].record(stream)
+    torch.cuda.synchronize()
+    ms = e[0].elapsed_time(e[1])
+    g.set_counting(True)
+    window(2000, 1)
+    st = g.stats()
+    g.release()
+    ch = tune["chosen"]
+    opts = {"traversal": 2 if ch["traversal"] == "dynamic" else 1, "block_size": ch["block"],
+            "bvh_width": ch["bvh_width"], "sort_threshold": 0, "queue_capacity": ch["queue_capacity"]}
+    r = DiffRenderer(d, LW, LH, adj_spp, LD, precision="fp32", integrator="wavefront", bvh_builder=1, device=device,
+                     **opts)
+    img = r.render(s0=3000)
+    torch.cuda.synchronize()
+    e[0].record(stream)
+    r.backward(torch.ones_like(img), s0=3000)
+    e[1].record(stream)
+    torch.cuda.synchronize()
+    adj_ms = e[0].elapsed_time(e[1])
+    n_params = r.n_params
+    r.release()
+    samples = LW * LH * spp
+    return {"workload": "3840x2160, depth 12, 10,374,259 prims: 2048^2 water heightfield (8.38M triangles) + "
+                        "57 trees (1.99M triangles) + 200 glass/metal spheres + 8 emitters + plane, soft sun (seed 5)",
+            "scene_gen_s": round(gen_s, 2), "scene_create_s": round(create_s, 2), "bvh": "device build",
+            "tuned": ch, "spp_timed": spp, "ms": round(ms, 1), "msamples_s": round(samples / ms / 1e3, 2),
+            "mrays_s": round(samples * (st.extension_rays + st.shadow_rays) / (LW * LH) / ms / 1e3, 2),
+            "adjoint": {"spp": adj_spp, "params": n_params, "backward_ms": round(adj_ms, 1),
+                        "backward_msamples_s": round(LW * LH * adj_spp / adj_ms / 1e3, 2)}}
+
+
 def cpu_baseline(desc, cam, spp: int):
     """The reference's own multithreaded path tracer (oracle/_ref) on the same
     scene: a bounded sample of the workload (full frame at `spp`)."""
@@ -524,6 +588,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--large", action="store_true",
+                    help="also run the 10M-triangle water / tree scene at 3840x2160 (tens of seconds)")
     ap.add_argument("--queue-capacity", type=int, default=0,
                     help="path slots per wavefront batch (0: the library default, 8M)")
     args = ap.parse_args()

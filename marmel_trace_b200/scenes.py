@@ -316,6 +316,125 @@ def water_scene(seed: int = 6, n_spheres: int = 16) -> SceneDesc:
                      camera=dict(eye=(0.0, 5.0, -14.0), target=(0.0, -1.5, 0.0), up=(0.0, 1.0, 0.0), vfov=50.0))
 
 
+# ---------------------------------------------------------------------
+# C5: large scene -- water heightfield, trees, spheres (seed 5)
+# ---------------------------------------------------------------------
+def heightfield_triangles(rng: np.random.Generator, grid: int, half: float) -> np.ndarray:
+    """(2 (grid-1)^2, 9) triangles of a grid x grid heightfield over
+    [-half, half]^2: a sum of 8 sines with amplitudes U(0.01, 0.1), random
+    directions, wavelengths U(2, 30) and phases; normals face +Y."""
+    xs = np.linspace(-half, half, grid)
+    X, Z = np.meshgrid(xs, xs, indexing="ij")
+    Y = np.zeros_like(X)
+    for _ in range(8):
+        a = rng.uniform(0.01, 0.1)
+        th = rng.uniform(0.0, 2 * math.pi)
+        k = 2 * math.pi / rng.uniform(2.0, 30.0)
+        Y += a * np.sin(k * (math.cos(th) * X + math.sin(th) * Z) + rng.uniform(0.0, 2 * math.pi))
+    V = np.stack([X, Y, Z], axis=-1)
+    v00, v10, v01, v11 = V[:-1, :-1], V[1:, :-1], V[:-1, 1:], V[1:, 1:]
+    t1 = np.concatenate([v00, v01, v11], axis=-1).reshape(-1, 9)
+    t2 = np.concatenate([v00, v11, v10], axis=-1).reshape(-1, 9)
+    return np.concatenate([t1, t2], axis=0)
+
+
+def tree_triangles(rng: np.random.Generator, n_trees: int, half: float, generations: int = 7,
+                   sides: int = 16) -> np.ndarray:
+    """Procedural trees as tapered-cylinder branches (2 * sides triangles
+    each, no caps): a trunk, then 3 children per branch per generation with
+    length x0.72 and radius x0.62, tilted 25-55 degrees from the parent."""
+    base = np.stack([rng.uniform(-half, half, n_trees), np.full(n_trees, -3.0), rng.uniform(-half, half, n_trees)], 1)
+    dirs = np.tile([0.0, 1.0, 0.0], (n_trees, 1))
+    lens = rng.uniform(6.0, 9.0, n_trees)
+    rads = rng.uniform(0.35, 0.55, n_trees)
+    segs = []
+    for g in range(generations):
+        tops = base + dirs * lens[:, None]
+        segs.append((base, tops, rads, rads * 0.62))
+        if g == generations - 1:
+            break
+        n = len(base)
+        # 3 children: tilt away from the parent direction around a random axis
+        up = np.where(np.abs(dirs[:, 1:2]) < 0.9, np.array([[0.0, 1.0, 0.0]]), np.array([[1.0, 0.0, 0.0]]))
+        t = np.cross(dirs, up)
+        t /= np.linalg.norm(t, axis=1, keepdims=True)
+        bvec = np.cross(dirs, t)
+        kids_b, kids_d = [], []
+        phi0 = rng.uniform(0, 2 * math.pi, n)
+        for c in range(3):
+            phi = phi0 + c * 2 * math.pi / 3
+            tilt = np.radians(rng.uniform(25.0, 55.0, n))
+            side = np.cos(phi)[:, None] * t + np.sin(phi)[:, None] * bvec
+            nd = np.cos(tilt)[:, None] * dirs + np.sin(tilt)[:, None] * side
+            kids_b.append(base + dirs * (lens * rng.uniform(0.6, 1.0, n))[:, None])
+            kids_d.append(nd / np.linalg.norm(nd, axis=1, keepdims=True))
+        base = np.concatenate(kids_b)
+        dirs = np.concatenate(kids_d)
+        lens = np.tile(lens * 0.72, 3)
+        rads = np.tile(rads * 0.62, 3)
+    tris = []
+    ang = np.arange(sides + 1) * (2 * math.pi / sides)
+    for b0, b1, r0, r1 in segs:
+        d = b1 - b0
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        up = np.where(np.abs(d[:, 1:2]) < 0.9, np.array([[0.0, 1.0, 0.0]]), np.array([[1.0, 0.0, 0.0]]))
+        t = np.cross(d, up)
+        t /= np.linalg.norm(t, axis=1, keepdims=True)
+        bb = np.cross(d, t)
+        ring = np.cos(ang)[None, :, None] * t[:, None, :] + np.sin(ang)[None, :, None] * bb[:, None, :]
+        lo = b0[:, None, :] + ring * r0[:, None, None]
+        hi = b1[:, None, :] + ring * r1[:, None, None]
+        a0, a1, c0, c1 = lo[:, :-1], lo[:, 1:], hi[:, :-1], hi[:, 1:]
+        tris.append(np.concatenate([a0, a1, c1], axis=-1).reshape(-1, 9))
+        tris.append(np.concatenate([a0, c1, c0], axis=-1).reshape(-1, 9))
+    return np.concatenate(tris, axis=0)
+
+
+def large_scene(seed: int = 5, grid: int = 2048, n_trees: int = 57, n_spheres: int = 200, n_lights: int = 8,
+                half: float = 100.0) -> SceneDesc:
+    """Config 5: a grid x grid water heightfield (2 (grid-1)^2 triangles; the
+    water preset: IOR 1.33, Beer-Lambert absorption) over a sandy ground
+    plane at y = -3, n_trees procedural trees (about 35k triangles each),
+    n_spheres glass / metal spheres, n_lights emissive spheres, a soft sun
+    (0.5 degree radius). 2048 and 57 give 8.38M + 2.0M triangles."""
+    rng = np.random.default_rng(seed)
+    water = heightfield_triangles(rng, grid, half)
+    tree = tree_triangles(rng, n_trees, 0.8 * half)
+    mats = [material(albedo=(0.76, 0.70, 0.50)),          # 0 sand
+            water_material(),                              # 1 water
+            material(albedo=(0.36, 0.25, 0.16)),           # 2 bark
+            glass_material(),                              # 3 glass
+            material(albedo=(0.9, 0.8, 0.6), metallic=1.0, roughness=0.2, pbr=1),   # 4 gold-ish metal
+            material(albedo=(0.8, 0.8, 0.85), metallic=1.0, roughness=0.05, pbr=1)]  # 5 mirror-like metal
+    first_light = len(mats)
+    for _ in range(n_lights):
+        mats.append(light_material(tuple(rng.uniform(0.7, 1.0, 3)), float(rng.uniform(5.0, 20.0))))
+    n = 1 + len(water) + len(tree) + n_spheres + n_lights
+    prims = prims_array(n)
+    set_plane(prims[0], (0.0, -3.0, 0.0), (0.0, 1.0, 0.0), 0)
+    w = prims[1:1 + len(water)]
+    w["kind"] = PRIM_TRIANGLE
+    w["material"] = 1
+    w["v"] = water
+    t = prims[1 + len(water):1 + len(water) + len(tree)]
+    t["kind"] = PRIM_TRIANGLE
+    t["material"] = 2
+    t["v"] = tree
+    base = 1 + len(water) + len(tree)
+    for i in range(n_spheres):
+        r = float(rng.uniform(0.5, 2.0))
+        c = (float(rng.uniform(-0.8 * half, 0.8 * half)), float(rng.uniform(-2.0, 3.0)),
+             float(rng.uniform(-0.8 * half, 0.8 * half)))
+        set_sphere(prims[base + i], c, r, 3 + int(rng.integers(0, 3)))
+    for k in range(n_lights):
+        c = (float(rng.uniform(-0.6 * half, 0.6 * half)), float(rng.uniform(6.0, 12.0)),
+             float(rng.uniform(-0.6 * half, 0.6 * half)))
+        set_sphere(prims[base + n_spheres + k], c, 0.8, first_light + k)
+    return SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=default_sky(sun_radius=0.5),
+                     camera=dict(eye=(0.0, 8.0, -0.95 * half), target=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0),
+                                 vfov=50.0))
+
+
 def material_params(desc: SceneDesc) -> np.ndarray:
     """Flat parameter vector of the adjoint: per material albedo rgb,
     roughness, metallic, emissive rgb; then the sun radiance rgb; then per

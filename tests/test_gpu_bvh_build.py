@@ -67,3 +67,19 @@ def test_device_build_time(mtlib):
     dev_wall = time.perf_counter() - t0
     print(f"host build {host_s:.2f} s; device build {ms:.1f} ms device time, {dev_wall:.2f} s wall per call")
     assert len(hb) == len(db)
+
+
+def test_large_scene_shape_matches_reference(mtlib, oracle):
+    """A scaled-down version of the large configuration (water heightfield,
+    trees, spheres, emitters, soft sun) built on the device: the FP64 image
+    equals the reference's except where rays meet the water near the
+    critical angle (last-ulp cos / sin differences amplified by refraction)."""
+    d = scenes.large_scene(grid=64, n_trees=2, n_spheres=20)
+    w, h = 96, 64
+    cam = d.make_camera(w, h)
+    rs = oracle.RefScene.from_desc(d, cam)
+    want = rs.pathtrace_render(w, h, 4, 12)
+    rs.free()
+    with mt.GpuScene(d, precision="fp64", integrator="wavefront", bvh_builder=1) as g:
+        got = g.pathtrace(cam, w, h, 4, 12)
+    assert (got != want).mean() < 2e-3
