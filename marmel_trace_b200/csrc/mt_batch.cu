@@ -200,7 +200,10 @@ int mt_batch_render(mt_batch *b, int32_t n, const mt_batch_item *items, void *st
                                                       (size_t)(S0.stack_depth > 0 ? S0.stack_depth : 1) * 128 * 4);
         b->grid = sms * (per_sm > 0 ? per_sm : 1);
     }
-    for (int l = 0; l < b->lanes; ++l) b->st[l]->grid = b->grid;
+    for (int l = 0; l < b->lanes; ++l) {
+        b->st[l]->grid = b->grid;
+        b->st[l]->occ_cache_on = false;  // a lane renders several scenes
+    }
     // ---- parameter blocks ----
     if (n > b->params_cap) {
         if (b->params) cudaFree(b->params);

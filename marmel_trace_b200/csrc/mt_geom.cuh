@@ -523,6 +523,7 @@ template <typename R> struct Trav {
     int node;   // next node to visit, kEmpty when the walk is over
     int sp;     // stack entries in use
     bool found;
+    int any_code;  // any hit: the tree primitive that blocked (kind << 28 | slot), -1 for a plane
 };
 
 // Nearest hit (ANY = false) or any hit (ANY = true) in [tmin, tmax].
@@ -543,6 +544,7 @@ MT_D void trav_init(const DevScene<R> &S, Trav<R> &tv, const RayPre<R> &rp, R tm
     tv.closest = tmax;
     tv.found = false;
     tv.sp = 0;
+    tv.any_code = -1;
     for (int i = 0; i < S.plane_count; ++i) {
         R t;
         ++c.ntest;
@@ -582,6 +584,7 @@ MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, T
             if (tri_t(S, first + i, rp, tmin, tv.closest, &t, &u, &v)) {
                 if (ANY) {
                     tv.found = true;
+                    tv.any_code = (KIND_TRIANGLE << 28) | (first + i);
                     break;
                 }
                 int pi = tri_prim_index(S, first + i);
@@ -607,6 +610,7 @@ MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, T
             if (hit) {
                 if (ANY) {
                     tv.found = true;
+                    tv.any_code = ref.y;
                     break;
                 }
                 if (!tv.found || t < best->t || (t == best->t && ref.x < best->prim)) {
@@ -801,6 +805,31 @@ template <typename R, int W = 2> MT_D bool scene_any(const DevScene<R> &S, const
 {
     Hit<R> dummy;
     return traverse<R, true, W>(S, rp, tmin, tmax, &dummy);
+}
+
+// Any hit that first tries the primitive in *cache (kind << 28 | slot, -1
+// none) -- a hit there is a hit of the query, so the answer is the same --
+// and otherwise walks the tree and leaves the blocking primitive in *cache.
+template <typename R, int W = 2>
+MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, int *cache)
+{
+    const int c = *cache;
+    if (c >= 0 && prim_occluded(S, c, rp, tmin, tmax)) {
+        if (S.counters) count_add(&S.counters->any_prim_tests, 1ull);
+        return true;
+    }
+    TravCount cnt;
+    Trav<R> tv;
+    Hit<R> dummy;
+    trav_init<R, true>(S, tv, rp, tmin, tmax, &dummy, cnt);
+    if (tv.node != kEmpty) {
+        int *stk = mt_stack_smem + threadIdx.x;
+        while (trav_step<R, true, W>(S, tv, stk, blockDim.x, &dummy, cnt)) {
+        }
+    }
+    trav_count_flush<R, true>(S, cnt);
+    if (tv.found && tv.any_code >= 0 && tv.any_code != c) *cache = tv.any_code;
+    return tv.found;
 }
 
 // scene_intersect / scene_occluded entry semantics: a direction that is not

@@ -577,9 +577,13 @@ __global__ void k_wf_sort_scatter(const DevScene<R> S, const WfCounters *C, int 
 // ------------------------------------------------------------------
 // ADJ: also keep the connection's transmittance (zero when it adds no light)
 // for the replay's gradient terms.
+//
+// occ_cache (may be NULL): per pixel and NEE slot, the primitive that last blocked
+// that pixel's bounce-0 connection (see scene_any_cached); used at b == 0,
+// where the samples of a pixel shade nearly the same point.
 template <typename R, bool ADJ, int W>
 __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
-                                                   R *nee, R *att)
+                                                   R *nee, R *att, int *occ_cache, int wh, int b)
 {
     const int n = C->shadow_count;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -599,7 +603,11 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, 
             // walk stops at its first hit, so it equals an any-hit query.
             atten = v3(R(1), R(1), R(1));
             if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
-            occ = scene_any<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
+            if (occ_cache && b == 0)
+                occ = scene_any_cached<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax,
+                                             occ_cache + (size_t)(s.slot % wh) * kNeeSlots + s.li);
+            else
+                occ = scene_any<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
         }
         V3<R> res = v3(R(0), R(0), R(0));
         bool lit = false;

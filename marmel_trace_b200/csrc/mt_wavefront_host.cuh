@@ -41,6 +41,11 @@ struct WavefrontState {
     void *sorted_rays = nullptr, *sorted_hits = nullptr, *sort_keys = nullptr, *sort_buckets = nullptr;
     int sort_bucket_cap = 0;
     int grid_block = 0;        // block size the persistent grid was sized for
+    // per pixel and NEE slot, the primitive that last blocked the pixel's
+    // bounce-0 shadow ray (k_wf_shadow); only for a state that serves one
+    // scene (a batch lane renders several, so it turns this off)
+    void *occ_cache = nullptr;
+    bool occ_cache_on = true;
     int grid = 0;              // persistent grid (blocks) of the stage kernels
     cudaEvent_t kev[64];       // per-kernel timing events (profiling mode)
     bool kev_init = false;
@@ -72,7 +77,8 @@ inline void wf_free(WavefrontState *st)
 {
     void **bufs[] = {&st->paths,       &st->rays[0],    &st->rays[1],     &st->hits,        &st->nee,
                      &st->shadow,      &st->sample_buf, &st->acc,         &st->params,      &st->adj_verts,
-                     &st->adj_att,     &st->sorted_rays, &st->sorted_hits, &st->sort_keys, &st->sort_buckets};
+                     &st->adj_att,     &st->sorted_rays, &st->sorted_hits, &st->sort_keys, &st->sort_buckets,
+                     &st->occ_cache};
     for (void **b : bufs) {
         if (*b) cudaFree(*b);
         *b = nullptr;
@@ -128,6 +134,8 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
     WF_CK(cudaMalloc(&st->acc, wh * 3 * sizeof(R)), "cudaMalloc(acc)");
     WF_CK(cudaMalloc(&st->params, sizeof(WfParams<R>)), "cudaMalloc(params)");
     WF_CK(cudaMalloc((void **)&st->counters, sizeof(WfCounters)), "cudaMalloc(counters)");
+    WF_CK(cudaMalloc(&st->occ_cache, wh * kNeeSlots * sizeof(int)), "cudaMalloc(occluder cache)");
+    WF_CK(cudaMemset(st->occ_cache, 0xFF, wh * kNeeSlots * sizeof(int)), "cudaMemset(occluder cache)");
     if (!st->h_params) WF_CK(cudaMallocHost(&st->h_params, 256), "cudaMallocHost(params)");
     st->cap_paths = n_paths;
     st->acc_pixels = wh;
@@ -157,23 +165,23 @@ void launch_extend(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
 
 template <typename R, bool ADJ, int W>
 void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
-                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att)
+                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b)
 {
     if (dyn && !S.has_passthrough)
         k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
     else
-        k_wf_shadow<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
+        k_wf_shadow<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b);
 }
 
 template <typename R, bool ADJ>
 void launch_shadow_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
-                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att)
+                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b)
 {
     if constexpr (sizeof(R) == 4) {
-        if (W == 4) return launch_shadow<R, ADJ, 4>(dyn, g, block, smem, s, S, sq, C, nee, att);
-        if (W == 8) return launch_shadow<R, ADJ, 8>(dyn, g, block, smem, s, S, sq, C, nee, att);
+        if (W == 4) return launch_shadow<R, ADJ, 4>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b);
+        if (W == 8) return launch_shadow<R, ADJ, 8>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b);
     }
-    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att);
+    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b);
 }
 
 template <typename R>
@@ -253,6 +261,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         st->kernel_launches[kind] += 1;
         ev += 2;
     };
+    int *occ = st->occ_cache_on ? (int *)st->occ_cache : nullptr;
     const WfAdj<R> none{nullptr, nullptr, nullptr, P};
     const WfAdj<R> A{(AdjVertex<R> *)st->adj_verts, (R *)st->adj_att, sample_buf, P};
     // generate -> (extend, shade, shadow) x (depth + 1); the replay pass uses
@@ -297,9 +306,9 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             toc(1);
             tic();
             if (replay)
-                launch_shadow_w<R, true>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, A.att);
+                launch_shadow_w<R, true>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, A.att, occ, wh, b);
             else
-                launch_shadow_w<R, false>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, nullptr);
+                launch_shadow_w<R, false>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, nullptr, occ, wh, b);
             toc(2);
             which ^= 1;
         }
