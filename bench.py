@@ -60,6 +60,25 @@ def _dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def max_over_ranks(x: float, dist=None, device="cpu") -> float:
+    """The largest per-rank value over the process group (the slowest rank's
+    time). Every rank must call it, in the same order; without a process group
+    it returns `x`."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, world: int, seconds: float) -> float:
+    """Whole-job throughput in millions of units per second: every replica
+    processes `units_per_rank`, and the job ends with the slowest rank."""
+    return units_per_rank * world / seconds / 1e6
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -228,13 +247,9 @@ def run_ours(args):
         t_wall = time.perf_counter() - t_wall
     if dist:
         dist.barrier()
-    dev_s = sum(ms) / 1e3
-    if dist:
-        t = torch.tensor([dev_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_s = float(t.item())
+    dev_s = max_over_ranks(sum(ms) / 1e3, dist, "cuda")
     samples_per_rank = W * H * SPP * args.steps
-    value = samples_per_rank * world / dev_s / 1e6
+    value = whole_job_rate(samples_per_rank, world, dev_s)
     launches = int(g.stats().launches)
 
     # e2e through the drop-in entry point (host camera in, host RGB8 out)
@@ -245,7 +260,8 @@ def run_ours(args):
         t0 = time.perf_counter()
         _capi.check(g.lib.mt_pathtrace_render(g.h, cam.ref, W, H, SPP, DEPTH, rgb.ctypes.data), "mt_pathtrace_render")
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_val = W * H * SPP / (statistics.median(e2e_ms) / 1e3) / 1e6 * world if e2e_ms else None
+    e2e_val = whole_job_rate(W * H * SPP, world, max_over_ranks(statistics.median(e2e_ms) / 1e3, dist, "cuda")) \
+        if e2e_ms else None
 
     # dominant-kernel duration: one frame with every stage bracketed by events
     stage = None
