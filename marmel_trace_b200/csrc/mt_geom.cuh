@@ -28,6 +28,7 @@ template <typename R> struct Hit {
 // Per-ray precomputation shared by every node and primitive test.
 template <typename R> struct RayPre {
     V3<R> o, d, inv;
+    V3<R> oi;  // o * inv: an FP32 slab distance is one fma, box * inv - oi
     // watertight-triangle shear (FP32 path)
     int kx, ky, kz;
     float sx, sy, sz;
@@ -40,6 +41,15 @@ template <typename R> MT_D RayPre<R> ray_pre(V3<R> o, V3<R> d)
     p.d = d;
     // 1/dir per component (src/bvh.c:571): IEEE infinities for zero components.
     p.inv = v3<R>(R(1) / d.x, R(1) / d.y, R(1) / d.z);
+    if constexpr (sizeof(R) == 4) {
+        // FP32 slab tests use the fma form, where an infinite inverse would give
+        // inf - inf; a (near-)zero component gets a finite 1e30 of its sign
+        // instead, which orders every slab of the scene the same way.
+        p.inv.x = fabsf(d.x) < 1e-30f ? copysignf(1e30f, d.x) : p.inv.x;
+        p.inv.y = fabsf(d.y) < 1e-30f ? copysignf(1e30f, d.y) : p.inv.y;
+        p.inv.z = fabsf(d.z) < 1e-30f ? copysignf(1e30f, d.z) : p.inv.z;
+    }
+    p.oi = v3<R>(o.x * p.inv.x, o.y * p.inv.y, o.z * p.inv.z);
     float ax = fabsf((float)d.x), ay = fabsf((float)d.y), az = fabsf((float)d.z);
     int kz = (ax > ay) ? ((ax > az) ? 0 : 2) : ((ay > az) ? 1 : 2);
     int kx = kz + 1 == 3 ? 0 : kz + 1;
@@ -348,9 +358,13 @@ MT_D bool tri_t(const DevScene<double> &S, int slot, const RayPre<double> &rp, d
 
 // FP32: watertight test (Woop, Benthin, Wald 2013). Vertices are stored
 // relative to nothing (v0, v1, v2) so the shear is applied to exact
-// differences from the ray origin.
-MT_D bool tri_t(const DevScene<float> &S, int slot, const RayPre<float> &rp, float tmin, float tmax,
-                float *t_out, float *u_out, float *v_out)
+// differences from the ray origin. tri_edges evaluates the edge functions
+// U, V, W (one sign for a hit), det = U + V + W and the scaled distance T, so
+// that t = T / det; false when the ray misses the triangle's edges.
+struct TriEdges {
+    float U, V, W, det, T;
+};
+MT_D bool tri_edges(const DevScene<float> &S, int slot, const RayPre<float> &rp, TriEdges *e)
 {
     const float4 *T = S.tri4 + 3 * (size_t)slot;
     float4 q0 = __ldg(T), q1 = __ldg(T + 1), q2 = __ldg(T + 2);
@@ -376,14 +390,44 @@ MT_D bool tri_t(const DevScene<float> &S, int slot, const RayPre<float> &rp, flo
     float det = U + V + W;
     if (det == 0.0f) return false;
     float Az = rp.sz * Akz, Bz = rp.sz * Bkz, Cz = rp.sz * Ckz;
-    float T_ = U * Az + V * Bz + W * Cz;
-    float rcp = 1.0f / det;
-    float t = T_ * rcp;
+    e->U = U;
+    e->V = V;
+    e->W = W;
+    e->det = det;
+    e->T = U * Az + V * Bz + W * Cz;
+    return true;
+}
+
+MT_D bool tri_t(const DevScene<float> &S, int slot, const RayPre<float> &rp, float tmin, float tmax,
+                float *t_out, float *u_out, float *v_out)
+{
+    TriEdges e;
+    if (!tri_edges(S, slot, rp, &e)) return false;
+    float rcp = 1.0f / e.det;
+    float t = e.T * rcp;
     if (!(t >= tmin && t <= tmax)) return false;
     *t_out = t;
-    *u_out = V * rcp;
-    *v_out = W * rcp;
+    *u_out = e.V * rcp;
+    *v_out = e.W * rcp;
     return true;
+}
+
+// Any-hit form: t = T / det in [tmin, tmax] is decided as T against
+// tmin * det and tmax * det, with det made positive (no division).
+MT_D bool tri_occ(const DevScene<float> &S, int slot, const RayPre<float> &rp, float tmin, float tmax)
+{
+    TriEdges e;
+    if (!tri_edges(S, slot, rp, &e)) return false;
+    const float T = e.det < 0.0f ? -e.T : e.T;
+    const float det = fabsf(e.det);
+    return T >= tmin * det && T <= tmax * det;
+}
+
+// FP64: the any-hit test is the nearest-hit test's boolean.
+MT_D bool tri_occ(const DevScene<double> &S, int slot, const RayPre<double> &rp, double tmin, double tmax)
+{
+    double t, u, v;
+    return tri_t(S, slot, rp, tmin, tmax, &t, &u, &v);
 }
 
 // ------------------------------------------------------------------
@@ -422,7 +466,7 @@ MT_D bool prim_occluded(const DevScene<R> &S, int code, const RayPre<R> &rp, R t
     R t, u, v;
     switch (kind) {
     case KIND_TRIANGLE:
-        return tri_t(S, slot, rp, tmin, tmax, &t, &u, &v);
+        return tri_occ(S, slot, rp, tmin, tmax);
     case KIND_SPHERE:
         return sphere_t(S.spheres + 4 * (size_t)slot, rp, tmin, tmax, &t);
     case KIND_BOX:
@@ -439,10 +483,36 @@ MT_D bool prim_occluded(const DevScene<R> &S, int code, const RayPre<R> &rp, R t
 // ------------------------------------------------------------------
 // Two-child slab test on one 64-byte node (bvh_slab_2way, src/bvh.c:495-533).
 // ------------------------------------------------------------------
+//
+// FP32: one fma per slab plane (box * inv - o * inv). FP64: the reference's
+// (box - o) * inv.
 template <typename R>
 MT_D void node_test(const float4 q0, const float4 q1, const float4 q2, const RayPre<R> &rp, R tmin, R tmax,
-                    bool *hl, bool *hr, R *tl, R *tr)
+                    bool *hl, bool *hr, R *tl, R *tr);
+template <>
+MT_D void node_test<float>(const float4 q0, const float4 q1, const float4 q2, const RayPre<float> &rp, float tmin,
+                           float tmax, bool *hl, bool *hr, float *tl, float *tr)
 {
+    float lx0 = fmaf(q0.x, rp.inv.x, -rp.oi.x), lx1 = fmaf(q0.y, rp.inv.x, -rp.oi.x);
+    float ly0 = fmaf(q0.z, rp.inv.y, -rp.oi.y), ly1 = fmaf(q0.w, rp.inv.y, -rp.oi.y);
+    float lz0 = fmaf(q2.x, rp.inv.z, -rp.oi.z), lz1 = fmaf(q2.y, rp.inv.z, -rp.oi.z);
+    float rx0 = fmaf(q1.x, rp.inv.x, -rp.oi.x), rx1 = fmaf(q1.y, rp.inv.x, -rp.oi.x);
+    float ry0 = fmaf(q1.z, rp.inv.y, -rp.oi.y), ry1 = fmaf(q1.w, rp.inv.y, -rp.oi.y);
+    float rz0 = fmaf(q2.z, rp.inv.z, -rp.oi.z), rz1 = fmaf(q2.w, rp.inv.z, -rp.oi.z);
+    float lenter = fmaxf(fmaxf(fminf(lx0, lx1), fminf(ly0, ly1)), fminf(lz0, lz1));
+    float lexit = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fmaxf(lz0, lz1));
+    float renter = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fminf(rz0, rz1));
+    float rexit = fminf(fminf(fmaxf(rx0, rx1), fmaxf(ry0, ry1)), fmaxf(rz0, rz1));
+    *hl = (lexit >= lenter && lexit >= tmin && lenter <= tmax);
+    *hr = (rexit >= renter && rexit >= tmin && renter <= tmax);
+    *tl = lenter < tmin ? tmin : lenter;
+    *tr = renter < tmin ? tmin : renter;
+}
+template <>
+MT_D void node_test<double>(const float4 q0, const float4 q1, const float4 q2, const RayPre<double> &rp, double tmin,
+                            double tmax, bool *hl, bool *hr, double *tl, double *tr)
+{
+    using R = double;
     R lx0 = (R(q0.x) - rp.o.x) * rp.inv.x, lx1 = (R(q0.y) - rp.o.x) * rp.inv.x;
     R ly0 = (R(q0.z) - rp.o.y) * rp.inv.y, ly1 = (R(q0.w) - rp.o.y) * rp.inv.y;
     R lz0 = (R(q2.x) - rp.o.z) * rp.inv.z, lz1 = (R(q2.y) - rp.o.z) * rp.inv.z;
@@ -581,7 +651,9 @@ MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, T
             R t, u, v;
             ++c.ntest;
             ++c.ntri;
-            if (tri_t(S, first + i, rp, tmin, tv.closest, &t, &u, &v)) {
+            const bool hit = ANY ? tri_occ(S, first + i, rp, tmin, tv.closest)
+                                 : tri_t(S, first + i, rp, tmin, tv.closest, &t, &u, &v);
+            if (hit) {
                 if (ANY) {
                     tv.found = true;
                     tv.any_code = (KIND_TRIANGLE << 28) | (first + i);
@@ -669,9 +741,10 @@ template <typename R>
 MT_D bool box_hit(float lx, float hx, float ly, float hy, float lz, float hz, const RayPre<R> &rp, R tmin, R tmax,
                   R *enter)
 {
-    R x0 = (R(lx) - rp.o.x) * rp.inv.x, x1 = (R(hx) - rp.o.x) * rp.inv.x;
-    R y0 = (R(ly) - rp.o.y) * rp.inv.y, y1 = (R(hy) - rp.o.y) * rp.inv.y;
-    R z0 = (R(lz) - rp.o.z) * rp.inv.z, z1 = (R(hz) - rp.o.z) * rp.inv.z;
+    static_assert(sizeof(R) == 4, "wide trees are an FP32 path");
+    R x0 = fmaf(lx, rp.inv.x, -rp.oi.x), x1 = fmaf(hx, rp.inv.x, -rp.oi.x);
+    R y0 = fmaf(ly, rp.inv.y, -rp.oi.y), y1 = fmaf(hy, rp.inv.y, -rp.oi.y);
+    R z0 = fmaf(lz, rp.inv.z, -rp.oi.z), z1 = fmaf(hz, rp.inv.z, -rp.oi.z);
     R en = mfmax(mfmax(mfmin(x0, x1), mfmin(y0, y1)), mfmin(z0, z1));
     R ex = mfmin(mfmin(mfmax(x0, x1), mfmax(y0, y1)), mfmax(z0, z1));
     *enter = en < tmin ? tmin : en;

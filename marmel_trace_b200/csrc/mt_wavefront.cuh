@@ -495,13 +495,53 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
 }
 
 // ------------------------------------------------------------------
-// sort by material: a counting sort of one bounce's extend results by the
-// material hit (bucket M = no surface), so that the shade kernel's warps see
-// one material, hence one BSDF code path, at a time. It runs only when the
-// queue holds at least `threshold` rays (decided on the device). Queue order
-// never changes a path's result: every path keeps its own slot, NEE slots and
-// sample index. Lanes of a warp with the same key share one atomicAdd.
+// sort by material and place: a counting sort of one bounce's extend results
+// by (material hit, Morton cell of the hit point), bucket M = no surface, so
+// that the shade kernel's warps see one material, hence one BSDF code path, at
+// a time, and consecutive paths sit close together in the scene. The shade
+// kernel appends each warp's NEE connections light by light, so the shadow
+// queue then holds runs of up to 32 rays toward one light from nearby points,
+// which walk nearly the same nodes. The cells split the root box into
+// 2^bits per axis; bits shrinks as the material count grows so the bucket
+// count stays <= kSortMaxBuckets. It runs only when the queue holds at least
+// `threshold` rays (decided on the device). Queue order never changes a
+// path's result: every path keeps its own slot, NEE slots and sample index.
+// Lanes of a warp with the same key share one atomicAdd.
 // ------------------------------------------------------------------
+static constexpr int kSortMaxBuckets = 1 << 16;
+static constexpr int kSortMaxCellBits = 4;
+
+// Cell bits per axis for `keys` material keys (materials + 1).
+MT_HD int sort_cell_bits(int keys)
+{
+    int b = kSortMaxCellBits;
+    while (b > 0 && ((long long)keys << (3 * b)) > kSortMaxBuckets) --b;
+    return b;
+}
+
+// Buckets of the sort: material keys x cells.
+MT_HD int sort_buckets(int keys) { return keys << (3 * sort_cell_bits(keys)); }
+
+// Morton cell (bits per axis) of point p in the root box of the tree.
+template <typename R> MT_D int sort_cell(const DevScene<R> &S, R px, R py, R pz, int bits)
+{
+    if (bits == 0 || S.node_count <= 0) return 0;
+    const float4 q0 = __ldg(S.nodes), q1 = __ldg(S.nodes + 1), q2 = __ldg(S.nodes + 2);
+    const float lo[3] = {fminf(q0.x, q1.x), fminf(q0.z, q1.z), fminf(q2.x, q2.z)};
+    const float hi[3] = {fmaxf(q0.y, q1.y), fmaxf(q0.w, q1.w), fmaxf(q2.y, q2.w)};
+    const float p[3] = {(float)px, (float)py, (float)pz};
+    const int top = (1 << bits) - 1;
+    int cell = 0;
+    for (int k = 0; k < 3; ++k) {
+        const float ext = hi[k] - lo[k];
+        const float f = ext > 0.f ? (p[k] - lo[k]) * ((float)(1 << bits) / ext) : 0.f;
+        int v = f > 0.f ? (int)f : 0;  // NaN and points below the box go to cell 0
+        v = v > top ? top : v;
+        for (int j = 0; j < bits; ++j) cell |= ((v >> j) & 1) << (3 * j + k);
+    }
+    return cell;
+}
+
 MT_D int warp_add_by_key(int *counters, int key, bool want)
 {
     const unsigned active = __ballot_sync(0xffffffffu, want);
@@ -516,22 +556,27 @@ MT_D int warp_add_by_key(int *counters, int key, bool want)
 }
 
 template <typename R>
-__global__ void k_wf_sort_count(const DevScene<R> S, WfCounters *C, int which, const WfHit<R> *hits, int *keys,
-                                int *buckets, int threshold)
+__global__ void k_wf_sort_count(const DevScene<R> S, WfCounters *C, int which, const WfRay<R> *rays,
+                                const WfHit<R> *hits, int *keys, int *buckets, int threshold)
 {
     const int n = C->ray_count[which];
     if (blockIdx.x == 0 && threadIdx.x == 0) C->sorted = n >= threshold;
     if (n < threshold) return;
     const int M = S.material_count;
+    const int bits = sort_cell_bits(M + 1);
     const int stride = gridDim.x * blockDim.x;
     const int n_round = (n + stride - 1) / stride * stride;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
-        int key = M;
+        int key = M << (3 * bits);
         if (q < n) {
-            const int prim = hits[q].prim;
-            if (prim >= 0) {
-                const int m = __ldg(S.prim_info + prim).y;
-                if (m >= 0 && m < M) key = m;
+            const WfHit<R> hq = hits[q];
+            if (hq.prim >= 0) {
+                const int m = __ldg(S.prim_info + hq.prim).y;
+                if (m >= 0 && m < M) {
+                    const WfRay<R> &r = rays[q];
+                    key = (m << (3 * bits)) | sort_cell(S, r.o[0] + hq.t * r.d[0], r.o[1] + hq.t * r.d[1],
+                                                        r.o[2] + hq.t * r.d[2], bits);
+                }
             }
             keys[q] = key;
         }
@@ -539,27 +584,52 @@ __global__ void k_wf_sort_count(const DevScene<R> S, WfCounters *C, int which, c
     }
 }
 
-// exclusive scan of the bucket counts into the cursors (one thread: the
-// bucket count is the material count + 1)
-template <typename R> __global__ void k_wf_sort_scan(const DevScene<R> S, const WfCounters *C, int *buckets)
+// Exclusive scan of the nb bucket counts into the cursors (buckets[nb..2nb)):
+// one block of kSortScanThreads, each thread a contiguous run of buckets.
+static constexpr int kSortScanThreads = 1024;
+template <typename R>
+__global__ void __launch_bounds__(kSortScanThreads) k_wf_sort_scan(const WfCounters *C, int *buckets, int nb)
 {
-    if (!C->sorted || threadIdx.x != 0) return;
-    const int nb = S.material_count + 1;
-    int acc = 0;
-    for (int k = 0; k < nb; ++k) {
+    __shared__ int warp_sum[kSortScanThreads / 32];
+    if (!C->sorted) return;
+    const int per = (nb + kSortScanThreads - 1) / kSortScanThreads;
+    const int b0 = threadIdx.x * per;
+    const int b1 = min(b0 + per, nb);
+    int sum = 0;
+    for (int k = b0; k < b1; ++k) sum += buckets[k];
+    // inclusive scan of the thread sums: within the warp, then across warps
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = sum;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int w = warp_sum[lane];
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        warp_sum[lane] = w;
+    }
+    __syncthreads();
+    int acc = x - sum + (wid > 0 ? warp_sum[wid - 1] : 0);
+    for (int k = b0; k < b1; ++k) {
         buckets[nb + k] = acc;
         acc += buckets[k];
     }
 }
 
 template <typename R>
-__global__ void k_wf_sort_scatter(const DevScene<R> S, const WfCounters *C, int which, const WfRay<R> *rays,
-                                  const WfHit<R> *hits, const int *keys, int *buckets, WfRay<R> *sorted_rays,
+__global__ void k_wf_sort_scatter(const WfCounters *C, int which, const WfRay<R> *rays, const WfHit<R> *hits,
+                                  const int *keys, int *buckets, int nb, WfRay<R> *sorted_rays,
                                   WfHit<R> *sorted_hits)
 {
     if (!C->sorted) return;
     const int n = C->ray_count[which];
-    int *cursors = buckets + S.material_count + 1;
+    int *cursors = buckets + nb;
     const int stride = gridDim.x * blockDim.x;
     const int n_round = (n + stride - 1) / stride * stride;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
@@ -581,7 +651,10 @@ __global__ void k_wf_sort_scatter(const DevScene<R> S, const WfCounters *C, int 
 // occ_cache (may be NULL): per pixel and NEE slot, the primitive that last blocked
 // that pixel's bounce-0 connection (see scene_any_cached); used at b == 0,
 // where the samples of a pixel shade nearly the same point.
-template <typename R, bool ADJ, int W>
+//
+// PASS: some material of the scene lets shadow rays through (has_passthrough),
+// so connections take the chained walk; otherwise one any-hit query each.
+template <typename R, bool ADJ, int W, bool PASS>
 __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
                                                    R *nee, R *att, int *occ_cache, int wh, int b)
 {
@@ -595,7 +668,7 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, 
         ab.mat[0] = ab.mat[1] = -1;
         ab.dist[0] = ab.dist[1] = R(0);
         bool occ;
-        if (S.has_passthrough) {
+        if constexpr (PASS) {
             occ = ADJ ? pt_occluded_segment_abs(S, o, d, R(1e-3), s.tmax, &atten, &ab)
                       : pt_occluded_segment(S, o, d, R(1e-3), s.tmax, &atten);
         } else {

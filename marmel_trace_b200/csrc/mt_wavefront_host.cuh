@@ -167,10 +167,12 @@ template <typename R, bool ADJ, int W>
 void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
                    const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b)
 {
-    if (dyn && !S.has_passthrough)
+    if (S.has_passthrough)
+        k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b);
+    else if (dyn)
         k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
     else
-        k_wf_shadow<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b);
+        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b);
 }
 
 template <typename R, bool ADJ>
@@ -282,14 +284,14 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             WF_CK(cudaMemsetAsync(&C->shadow_count, 0, 3 * sizeof(int), s), "memset(shadow_count)");
             const bool sort = sort_threshold > 0 && !replay && st->sorted_rays;
             if (sort) {
-                const int nb = S.material_count + 1;
+                const int nb = sort_buckets(S.material_count + 1);
                 WF_CK(cudaMemsetAsync(st->sort_buckets, 0, 2 * (size_t)nb * sizeof(int), s), "memset(buckets)");
                 tic();
-                k_wf_sort_count<R><<<g, block, 0, s>>>(S, C, which, hits, (int *)st->sort_keys,
+                k_wf_sort_count<R><<<g, block, 0, s>>>(S, C, which, rays[which], hits, (int *)st->sort_keys,
                                                        (int *)st->sort_buckets, sort_threshold);
-                k_wf_sort_scan<R><<<1, 32, 0, s>>>(S, C, (int *)st->sort_buckets);
-                k_wf_sort_scatter<R><<<g, block, 0, s>>>(S, C, which, rays[which], hits, (const int *)st->sort_keys,
-                                                         (int *)st->sort_buckets, (WfRay<R> *)st->sorted_rays,
+                k_wf_sort_scan<R><<<1, kSortScanThreads, 0, s>>>(C, (int *)st->sort_buckets, nb);
+                k_wf_sort_scatter<R><<<g, block, 0, s>>>(C, which, rays[which], hits, (const int *)st->sort_keys,
+                                                         (int *)st->sort_buckets, nb, (WfRay<R> *)st->sorted_rays,
                                                          (WfHit<R> *)st->sorted_hits);
                 toc(3);
             }
@@ -349,7 +351,7 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     if (adjoint && (rc = wf_reserve_adj<R>(st))) return rc;
     const int block = (opts && opts->block_size == 64) ? 64 : 128;
     const int sort_threshold = (!adjoint && opts && opts->sort_threshold > 0) ? opts->sort_threshold : 0;
-    if (sort_threshold && (rc = wf_reserve_sort<R>(st, S.material_count + 1))) return rc;
+    if (sort_threshold && (rc = wf_reserve_sort<R>(st, sort_buckets(S.material_count + 1)))) return rc;
     if (!st->grid || st->grid_block != block) {
         st->grid_block = block;
         int dev = 0, sms = 0, per_sm = 0;
