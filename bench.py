@@ -378,7 +378,8 @@ def run_ours(args):
                                        "write per sample x samples per launch",
                      "second_kernel": secondary},
         "e2e": {"value": round(e2e_val, 3) if e2e_val else None, "unit": "Msamples/s", "h2d_bytes_per_step": 128,
-                "d2h_bytes_per_step": W * H * 3, "entry_point": "mt_pathtrace_render"},
+                "d2h_bytes_per_step": W * H * 3, "entry_point": "mt_pathtrace_render",
+                "calls_ms": [round(x, 1) for x in e2e_ms]},
         "gpu_launches": launches * args.steps,
         "wall_s_timed_loop": round(t_wall, 3),
     }

@@ -194,7 +194,8 @@ typedef struct {
     int32_t block_size;      /* threads per block, 0 = library default          */
     int32_t queue_capacity;  /* wavefront paths in flight, 0 = library default  */
     int32_t bvh_width;       /* 2, 4 or 8; 0 = library default                  */
-    int32_t sort_threshold;  /* wavefront: sort by material above this many paths (0 = never) */
+    int32_t sort_threshold;  /* wavefront: sort a bounce's hits by material and place when
+                                it holds at least this many paths (0 = never; default 1 << 18) */
     int32_t use_graph;       /* wavefront: 1 = capture the sample window in a CUDA graph,
                                 0 = plain launches, -1 = plain launches timed per stage */
     int32_t device;          /* CUDA device ordinal                             */

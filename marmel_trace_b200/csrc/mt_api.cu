@@ -587,7 +587,7 @@ void mt_options_default(mt_options *o)
     o->block_size = 128;
     o->queue_capacity = 0;
     o->bvh_width = 2;
-    o->sort_threshold = 0;
+    o->sort_threshold = 1 << 18;
     o->use_graph = 1;
     o->device = 0;
     o->traversal = MT_TRAVERSAL_DEFAULT;
@@ -1002,7 +1002,7 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
     cur.traversal = MT_TRAVERSAL_STATIC;
     cur.block_size = 128;
     cur.bvh_width = 2;
-    cur.sort_threshold = 0;
+    cur.sort_threshold = 1 << 18;
     cur.queue_capacity = 0;
     cur.use_graph = 1;
     float cur_ms = 0.f;
@@ -1016,7 +1016,7 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
         case 0: vals[nv++] = MT_TRAVERSAL_DYNAMIC; break;
         case 1: vals[nv++] = 64; break;
         case 2: vals[nv++] = 4; vals[nv++] = 8; break;
-        case 3: vals[nv++] = 1 << 18; vals[nv++] = 1; break;
+        case 3: vals[nv++] = 0; vals[nv++] = 1; break;
         default: vals[nv++] = 4 << 20; vals[nv++] = 2 << 20; vals[nv++] = 1 << 20; break;
         }
         for (int i = 0; i < nv && !rc; ++i) {

@@ -883,11 +883,13 @@ template <typename R, int W = 2> MT_D bool scene_any(const DevScene<R> &S, const
 // Any hit that first tries the primitive in *cache (kind << 28 | slot, -1
 // none) -- a hit there is a hit of the query, so the answer is the same --
 // and otherwise walks the tree and leaves the blocking primitive in *cache.
+// test_cached = false: the caller has already tested *cache and it missed.
 template <typename R, int W = 2>
-MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, int *cache)
+MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, int *cache,
+                           bool test_cached = true)
 {
     const int c = *cache;
-    if (c >= 0 && prim_occluded(S, c, rp, tmin, tmax)) {
+    if (test_cached && c >= 0 && prim_occluded(S, c, rp, tmin, tmax)) {
         if (S.counters) count_add(&S.counters->any_prim_tests, 1ull);
         return true;
     }

@@ -109,7 +109,8 @@ struct WfCounters {
     int shadow_fetch;  // next shadow ray handed out by the dynamic-fetch kernel
     int ray_fetch;     // next ray handed out by the dynamic-fetch extend kernel
     int sorted;        // this bounce's extend results were sorted by material
-    int pad[2];
+    int walk_count;    // bounce-0 shadow rays whose cached occluder missed (k_wf_shadow_cache)
+    int pad;
 };
 
 // Warp-aggregated queue append: one atomicAdd per warp, lanes get
@@ -648,19 +649,54 @@ __global__ void k_wf_sort_scatter(const WfCounters *C, int which, const WfRay<R>
 // ADJ: also keep the connection's transmittance (zero when it adds no light)
 // for the replay's gradient terms.
 //
-// occ_cache (may be NULL): per pixel and NEE slot, the primitive that last blocked
-// that pixel's bounce-0 connection (see scene_any_cached); used at b == 0,
-// where the samples of a pixel shade nearly the same point.
-//
 // PASS: some material of the scene lets shadow rays through (has_passthrough),
 // so connections take the chained walk; otherwise one any-hit query each.
+//
+// Bounce 0 of a scene without pass-through materials runs in two passes over
+// the occluder cache (per pixel and NEE slot, the primitive that last blocked
+// that pixel's bounce-0 connection; see scene_any_cached), because the samples
+// of a pixel shade nearly the same point: k_wf_shadow_cache tests every
+// connection's cached primitive, resolves the blocked ones and appends the
+// others to `walk`; k_wf_shadow then walks the tree for `walk` only, so cache
+// hits (one primitive test) and walks (the whole tree) do not share warps.
+
+// Result of one connection: its NEE slot (and, ADJ, its transmittance record).
+template <typename R, bool ADJ>
+MT_D void shadow_result(const WfShadow<R> &s, bool occ, V3<R> atten, const AbsorbPath<R> &ab, R *nee, R *att)
+{
+    V3<R> res = v3(R(0), R(0), R(0));
+    bool lit = false;
+    if (!occ) {
+        bool dark = s.li == kMaxLights && atten.x < R(1e-4) && atten.y < R(1e-4) && atten.z < R(1e-4);
+        if (!dark) {
+            res = mul(v3(s.contrib[0], s.contrib[1], s.contrib[2]), atten);
+            lit = true;
+        }
+    }
+    const size_t at = ((size_t)s.slot * kNeeSlots + s.li) * 3;
+    R *slot = nee + at;
+    slot[0] = res.x;
+    slot[1] = res.y;
+    slot[2] = res.z;
+    if constexpr (ADJ) {
+        R *rec = att + ((size_t)s.slot * kNeeSlots + s.li) * kAttStride;
+        if (lit) {
+            set_att(rec, atten, ab);
+        } else {
+            for (int k = 0; k < kAttStride; ++k) rec[k] = R(0);
+        }
+    }
+}
+
+// `walk` (may be NULL): the connections to process are sq[walk[0 .. C->walk_count)]
+// and their cached occluder has already missed; otherwise sq[0 .. C->shadow_count).
 template <typename R, bool ADJ, int W, bool PASS>
 __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
-                                                   R *nee, R *att, int *occ_cache, int wh, int b)
+                                                   R *nee, R *att, int *occ_cache, int wh, int b, const int *walk)
 {
-    const int n = C->shadow_count;
+    const int n = walk ? C->walk_count : C->shadow_count;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const WfShadow<R> s = sq[q];
+        const WfShadow<R> s = sq[walk ? walk[q] : q];
         V3<R> o = v3(s.o[0], s.o[1], s.o[2]);
         V3<R> d = v3(s.d[0], s.d[1], s.d[2]);
         V3<R> atten;
@@ -675,35 +711,48 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, 
             // No material lets a shadow ray through: the chained nearest-hit
             // walk stops at its first hit, so it equals an any-hit query.
             atten = v3(R(1), R(1), R(1));
-            if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
+            if (S.counters && !walk) atomicAdd(&S.counters->shadow_rays, 1ull);
             if (occ_cache && b == 0)
                 occ = scene_any_cached<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax,
-                                             occ_cache + (size_t)(s.slot % wh) * kNeeSlots + s.li);
+                                             occ_cache + (size_t)(s.slot % wh) * kNeeSlots + s.li, !walk);
             else
                 occ = scene_any<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
         }
-        V3<R> res = v3(R(0), R(0), R(0));
-        bool lit = false;
-        if (!occ) {
-            bool dark = s.li == kMaxLights && atten.x < R(1e-4) && atten.y < R(1e-4) && atten.z < R(1e-4);
-            if (!dark) {
-                res = mul(v3(s.contrib[0], s.contrib[1], s.contrib[2]), atten);
-                lit = true;
-            }
-        }
-        const size_t at = ((size_t)s.slot * kNeeSlots + s.li) * 3;
-        R *slot = nee + at;
-        slot[0] = res.x;
-        slot[1] = res.y;
-        slot[2] = res.z;
-        if constexpr (ADJ) {
-            R *rec = att + ((size_t)s.slot * kNeeSlots + s.li) * kAttStride;
-            if (lit) {
-                set_att(rec, atten, ab);
+        shadow_result<R, ADJ>(s, occ, atten, ab, nee, att);
+    }
+}
+
+// First pass of bounce 0 (scenes without pass-through materials): the cached
+// occluder of every connection; misses go to `walk` (warp-aggregated appends).
+template <typename R, bool ADJ>
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const DevScene<R> S, const WfShadow<R> *sq,
+                                                         WfCounters *C, R *nee, R *att, const int *occ_cache, int wh,
+                                                         int *walk)
+{
+    const int n = C->shadow_count;
+    const int stride = gridDim.x * blockDim.x;
+    const int n_round = (n + stride - 1) / stride * stride;
+    AbsorbPath<R> ab;
+    ab.mat[0] = ab.mat[1] = -1;
+    ab.dist[0] = ab.dist[1] = R(0);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
+        bool miss = false;
+        if (q < n) {
+            const WfShadow<R> s = sq[q];
+            if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
+            const int c = occ_cache[(size_t)(s.slot % wh) * kNeeSlots + s.li];
+            const bool blocked =
+                c >= 0 && prim_occluded(S, c, ray_pre(v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2]))),
+                                        R(1e-3), s.tmax);
+            if (blocked) {
+                if (S.counters) atomicAdd(&S.counters->any_prim_tests, 1ull);
+                shadow_result<R, ADJ>(s, true, v3(R(1), R(1), R(1)), ab, nee, att);
             } else {
-                for (int k = 0; k < kAttStride; ++k) rec[k] = R(0);
+                miss = true;
             }
         }
+        const int at = warp_append(&C->walk_count, miss);
+        if (miss) walk[at] = q;
     }
 }
 

@@ -46,6 +46,7 @@ struct WavefrontState {
     // scene (a batch lane renders several, so it turns this off)
     void *occ_cache = nullptr;
     bool occ_cache_on = true;
+    void *walk = nullptr;      // bounce-0 shadow rays left to walk after the cache pass
     int grid = 0;              // persistent grid (blocks) of the stage kernels
     cudaEvent_t kev[64];       // per-kernel timing events (profiling mode)
     bool kev_init = false;
@@ -78,7 +79,7 @@ inline void wf_free(WavefrontState *st)
     void **bufs[] = {&st->paths,       &st->rays[0],    &st->rays[1],     &st->hits,        &st->nee,
                      &st->shadow,      &st->sample_buf, &st->acc,         &st->params,      &st->adj_verts,
                      &st->adj_att,     &st->sorted_rays, &st->sorted_hits, &st->sort_keys, &st->sort_buckets,
-                     &st->occ_cache};
+                     &st->occ_cache,   &st->walk};
     for (void **b : bufs) {
         if (*b) cudaFree(*b);
         *b = nullptr;
@@ -136,6 +137,7 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
     WF_CK(cudaMalloc((void **)&st->counters, sizeof(WfCounters)), "cudaMalloc(counters)");
     WF_CK(cudaMalloc(&st->occ_cache, wh * kNeeSlots * sizeof(int)), "cudaMalloc(occluder cache)");
     WF_CK(cudaMemset(st->occ_cache, 0xFF, wh * kNeeSlots * sizeof(int)), "cudaMemset(occluder cache)");
+    WF_CK(cudaMalloc(&st->walk, (nshadow ? nshadow : 1) * sizeof(int)), "cudaMalloc(shadow walk list)");
     if (!st->h_params) WF_CK(cudaMallocHost(&st->h_params, 256), "cudaMallocHost(params)");
     st->cap_paths = n_paths;
     st->acc_pixels = wh;
@@ -165,25 +167,30 @@ void launch_extend(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
 
 template <typename R, bool ADJ, int W>
 void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
-                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b)
+                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk)
 {
-    if (S.has_passthrough)
-        k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b);
-    else if (dyn)
+    if (S.has_passthrough) {
+        k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
+    } else if (dyn) {
         k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
-    else
-        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b);
+    } else if (occ && b == 0 && walk) {
+        // cached occluders first, then the tree walk for the misses
+        k_wf_shadow_cache<R, ADJ><<<g, block, 0, s>>>(S, sq, C, nee, att, occ, wh, walk);
+        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
+    } else {
+        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
+    }
 }
 
 template <typename R, bool ADJ>
 void launch_shadow_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
-                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b)
+                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk)
 {
     if constexpr (sizeof(R) == 4) {
-        if (W == 4) return launch_shadow<R, ADJ, 4>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b);
-        if (W == 8) return launch_shadow<R, ADJ, 8>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b);
+        if (W == 4) return launch_shadow<R, ADJ, 4>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
+        if (W == 8) return launch_shadow<R, ADJ, 8>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
     }
-    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b);
+    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
 }
 
 template <typename R>
@@ -280,8 +287,9 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             launch_extend_w<R>(W, dyn, g, block, smem_w, s, S, rays[which], C, which, hits);
             toc(0);
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
-            // shadow_count, shadow_fetch and ray_fetch (the next extend's)
-            WF_CK(cudaMemsetAsync(&C->shadow_count, 0, 3 * sizeof(int), s), "memset(shadow_count)");
+            // shadow_count, shadow_fetch, ray_fetch (the next extend's), sorted
+            // and walk_count
+            WF_CK(cudaMemsetAsync(&C->shadow_count, 0, 5 * sizeof(int), s), "memset(shadow_count)");
             const bool sort = sort_threshold > 0 && !replay && st->sorted_rays;
             if (sort) {
                 const int nb = sort_buckets(S.material_count + 1);
@@ -308,9 +316,11 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             toc(1);
             tic();
             if (replay)
-                launch_shadow_w<R, true>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, A.att, occ, wh, b);
+                launch_shadow_w<R, true>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, A.att, occ, wh, b,
+                                         (int *)st->walk);
             else
-                launch_shadow_w<R, false>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, nullptr, occ, wh, b);
+                launch_shadow_w<R, false>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, nullptr, occ, wh, b,
+                                          (int *)st->walk);
             toc(2);
             which ^= 1;
         }
@@ -390,8 +400,11 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     cudaStreamSynchronize(stream);  // the pinned block may still be in use by a previous copy
     memcpy(st->h_params, &hp, sizeof hp);
     WF_CK(cudaMemcpyAsync(st->params, st->h_params, sizeof hp, cudaMemcpyHostToDevice, stream), "params copy");
-    int kernels_per_window = adjoint ? n_batches * 2 * (3 * (depth + 1) + 2)
-                                     : n_batches * ((3 + (sort_threshold ? 3 : 0)) * (depth + 1) + 3);
+    // the bounce-0 shadow stage is two kernels when it uses the occluder cache
+    const int cache_pass = st->occ_cache_on && st->occ_cache && st->walk && !S.has_passthrough &&
+                           !(opts && opts->traversal == MT_TRAVERSAL_DYNAMIC);
+    int kernels_per_window = adjoint ? n_batches * 2 * (3 * (depth + 1) + 2 + cache_pass)
+                                     : n_batches * ((3 + (sort_threshold ? 3 : 0)) * (depth + 1) + 3 + cache_pass);
     cudaGraphExec_t &exec = adjoint ? st->adj_exec : st->exec;
     // dynamic fetch reorders rays across lanes: on coherent queues (primary
     // rays, NEE rays grouped by light) the grid-stride kernels are faster, so
