@@ -109,7 +109,7 @@ struct WfCounters {
     int shadow_fetch;  // next shadow ray handed out by the dynamic-fetch kernel
     int ray_fetch;     // next ray handed out by the dynamic-fetch extend kernel
     int sorted;        // this bounce's extend results were sorted by material
-    int walk_count;    // bounce-0 shadow rays whose cached occluder missed (k_wf_shadow_cache)
+    int walk_count;    // shadow rays whose cached occluder missed (k_wf_shadow_cache)
     int pad;
 };
 
@@ -652,13 +652,48 @@ __global__ void k_wf_sort_scatter(const WfCounters *C, int which, const WfRay<R>
 // PASS: some material of the scene lets shadow rays through (has_passthrough),
 // so connections take the chained walk; otherwise one any-hit query each.
 //
-// Bounce 0 of a scene without pass-through materials runs in two passes over
-// the occluder cache (per pixel and NEE slot, the primitive that last blocked
-// that pixel's bounce-0 connection; see scene_any_cached), because the samples
-// of a pixel shade nearly the same point: k_wf_shadow_cache tests every
-// connection's cached primitive, resolves the blocked ones and appends the
-// others to `walk`; k_wf_shadow then walks the tree for `walk` only, so cache
-// hits (one primitive test) and walks (the whole tree) do not share warps.
+// In a scene without pass-through materials the stage runs in two passes
+// over the occluder cache, which holds for each connection's entry (see
+// occ_entry) the primitive that last blocked a connection there:
+// k_wf_shadow_cache tests every connection's cached primitive (a hit there is
+// a hit of the any-hit query, so the answer cannot change), resolves the
+// blocked ones and appends the others to `walk`; k_wf_shadow then walks the
+// tree for `walk` only and stores each blocker it finds (scene_any_cached).
+// Cache hits (one primitive test) and walks (the whole tree) therefore do not
+// share warps.
+
+// Occluder cache entry of a connection. At bounce 0, per pixel and NEE slot:
+// the samples of a pixel shade nearly the same point. Later, a hash of (cell
+// of the origin, NEE slot) into kOccHash entries after the per-pixel part,
+// with 2^kOccCellBits cells per axis of the root box: nearby origins toward
+// one light tend to share a blocker. A collision only costs a primitive test,
+// since an entry is just a candidate. (On the 1M-triangle torus field 256
+// cells per axis did best: 64 and 4096 were both slower.)
+static constexpr int kOccHashBits = 22;
+static constexpr int kOccHash = 1 << kOccHashBits;
+static constexpr int kOccCellBits = 8;
+template <typename R> MT_D int *occ_entry(const DevScene<R> &S, int *occ_cache, int wh, int b, const WfShadow<R> &s)
+{
+    if (b == 0) return occ_cache + (size_t)(s.slot % wh) * kNeeSlots + s.li;
+    unsigned c[3] = {0u, 0u, 0u};
+    if (S.node_count > 0) {
+        const float4 q0 = __ldg(S.nodes), q1 = __ldg(S.nodes + 1), q2 = __ldg(S.nodes + 2);
+        const float lo[3] = {fminf(q0.x, q1.x), fminf(q0.z, q1.z), fminf(q2.x, q2.z)};
+        const float hi[3] = {fmaxf(q0.y, q1.y), fmaxf(q0.w, q1.w), fmaxf(q2.y, q2.w)};
+        const int top = (1 << kOccCellBits) - 1;
+        for (int k = 0; k < 3; ++k) {
+            const float ext = hi[k] - lo[k];
+            const float f = ext > 0.f ? ((float)s.o[k] - lo[k]) * ((float)(1 << kOccCellBits) / ext) : 0.f;
+            int v = f > 0.f ? (int)f : 0;
+            c[k] = (unsigned)(v > top ? top : v);
+        }
+    }
+    unsigned h = c[0] * 73856093u ^ c[1] * 19349663u ^ c[2] * 83492791u ^ (unsigned)s.li * 2654435761u;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    return occ_cache + (size_t)wh * kNeeSlots + (h & (kOccHash - 1));
+}
 
 // Result of one connection: its NEE slot (and, ADJ, its transmittance record).
 template <typename R, bool ADJ>
@@ -712,9 +747,9 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, 
             // walk stops at its first hit, so it equals an any-hit query.
             atten = v3(R(1), R(1), R(1));
             if (S.counters && !walk) atomicAdd(&S.counters->shadow_rays, 1ull);
-            if (occ_cache && b == 0)
+            if (occ_cache)
                 occ = scene_any_cached<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax,
-                                             occ_cache + (size_t)(s.slot % wh) * kNeeSlots + s.li, !walk);
+                                             occ_entry(S, occ_cache, wh, b, s), !walk);
             else
                 occ = scene_any<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
         }
@@ -726,8 +761,8 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, 
 // occluder of every connection; misses go to `walk` (warp-aggregated appends).
 template <typename R, bool ADJ>
 __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const DevScene<R> S, const WfShadow<R> *sq,
-                                                         WfCounters *C, R *nee, R *att, const int *occ_cache, int wh,
-                                                         int *walk)
+                                                         WfCounters *C, R *nee, R *att, int *occ_cache, int wh,
+                                                         int b, int *walk)
 {
     const int n = C->shadow_count;
     const int stride = gridDim.x * blockDim.x;
@@ -740,7 +775,7 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const DevScene<
         if (q < n) {
             const WfShadow<R> s = sq[q];
             if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
-            const int c = occ_cache[(size_t)(s.slot % wh) * kNeeSlots + s.li];
+            const int c = *occ_entry(S, occ_cache, wh, b, s);
             const bool blocked =
                 c >= 0 && prim_occluded(S, c, ray_pre(v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2]))),
                                         R(1e-3), s.tmax);

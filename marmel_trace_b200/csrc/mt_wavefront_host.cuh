@@ -41,12 +41,12 @@ struct WavefrontState {
     void *sorted_rays = nullptr, *sorted_hits = nullptr, *sort_keys = nullptr, *sort_buckets = nullptr;
     int sort_bucket_cap = 0;
     int grid_block = 0;        // block size the persistent grid was sized for
-    // per pixel and NEE slot, the primitive that last blocked the pixel's
-    // bounce-0 shadow ray (k_wf_shadow); only for a state that serves one
-    // scene (a batch lane renders several, so it turns this off)
+    // occluder cache (occ_entry): per pixel and NEE slot for bounce 0, then a
+    // hash of (origin cell, NEE slot); only for a state that serves one scene
+    // (a batch lane renders several, so it turns this off)
     void *occ_cache = nullptr;
     bool occ_cache_on = true;
-    void *walk = nullptr;      // bounce-0 shadow rays left to walk after the cache pass
+    void *walk = nullptr;      // shadow rays left to walk after the occluder-cache pass
     int grid = 0;              // persistent grid (blocks) of the stage kernels
     cudaEvent_t kev[64];       // per-kernel timing events (profiling mode)
     bool kev_init = false;
@@ -135,8 +135,8 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
     WF_CK(cudaMalloc(&st->acc, wh * 3 * sizeof(R)), "cudaMalloc(acc)");
     WF_CK(cudaMalloc(&st->params, sizeof(WfParams<R>)), "cudaMalloc(params)");
     WF_CK(cudaMalloc((void **)&st->counters, sizeof(WfCounters)), "cudaMalloc(counters)");
-    WF_CK(cudaMalloc(&st->occ_cache, wh * kNeeSlots * sizeof(int)), "cudaMalloc(occluder cache)");
-    WF_CK(cudaMemset(st->occ_cache, 0xFF, wh * kNeeSlots * sizeof(int)), "cudaMemset(occluder cache)");
+    WF_CK(cudaMalloc(&st->occ_cache, (wh * kNeeSlots + kOccHash) * sizeof(int)), "cudaMalloc(occluder cache)");
+    WF_CK(cudaMemset(st->occ_cache, 0xFF, (wh * kNeeSlots + kOccHash) * sizeof(int)), "cudaMemset(occluder cache)");
     WF_CK(cudaMalloc(&st->walk, (nshadow ? nshadow : 1) * sizeof(int)), "cudaMalloc(shadow walk list)");
     if (!st->h_params) WF_CK(cudaMallocHost(&st->h_params, 256), "cudaMallocHost(params)");
     st->cap_paths = n_paths;
@@ -173,9 +173,9 @@ void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
         k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
     } else if (dyn) {
         k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
-    } else if (occ && b == 0 && walk) {
+    } else if (occ && walk) {
         // cached occluders first, then the tree walk for the misses
-        k_wf_shadow_cache<R, ADJ><<<g, block, 0, s>>>(S, sq, C, nee, att, occ, wh, walk);
+        k_wf_shadow_cache<R, ADJ><<<g, block, 0, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
         k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
     } else {
         k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
@@ -403,8 +403,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     // the bounce-0 shadow stage is two kernels when it uses the occluder cache
     const int cache_pass = st->occ_cache_on && st->occ_cache && st->walk && !S.has_passthrough &&
                            !(opts && opts->traversal == MT_TRAVERSAL_DYNAMIC);
-    int kernels_per_window = adjoint ? n_batches * 2 * (3 * (depth + 1) + 2 + cache_pass)
-                                     : n_batches * ((3 + (sort_threshold ? 3 : 0)) * (depth + 1) + 3 + cache_pass);
+    int kernels_per_window = adjoint ? n_batches * 2 * ((3 + cache_pass) * (depth + 1) + 2)
+                                     : n_batches * ((3 + cache_pass + (sort_threshold ? 3 : 0)) * (depth + 1) + 3);
     cudaGraphExec_t &exec = adjoint ? st->adj_exec : st->exec;
     // dynamic fetch reorders rays across lanes: on coherent queues (primary
     // rays, NEE rays grouped by light) the grid-stride kernels are faster, so
