@@ -86,10 +86,10 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, tag: str = ""):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}{tag}.csv"
 
     def __enter__(self):
         try:
@@ -254,12 +254,15 @@ def run_ours(args):
 
     # e2e through the drop-in entry point (host camera in, host RGB8 out)
     rgb = np.zeros((H, W, 3), np.uint8)
-    e2e_ms = []
-    for _ in range(0 if args.no_e2e else max(1, min(args.steps, 3))):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        _capi.check(g.lib.mt_pathtrace_render(g.h, cam.ref, W, H, SPP, DEPTH, rgb.ctypes.data), "mt_pathtrace_render")
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms, e2e_dev_ms = [], []
+    with ClockSampler(local, "_e2e") as clk_e2e:
+        for _ in range(0 if args.no_e2e else max(1, min(args.steps, 3))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _capi.check(g.lib.mt_pathtrace_render(g.h, cam.ref, W, H, SPP, DEPTH, rgb.ctypes.data),
+                        "mt_pathtrace_render")
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            e2e_dev_ms.append(g.stats().kernel_ms)  # the render's own CUDA events
     e2e_val = whole_job_rate(W * H * SPP, world, max_over_ranks(statistics.median(e2e_ms) / 1e3, dist, "cuda")) \
         if e2e_ms else None
 
@@ -379,7 +382,8 @@ def run_ours(args):
                      "second_kernel": secondary},
         "e2e": {"value": round(e2e_val, 3) if e2e_val else None, "unit": "Msamples/s", "h2d_bytes_per_step": 128,
                 "d2h_bytes_per_step": W * H * 3, "entry_point": "mt_pathtrace_render",
-                "calls_ms": [round(x, 1) for x in e2e_ms]},
+                "calls_ms": [round(x, 1) for x in e2e_ms], "calls_device_ms": [round(x, 1) for x in e2e_dev_ms],
+                "clocks": clk_e2e.summary() if rank == 0 else None},
         "gpu_launches": launches * args.steps,
         "wall_s_timed_loop": round(t_wall, 3),
     }

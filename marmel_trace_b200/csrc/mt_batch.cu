@@ -46,6 +46,10 @@ struct mt_batch {
 
 namespace {
 
+// Lanes sort a bounce's hits by material and place above this many paths,
+// the library's default sort threshold.
+constexpr int kBatchSortThreshold = 1 << 18;
+
 int bfail(int code, const std::string &msg)
 {
     mt_set_last_error_text(msg.c_str());
@@ -190,6 +194,10 @@ int mt_batch_render(mt_batch *b, int32_t n, const mt_batch_item *items, void *st
         }
         if (!paths) continue;
         int rc = wf_reserve<float>(b->st[l], paths, pixels, kMaxLights);
+        int buckets = 1;
+        for (int i : lane_items[l])
+            buckets = std::max(buckets, sort_buckets(mt_scene_dev_f32(items[i].scene)->material_count + 1));
+        if (!rc) rc = wf_reserve_sort<float>(b->st[l], buckets);
         if (rc) return bfail(rc, std::string("mt_batch_render: ") + wavefront_last_error());
     }
     if (!b->grid) {
@@ -202,7 +210,7 @@ int mt_batch_render(mt_batch *b, int32_t n, const mt_batch_item *items, void *st
     }
     for (int l = 0; l < b->lanes; ++l) {
         b->st[l]->grid = b->grid;
-        b->st[l]->occ_cache_on = false;  // a lane renders several scenes
+        b->st[l]->occ_cache_on = true;  // reset before each item: a lane renders several scenes
     }
     // ---- parameter blocks ----
     if (n > b->params_cap) {
@@ -245,8 +253,12 @@ int mt_batch_render(mt_batch *b, int32_t n, const mt_batch_item *items, void *st
                 DevScene<float> S = *mt_scene_dev_f32(items[i].scene);
                 S.counters = nullptr;
                 const WfParams<float> *P = (const WfParams<float> *)b->params + i;
+                // the occluder cache holds primitive codes of one scene
+                ce = cudaMemsetAsync(b->st[l]->occ_cache, 0xFF,
+                                     (b->st[l]->acc_pixels * kNeeSlots + kOccHash) * sizeof(int), b->streams[l]);
+                if (ce != cudaSuccess) break;
                 erc = wf_enqueue<float>(b->st[l], S, items[i].width, items[i].height, bspp[i], nbat[i],
-                                        items[i].depth, b->streams[l], false, 128, false, false, P);
+                                        items[i].depth, b->streams[l], false, 128, false, false, P, kBatchSortThreshold);
                 if (!erc) ce = cudaEventRecordWithFlags(b->ev_item[i], b->streams[l], cudaEventRecordExternal);
             }
             if (ce == cudaSuccess && !erc) ce = cudaEventRecord(b->ev_join[l], b->streams[l]);

@@ -726,7 +726,9 @@ MT_D void shadow_result(const WfShadow<R> &s, bool occ, V3<R> atten, const Absor
 // `walk` (may be NULL): the connections to process are sq[walk[0 .. C->walk_count)]
 // and their cached occluder has already missed; otherwise sq[0 .. C->shadow_count).
 template <typename R, bool ADJ, int W, bool PASS>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
+// (binary tree: at most 72 registers, so 7 blocks of 128 fit an SM; the
+// pass-through instantiation would otherwise take 80 and run 6)
+__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? 7 : 1) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
                                                    R *nee, R *att, int *occ_cache, int wh, int b, const int *walk)
 {
     const int n = walk ? C->walk_count : C->shadow_count;
