@@ -149,9 +149,10 @@ def build_scene():
 
 # DRAM bytes (read + write) per path sample of the stage kernels, from an ncu
 # launch list of this workload (4-spp frames, 2M-slot queue; summarised under
-# profiles/): 26.54 GB (shadow) and 6.09 GB (extend) over 7 frames of
-# 4 x 2,073,600 samples.
-TRAFFIC_BYTES_PER_SAMPLE = {"shadow": 26.54e9 / (7 * 4 * 2073600), "extend": 6.09e9 / (7 * 4 * 2073600)}
+# profiles/): the shadow stage (cache pass 20.40 + 3.40 GB, walk 19.77 + 4.64
+# GB) and the extend kernel (5.74 + 0.43 GB) over 7 frames of 4 x 2,073,600
+# samples.
+TRAFFIC_BYTES_PER_SAMPLE = {"shadow": 48.21e9 / (7 * 4 * 2073600), "extend": 6.17e9 / (7 * 4 * 2073600)}
 
 
 def traversal_bytes(st, kind: str, width: int = 2) -> float:
@@ -329,7 +330,8 @@ def run_ours(args):
         # dominant stage kernel: the shadow (any-hit) stage on this workload
         dom = "shadow" if stage["shadow_ms"] >= stage["extend_ms"] else "extend"
         other = "extend" if dom == "shadow" else "shadow"
-        kinds = {"shadow": ("any", "k_wf_shadow<float> (any-hit traversal per NEE connection)"),
+        kinds = {"shadow": ("any", "shadow stage: k_wf_shadow_cache<float> (cached occluders) + k_wf_shadow<float> "
+                                   "(any-hit walk of the rest), per NEE connection"),
                  "extend": ("nearest", "k_wf_extend<float> (nearest-hit traversal)")}
         alg = traversal_bytes(cnt, kinds[dom][0], bw) * (W * H * SPP) / n_counted
         achieved = alg / (stage[f"{dom}_ms"] / 1e3) / 1e9
