@@ -363,7 +363,7 @@ def run_ours(args):
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": SPP, "depth": DEPTH,
                    "integrator": args.integrator, "parallelism": f"replicas x{world}",
-                   "queue_capacity": qopt.get("queue_capacity") or 8 << 20,
+                   "queue_capacity": qopt.get("queue_capacity") or 1 << 25,
                    "tuned": tune["chosen"] if tune else None,
                    "l2": "flushed between timed steps (256 MB write); the 90 MB scene fits in L2"},
         "plain_gpu_msamples_s": round(plain, 3) if plain else None,
@@ -614,7 +614,7 @@ def main():
     ap.add_argument("--large", action="store_true",
                     help="also run the 10M-triangle water / tree scene at 3840x2160 (tens of seconds)")
     ap.add_argument("--queue-capacity", type=int, default=0,
-                    help="path slots per wavefront batch (0: the library default, 8M)")
+                    help="path slots per wavefront batch (0: the library default, 32M)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -369,7 +369,7 @@ typedef struct {
  * keeping the fastest so far (library defaults first):
  *   traversal schedule (grid-stride, dynamic fetch), block size (128, 64),
  *   BVH width (2, 4, 8; wide trees built on first use), sort-by-material
- *   threshold (off, 256K rays, always), queue capacity (8M, 4M, 2M, 1M).
+ *   threshold (256K rays, off, always), queue capacity (32M, 8M, 2M).
  * Every candidate computes the same image (the tests check this), so the
  * choice only moves time. The scene must be FP32; on return its options are
  * the chosen ones with the wavefront integrator. Allocates probe buffers;

@@ -1008,6 +1008,14 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
     float cur_ms = 0.f;
     rc = probe(cur, &cur_ms);
     rep->default_ms = cur_ms;
+    // samples per batch of the probe window for a queue capacity (the largest
+    // divisor of probe_spp whose paths fit; 0 = the library default of 2^25)
+    auto probe_batch = [&](long long capacity) {
+        const long long cap = std::max<long long>(capacity > 0 ? capacity : (1ll << 25), (long long)w * h);
+        for (int d = probe_spp; d >= 1; --d)
+            if (probe_spp % d == 0 && (long long)w * h * d <= cap) return d;
+        return 1;
+    };
     // coordinate descent over the knobs, defaults first in each stage
     for (int stage = 0; stage < 5 && !rc; ++stage) {
         int vals[4];
@@ -1017,7 +1025,7 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
         case 1: vals[nv++] = 64; break;
         case 2: vals[nv++] = 4; vals[nv++] = 8; break;
         case 3: vals[nv++] = 0; vals[nv++] = 1; break;
-        default: vals[nv++] = 4 << 20; vals[nv++] = 2 << 20; vals[nv++] = 1 << 20; break;
+        default: vals[nv++] = 8 << 20; vals[nv++] = 2 << 20; break;
         }
         for (int i = 0; i < nv && !rc; ++i) {
             mt_options o = cur;
@@ -1026,7 +1034,9 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
             else if (stage == 2) o.bvh_width = vals[i];
             else if (stage == 3) o.sort_threshold = vals[i];
             else o.queue_capacity = vals[i];
-            if (stage == 4 && (long long)w * h >= o.queue_capacity) continue;  // one sample per batch already
+            // a capacity that splits the probe window into the same batches as
+            // the current one cannot be told apart by the probe: skip it
+            if (stage == 4 && probe_batch(o.queue_capacity) == probe_batch(cur.queue_capacity)) continue;
             float ms = 0.f;
             rc = probe(o, &ms);
             if (!rc && ms < cur_ms) {

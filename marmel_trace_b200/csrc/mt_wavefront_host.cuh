@@ -98,11 +98,17 @@ inline void wf_free(WavefrontState *st)
 }
 
 // Batch size of a window of `spp` samples over `wh` pixels: the largest
-// divisor of spp whose paths fit the queue capacity (default 8M path slots,
+// divisor of spp whose paths fit the queue capacity (default kDefaultQueuePaths,
 // at least one sample of every pixel).
+// Default path slots of a batch: 2^25 (about 25 GB of queues when a window
+// fills them; a window allocates only pixels x batch spp). Larger batches
+// leave fewer deep-bounce tails with a half-empty GPU: on the 1080p torus
+// field a 16-spp frame takes 161 / 156 / 154 ms with 8 M / 16 M / 33 M slots.
+static constexpr long long kDefaultQueuePaths = 1ll << 25;
+
 inline void wf_batch_split(int wh, int spp, long long capacity, int *batch_spp, int *n_batches)
 {
-    long long cap = capacity > 0 ? capacity : (8ll << 20);
+    long long cap = capacity > 0 ? capacity : kDefaultQueuePaths;
     if (cap < wh) cap = wh;
     *batch_spp = 1;
     for (int d = spp; d >= 1; --d)
