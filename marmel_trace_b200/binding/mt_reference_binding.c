@@ -18,6 +18,9 @@
  *     original `__real_*` functions (the reference's multithreaded CPU path);
  *     that switch exists for baseline timing and is never taken implicitly.
  *     `MT_PRECISION=fp64` selects the double-precision device path.
+ *     Path tracing runs on the wavefront integrator (the fast one);
+ *     `MT_INTEGRATOR=megakernel` selects the one-thread-per-pixel kernel.
+ *     Both give the same images.
  *
  * Device scenes are cached by (Scene pointer, primitive count); the cache is
  * released at process exit.
@@ -234,7 +237,7 @@ static int mtb_get_scene(const Scene *s, mt_scene **out)
 {
     static int registered = 0;
     mt_options o;
-    const char *prec;
+    const char *prec, *integ;
     int rc;
 
     if (g_cached_dev && g_cached_scene == s && g_cached_count == s->geo.count) {
@@ -245,6 +248,9 @@ static int mtb_get_scene(const Scene *s, mt_scene **out)
     mt_options_default(&o);
     prec = getenv("MT_PRECISION");
     if (prec != NULL && strcmp(prec, "fp64") == 0) o.precision = MT_PRECISION_FP64;
+    integ = getenv("MT_INTEGRATOR");
+    o.integrator = (integ != NULL && strcmp(integ, "megakernel") == 0) ? MT_INTEGRATOR_MEGAKERNEL
+                                                                      : MT_INTEGRATOR_WAVEFRONT;
     rc = mtb_scene_upload(s, &o, &g_cached_dev);
     if (rc != 0) {
         fprintf(stderr, "mtgpu: scene upload failed (code %d): %s\n", rc, mt_last_error());
