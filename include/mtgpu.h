@@ -21,8 +21,9 @@
  * (src/pathtrace.c:1260-1268, src/render.c:1630-1641):
  *   0 ok, 1 NULL pointer, 2 non-positive dimensions, 3 bad spp / depth,
  * and add codes >= 10 for device-side failures. Unsupported scene content
- * (CSG, SDF, fog, textures, bump maps, volumetric clouds, starfield) is
- * rejected with MT_ERR_UNSUPPORTED; there is no CPU fallback.
+ * (CSG, SDF, bump maps, starfield / nebula / galaxy sky terms) is rejected
+ * with MT_ERR_UNSUPPORTED; there is no CPU fallback. The adjoint also
+ * rejects fog, textures, volumetric clouds and marched media.
  *
  * Threading: a scene handle may be used from one host thread at a time.
  * All calls are synchronous unless they take a `stream` argument.
@@ -74,14 +75,18 @@ extern "C" {
  *              n[0..8] are the vertex normals na, nb, nc (the reference's
  *              prim_triangle_smooth, radius > 0.5 gate, src/geometry.c:506)
  *   CYLINDER : v[0..2] base, v[3..5] top, v[6] r_bottom, v[7] r_top
+ * A TRIANGLE with `has_uv` set carries vertex texture coordinates
+ * uv = (ua, va, ub, vb, uc, vc) (prim_triangle_uv, src/geometry.c:280-295);
+ * its hit (u, v) interpolates them instead of being the barycentrics.
  */
 typedef struct {
     int32_t kind;
     int32_t material;
     int32_t smooth;
-    int32_t reserved;
+    int32_t has_uv;
     double  v[9];
     double  n[9];
+    double  uv[6];
 } mt_prim;
 
 /* Surface material: the `Material` fields the hot path reads (src/material.h). */
@@ -102,8 +107,27 @@ typedef struct {
     int32_t is_water;
     int32_t beer_lambert;
     int32_t pbr;
-    int32_t texture_kind;    /* must be 0 (TEXTURE_NONE)                           */
+    int32_t texture_kind;    /* MT_TEXTURE_* (TextureKind, src/material.h:33-42)   */
+    double  texture_scale;   /* world units per cell / UV repeat; <= 0 means 1     */
+    double  texture_color_a[3];
+    double  texture_color_b[3];
+    /* MT_TEXTURE_IMAGE: texture_width x texture_height sRGB bytes, RGB, top row
+       first (ImageTexture, src/texture.h); the library copies them at scene
+       creation. NULL leaves the albedo untextured, as the reference does. */
+    const unsigned char *texture_rgb;
+    int32_t texture_width;
+    int32_t texture_height;
 } mt_material;
+
+/* Material.texture_kind values (TextureKind, src/material.h:33-42). */
+#define MT_TEXTURE_NONE         0
+#define MT_TEXTURE_CHECKER      1
+#define MT_TEXTURE_STRIPES      2
+#define MT_TEXTURE_PLANET_EARTH 3
+#define MT_TEXTURE_PLANET_MOON  4
+#define MT_TEXTURE_NOISE        5
+#define MT_TEXTURE_IMAGE        6
+#define MT_TEXTURE_UV_CHECKER   7
 
 /* Sky / sun parameters (SkyParams, src/material.h). */
 typedef struct {
@@ -119,13 +143,16 @@ typedef struct {
     double   cloud_coverage;
     double   cloud_softness;
     double   cloud_sharpness;
-    double   cloud_thickness;   /* must be <= 1e-4 (planar clouds only)  */
+    double   cloud_thickness;   /* > 1e-4: volumetric ray-marched slab   */
     double   sun_radius;        /* degrees; 0 = hard sun                 */
     double   star_intensity;    /* must be 0                             */
     double   nebula_intensity;  /* must be 0                             */
     double   galaxy_intensity;  /* must be 0                             */
     int32_t  cloud_octaves;
     uint32_t seed;
+    double   cloud_density;     /* volumetric extinction (<= 0 means 0.08) */
+    int32_t  cloud_steps;       /* volumetric march steps                 */
+    int32_t  reserved;
 } mt_sky;
 
 /* Procedural Gerstner ocean height parameters (SceneOceanParams, src/scene.h:67-77). */
@@ -146,11 +173,19 @@ typedef struct {
     int32_t            material_count;
     const mt_material *materials;
     mt_sky             sky;
-    double             fog_density;     /* must be 0: fog is not on the GPU path */
+    double             fog_density;     /* FogParams.density (0 = no fog)        */
     double             water_level;     /* Scene.water_level                     */
     int32_t            water_material;  /* Scene.water_material, -1 = none      */
-    int32_t            fog_shadow_steps;/* FogParams.shadow_steps: must be 0     */
+    int32_t            fog_shadow_steps;/* FogParams.shadow_steps (0 = analytic) */
     mt_ocean           ocean;           /* Scene.has_ocean / ocean_params        */
+    /* the rest of FogParams (src/material.h:199-209) */
+    double             fog_color[3];
+    double             fog_height;
+    double             fog_height_falloff;
+    double             fog_inscatter_strength;
+    double             fog_sun_anisotropy;
+    double             fog_noise_scale;
+    double             fog_noise_amount;
 } mt_scene_desc;
 
 /* Pinhole / thin-lens camera (Camera, src/camera.h). */

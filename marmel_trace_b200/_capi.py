@@ -32,10 +32,14 @@ PRECISION_FP32, PRECISION_FP64 = 0, 1
 INTEGRATOR_MEGAKERNEL, INTEGRATOR_WAVEFRONT = 0, 1
 MODE_PATHTRACE, MODE_WHITTED = 0, 1
 
-# mt_prim (160 bytes) and mt_material (216 bytes) as numpy structured dtypes,
+TEXTURE_NONE, TEXTURE_CHECKER, TEXTURE_STRIPES, TEXTURE_PLANET_EARTH = 0, 1, 2, 3
+TEXTURE_PLANET_MOON, TEXTURE_NOISE, TEXTURE_IMAGE, TEXTURE_UV_CHECKER = 4, 5, 6, 7
+
+# mt_prim (208 bytes) and mt_material (288 bytes) as numpy structured dtypes,
 # so large primitive arrays cross the C ABI without a copy.
 PRIM_DTYPE = np.dtype(
-    [("kind", "<i4"), ("material", "<i4"), ("smooth", "<i4"), ("reserved", "<i4"), ("v", "<f8", 9), ("n", "<f8", 9)]
+    [("kind", "<i4"), ("material", "<i4"), ("smooth", "<i4"), ("has_uv", "<i4"), ("v", "<f8", 9), ("n", "<f8", 9),
+     ("uv", "<f8", 6)]
 )
 MATERIAL_DTYPE = np.dtype(
     [
@@ -56,9 +60,15 @@ MATERIAL_DTYPE = np.dtype(
         ("beer_lambert", "<i4"),
         ("pbr", "<i4"),
         ("texture_kind", "<i4"),
+        ("texture_scale", "<f8"),
+        ("texture_color_a", "<f8", 3),
+        ("texture_color_b", "<f8", 3),
+        ("texture_rgb", "<u8"),     # const unsigned char * (address of the image bytes, or 0)
+        ("texture_width", "<i4"),
+        ("texture_height", "<i4"),
     ]
 )
-assert PRIM_DTYPE.itemsize == 160 and MATERIAL_DTYPE.itemsize == 216
+assert PRIM_DTYPE.itemsize == 208 and MATERIAL_DTYPE.itemsize == 288
 
 D3 = C.c_double * 3
 
@@ -84,6 +94,9 @@ class MtSky(C.Structure):
         ("galaxy_intensity", C.c_double),
         ("cloud_octaves", C.c_int32),
         ("seed", C.c_uint32),
+        ("cloud_density", C.c_double),
+        ("cloud_steps", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -112,6 +125,13 @@ class MtSceneDesc(C.Structure):
         ("water_material", C.c_int32),
         ("fog_shadow_steps", C.c_int32),
         ("ocean", MtOcean),
+        ("fog_color", D3),
+        ("fog_height", C.c_double),
+        ("fog_height_falloff", C.c_double),
+        ("fog_inscatter_strength", C.c_double),
+        ("fog_sun_anisotropy", C.c_double),
+        ("fog_noise_scale", C.c_double),
+        ("fog_noise_amount", C.c_double),
     ]
 
 

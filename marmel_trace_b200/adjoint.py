@@ -7,8 +7,10 @@ and `backward(dL_dimage)` the path-replay adjoint (mt_adjoint_backward_device).
 forward saves nothing but the sample window -- the backward replays every path
 from its random stream instead of storing vertices.
 
-Parameter layout (mt_scene_param_count = 8 * materials + 3): per material
-albedo rgb, roughness, metallic, emissive rgb; then the sun radiance rgb.
+Parameter layout (mt_scene_param_count = 11 * materials + 3): per material
+albedo rgb, roughness, metallic, emissive rgb; then the sun radiance rgb; then
+per material the Beer-Lambert absorption rgb. Scenes with fog, textures,
+volumetric clouds or marched media are rejected (MT_ERR_UNSUPPORTED).
 """
 from __future__ import annotations
 

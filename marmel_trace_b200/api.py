@@ -44,8 +44,22 @@ SKY_DEFAULTS = dict(
     cloud_sharpness=1.5,
     cloud_octaves=5,
     cloud_thickness=0.0,
+    cloud_density=0.08,
+    cloud_steps=16,
     seed=1337,
     sun_radius=0.0,
+)
+
+# FogParams defaults (FOG_DEFAULT_*, src/material.h:185-193) besides density.
+FOG_DEFAULTS = dict(
+    color=(0.70, 0.75, 0.80),
+    height=0.0,
+    height_falloff=0.0,
+    inscatter_strength=0.50,
+    sun_anisotropy=0.70,
+    noise_scale=0.0,
+    noise_amount=0.0,
+    shadow_steps=0,
 )
 
 
@@ -79,6 +93,8 @@ class SceneDesc:
     fog_density: float = 0.0
     camera: dict | None = None  # eye, target, up, vfov (the scene's camera block)
     material_names: list[str] | None = None
+    fog: dict | None = None  # the other FogParams fields (FOG_DEFAULTS keys)
+    images: dict | None = None  # material index -> (H, W, 3) uint8 sRGB image (MT_TEXTURE_IMAGE)
 
     def __post_init__(self):
         assert self.prims.dtype == PRIM_DTYPE and self.materials.dtype == MATERIAL_DTYPE
@@ -109,10 +125,23 @@ class SceneDesc:
             setattr(d.sky, k, float(s[k]))
         d.sky.cloud_octaves = int(s["cloud_octaves"])
         d.sky.seed = int(s["seed"]) & 0xFFFFFFFF
+        d.sky.cloud_density = float(s.get("cloud_density", SKY_DEFAULTS["cloud_density"]))
+        d.sky.cloud_steps = int(s.get("cloud_steps", SKY_DEFAULTS["cloud_steps"]))
         d.fog_density = float(self.fog_density)
         d.water_level = float(self.water_level)
         d.water_material = int(self.water_material)
-        d.fog_shadow_steps = 0
+        f = dict(FOG_DEFAULTS, **(self.fog or {}))
+        d.fog_color = capi.D3(*f["color"])
+        for k in ("height", "height_falloff", "inscatter_strength", "sun_anisotropy", "noise_scale", "noise_amount"):
+            setattr(d, "fog_" + k, float(f[k]))
+        d.fog_shadow_steps = int(f["shadow_steps"])
+        # image textures: the materials array carries the address of each image
+        for i, img in (self.images or {}).items():
+            img = np.ascontiguousarray(img, np.uint8)
+            assert img.ndim == 3 and img.shape[2] == 3
+            self.images[i] = img
+            self.materials[i]["texture_rgb"] = img.ctypes.data
+            self.materials[i]["texture_height"], self.materials[i]["texture_width"] = img.shape[:2]
         return d
 
     def make_camera(self, width: int, height: int) -> "Camera":

@@ -77,6 +77,15 @@ static int mtb_prim(const Primitive *p, mt_prim *o)
             v3(o->n + 3, p->axis);
             v3(o->n + 6, p->half);
         }
+        if (p->has_uv) { /* vertex texture coordinates, src/geometry.c:527-531 */
+            o->has_uv = 1;
+            o->uv[0] = p->uva.x;
+            o->uv[1] = p->uva.y;
+            o->uv[2] = p->uvb.x;
+            o->uv[3] = p->uvb.y;
+            o->uv[4] = p->uvc.x;
+            o->uv[5] = p->uvc.y;
+        }
         return 0;
     case PRIM_CYLINDER:
         o->kind = MT_PRIM_CYLINDER;
@@ -110,6 +119,15 @@ static void mtb_material(const Material *m, mt_material *o)
     o->beer_lambert = m->beer_lambert;
     o->pbr = m->pbr;
     o->texture_kind = m->texture_kind;
+    o->texture_scale = m->texture_scale;
+    v3(o->texture_color_a, m->texture_color_a);
+    v3(o->texture_color_b, m->texture_color_b);
+    if (m->texture_image) {
+        const ImageTexture *img = (const ImageTexture *)m->texture_image;
+        o->texture_rgb = img->rgb;
+        o->texture_width = img->width;
+        o->texture_height = img->height;
+    }
 }
 
 static void mtb_sky(const SkyParams *s, mt_sky *o)
@@ -134,6 +152,8 @@ static void mtb_sky(const SkyParams *s, mt_sky *o)
     o->galaxy_intensity = s->galaxy_intensity;
     o->cloud_octaves = s->cloud_octaves;
     o->seed = s->seed;
+    o->cloud_density = s->cloud_density;
+    o->cloud_steps = s->cloud_steps;
 }
 
 /*
@@ -155,6 +175,13 @@ int mtb_scene_to_desc(const Scene *s, mt_prim *prims, mt_material *mats, mt_scen
     mtb_sky(&s->sky, &d->sky);
     d->fog_density = s->fog.density;
     d->fog_shadow_steps = s->fog.shadow_steps;
+    v3(d->fog_color, s->fog.color);
+    d->fog_height = s->fog.height;
+    d->fog_height_falloff = s->fog.height_falloff;
+    d->fog_inscatter_strength = s->fog.inscatter_strength;
+    d->fog_sun_anisotropy = s->fog.sun_anisotropy;
+    d->fog_noise_scale = s->fog.noise_scale;
+    d->fog_noise_amount = s->fog.noise_amount;
     d->water_level = s->water_level;
     d->water_material = s->water_material;
     d->ocean.enabled = s->has_ocean;

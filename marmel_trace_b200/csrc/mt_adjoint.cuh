@@ -584,7 +584,7 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
 // One thread per pixel: both passes for each of the pixel's samples, then
 // the block's gradient is flushed with one atomic per parameter.
 template <typename R>
-__global__ void __launch_bounds__(128) k_adjoint(const DevScene<R> S, const DevCamera<R> cam, int w, int h, int s0,
+__global__ void __launch_bounds__(128) k_adjoint(const __grid_constant__ DevScene<R> S, const DevCamera<R> cam, int w, int h, int s0,
                                                  int s1, int depth, const float *adj_img, double adj_scale,
                                                  double *grad_out, int n_params)
 {

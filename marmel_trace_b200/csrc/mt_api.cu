@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -99,6 +100,7 @@ struct mt_scene {
     WavefrontState *wf = nullptr;
     // host copies used by parameter updates (mt_scene_set_material_params)
     std::vector<mt_material> h_mats;
+    std::vector<const unsigned char *> d_tex;  // per material: device copy of its image texture (or NULL)
     mt_sky h_sky;
     std::vector<HostSphere> h_spheres;
     int version = 0;
@@ -131,15 +133,15 @@ int validate(const mt_scene_desc *d)
     if (d->prim_count > 0 && !d->prims) return fail(MT_ERR_NULL, "prims is NULL");
     if (d->material_count > 0 && !d->materials) return fail(MT_ERR_NULL, "materials is NULL");
     if (d->prim_count >= (1 << 28)) return fail(MT_ERR_UNSUPPORTED, "more than 2^28 primitives");
-    if (d->fog_density > 0.0) return fail(MT_ERR_UNSUPPORTED, "fog is not on the GPU path");
-    if (d->fog_shadow_steps > 0) return fail(MT_ERR_UNSUPPORTED, "volumetric fog/water marching is not on the GPU path");
     const mt_sky &s = d->sky;
-    if (s.cloud_thickness > 1e-4) return fail(MT_ERR_UNSUPPORTED, "volumetric clouds are not on the GPU path");
     if (s.star_intensity > 0.0 || s.nebula_intensity > 0.0 || s.galaxy_intensity > 0.0)
         return fail(MT_ERR_UNSUPPORTED, "starfield / nebula / galaxy sky terms are not on the GPU path");
     for (int i = 0; i < d->material_count; ++i) {
         const mt_material &m = d->materials[i];
-        if (m.texture_kind != 0) return fail(MT_ERR_UNSUPPORTED, "material %d: textures are not on the GPU path", i);
+        if (m.texture_kind < MT_TEXTURE_NONE || m.texture_kind > MT_TEXTURE_UV_CHECKER)
+            return fail(MT_ERR_INVALID, "material %d: texture kind %d", i, m.texture_kind);
+        if (m.texture_rgb && (m.texture_width <= 0 || m.texture_height <= 0))
+            return fail(MT_ERR_INVALID, "material %d: image texture of %d x %d", i, m.texture_width, m.texture_height);
         if (m.bump_strength > 1e-6) return fail(MT_ERR_UNSUPPORTED, "material %d: bump maps are not on the GPU path", i);
     }
     for (int i = 0; i < d->prim_count; ++i) {
@@ -150,9 +152,19 @@ int validate(const mt_scene_desc *d)
     return 0;
 }
 
-template <typename R> void fill_material(const mt_material &m, DevMaterial<R> *o)
+// `tex`: the device copy of the material's image texture (or NULL).
+template <typename R> void fill_material(const mt_material &m, const unsigned char *tex, DevMaterial<R> *o)
 {
     memset(o, 0, sizeof *o);
+    o->texture_kind = m.texture_kind;
+    o->texture_scale = (R)m.texture_scale;
+    for (int k = 0; k < 3; ++k) {
+        o->texture_color_a[k] = (R)m.texture_color_a[k];
+        o->texture_color_b[k] = (R)m.texture_color_b[k];
+    }
+    o->texture_rgb = tex;
+    o->texture_width = tex ? m.texture_width : 0;
+    o->texture_height = tex ? m.texture_height : 0;
     for (int k = 0; k < 3; ++k) {
         o->albedo[k] = (R)m.albedo[k];
         o->specular[k] = (R)m.specular[k];
@@ -189,8 +201,25 @@ template <typename R> void fill_sky(const mt_sky &s, DevSky<R> *o)
     o->cloud_softness = (R)s.cloud_softness;
     o->cloud_sharpness = (R)s.cloud_sharpness;
     o->sun_radius = (R)s.sun_radius;
+    o->cloud_thickness = (R)s.cloud_thickness;
+    o->cloud_density = (R)s.cloud_density;
+    o->cloud_steps = s.cloud_steps;
     o->cloud_octaves = s.cloud_octaves;
     o->seed = s.seed;
+}
+
+template <typename R> void fill_fog(const mt_scene_desc &d, DevFog<R> *o)
+{
+    memset(o, 0, sizeof *o);
+    o->density = (R)d.fog_density;
+    for (int k = 0; k < 3; ++k) o->color[k] = (R)d.fog_color[k];
+    o->height = (R)d.fog_height;
+    o->height_falloff = (R)d.fog_height_falloff;
+    o->inscatter_strength = (R)d.fog_inscatter_strength;
+    o->sun_anisotropy = (R)d.fog_sun_anisotropy;
+    o->noise_scale = (R)d.fog_noise_scale;
+    o->noise_amount = (R)d.fog_noise_amount;
+    o->shadow_steps = d.fog_shadow_steps;
 }
 
 // scene_collect_emissive_lights (src/scene.c:1384-1426): the first 8 emissive
@@ -229,11 +258,13 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     std::vector<int2> prim_info(n > 0 ? n : 1, make_int2(0, -1));
     std::vector<int2> refs(fb.ref_prim.size());
     std::vector<float4> tri4;
-    std::vector<R> tris, tri_normals, spheres, boxes, cyls, planes;
+    std::vector<R> tris, tri_normals, tri_uv, spheres, boxes, cyls, planes;
     std::vector<int> tri_smooth, plane_prims;
-    bool any_smooth = false;
-    for (int i = 0; i < n; ++i)
+    bool any_smooth = false, any_uv = false;
+    for (int i = 0; i < n; ++i) {
         if (d->prims[i].kind == MT_PRIM_TRIANGLE && d->prims[i].smooth) any_smooth = true;
+        if (d->prims[i].kind == MT_PRIM_TRIANGLE && d->prims[i].has_uv) any_uv = true;
+    }
 
     int ntri = 0, nsph = 0, nbox = 0, ncyl = 0;
     for (size_t k = 0; k < fb.ref_prim.size(); ++k) {
@@ -274,6 +305,9 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
             }
             if (any_smooth)
                 for (int j = 0; j < 9; ++j) tri_normals.push_back((R)p.n[j]);
+            if (any_uv)
+                for (int j = 0; j < 6; ++j)
+                    tri_uv.push_back(p.has_uv ? (R)p.uv[j] : std::numeric_limits<R>::quiet_NaN());
             break;
         }
         default:
@@ -293,8 +327,23 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
         prim_info[pi] = make_int2((KIND_PLANE << 28) | (int)k, p.material);
     }
 
+    // image textures: one device copy per material, kept for the scene's life
+    // (shared by the FP32 and FP64 uploads)
+    if (sc->d_tex.size() != (size_t)d->material_count) {
+        sc->d_tex.assign(d->material_count, nullptr);
+        for (int i = 0; i < d->material_count; ++i) {
+            const mt_material &m = d->materials[i];
+            if (!m.texture_rgb) continue;
+            std::vector<unsigned char> img(m.texture_rgb,
+                                           m.texture_rgb + (size_t)m.texture_width * m.texture_height * 3);
+            const unsigned char *dp = nullptr;
+            int rc = sc->upload(img, &dp);
+            if (rc) return rc;
+            sc->d_tex[i] = dp;
+        }
+    }
     std::vector<DevMaterial<R>> mats(d->material_count);
-    for (int i = 0; i < d->material_count; ++i) fill_material(d->materials[i], &mats[i]);
+    for (int i = 0; i < d->material_count; ++i) fill_material(d->materials[i], sc->d_tex[i], &mats[i]);
 
     std::vector<float4> nodes(fb.nodes.size() / 4);
     if (!fb.nodes.empty()) memcpy(nodes.data(), fb.nodes.data(), fb.nodes.size() * sizeof(float));
@@ -323,6 +372,7 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     if ((rc = sc->upload(tri4, &S->tri4))) return rc;
     if ((rc = sc->upload(tris, &S->tris))) return rc;
     if ((rc = sc->upload(tri_normals, &S->tri_normals))) return rc;
+    if ((rc = sc->upload(tri_uv, &S->tri_uv))) return rc;
     if ((rc = sc->upload(tri_smooth, &S->tri_smooth))) return rc;
     if (sizeof(R) == 8 && ntri > 0)
         if ((rc = sc->upload(tri_prim, &S->tri_prim))) return rc;
@@ -363,9 +413,12 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     S->ocean.chop = (R)d->ocean.chop;
     S->ocean.chop_wavelength = (R)d->ocean.chop_wavelength;
     fill_sky(d->sky, &S->sky);
+    fill_fog(*d, &S->fog);
 
-    // host copies for parameter updates (materials, sun, sphere list)
+    // host copies for parameter updates (materials, sun, sphere list); the
+    // image pointers are the caller's and are not kept
     sc->h_mats.assign(d->materials, d->materials + d->material_count);
+    for (mt_material &m : sc->h_mats) m.texture_rgb = nullptr;
     sc->h_sky = d->sky;
     sc->h_spheres.clear();
     for (int i = 0; i < n; ++i)
@@ -1241,7 +1294,7 @@ namespace {
 template <typename R> int apply_params(mt_scene *sc, DevScene<R> *S)
 {
     std::vector<DevMaterial<R>> mats(sc->h_mats.size());
-    for (size_t i = 0; i < mats.size(); ++i) fill_material(sc->h_mats[i], &mats[i]);
+    for (size_t i = 0; i < mats.size(); ++i) fill_material(sc->h_mats[i], sc->d_tex[i], &mats[i]);
     if (!mats.empty())
         CK(cudaMemcpy((void *)S->materials, mats.data(), mats.size() * sizeof(DevMaterial<R>), cudaMemcpyHostToDevice),
            "cudaMemcpy(materials)");
@@ -1288,6 +1341,16 @@ int mt_adjoint_backward_device(mt_scene *sc, const mt_camera *cam, int w, int h,
     if (!grad_dev) return fail(MT_ERR_NULL, "NULL gradient buffer");
     if (s0 < 0) return fail(MT_ERR_COUNTS, "negative first sample");
     const int M = (int)sc->h_mats.size();
+    // the replay's gradient terms cover the scene content of the benchmark
+    // configurations; these features change paths in ways it does not model
+    if (sc->sf.fog.density > 0 || sc->sd.fog.density > 0)
+        return fail(MT_ERR_UNSUPPORTED, "the adjoint does not support fog");
+    if (sc->sf.fog.shadow_steps > 0 || sc->sd.fog.shadow_steps > 0)
+        return fail(MT_ERR_UNSUPPORTED, "the adjoint does not support marched media (fog shadow_steps > 0)");
+    if (sc->h_sky.cloud_thickness > 1e-4) return fail(MT_ERR_UNSUPPORTED, "the adjoint does not support volumetric clouds");
+    for (int m = 0; m < M; ++m)
+        if (sc->h_mats[m].texture_kind != MT_TEXTURE_NONE)
+            return fail(MT_ERR_UNSUPPORTED, "the adjoint does not support textures (material %d)", m);
     if (M > kAdjMaxMaterialsApi) return fail(MT_ERR_UNSUPPORTED, "the adjoint supports at most %d materials",
                                              kAdjMaxMaterialsApi);
     if ((rc = set_device(sc))) return rc;

@@ -225,8 +225,16 @@ template <typename R> MT_D bool box_occluded(const R *b, V3<R> o, V3<R> d, R tmi
 // Tapered capped cylinder (intersect_cylinder src/geometry.c:549-699).
 // Returns t and the outward normal (before facing the ray).
 // ------------------------------------------------------------------
+// Which surface of a tapered cylinder was hit (for the hit's texture u, v).
+template <typename R> struct CylPart {
+    int is_cap;  // 1: a cap disc, 0: the side
+    int cap;     // 0: base (s = 0), 1: top (s = 1)
+    R s;         // side: axial coordinate in [0, 1]
+};
+
 template <typename R>
-MT_D bool cylinder_hit(const R *c, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out, V3<R> *n_out)
+MT_D bool cylinder_hit(const R *c, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out, V3<R> *n_out,
+                       CylPart<R> *part = nullptr)
 {
     V3<R> pa = v3(c[0], c[1], c[2]);
     V3<R> pb = v3(c[3], c[4], c[5]);
@@ -248,7 +256,8 @@ MT_D bool cylinder_hit(const R *c, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out, V
     R qc = length_sq(d0_perp) - rb * rb;
 
     bool found = false;
-    R best_t = R(0);
+    R best_t = R(0), best_s = R(0);
+    int best_is_cap = 0, best_cap = 0;
     V3<R> best_n = v3(R(0), R(0), R(0));
 
     if (mfabs(qa) > R(1e-15)) {
@@ -280,6 +289,7 @@ MT_D bool cylinder_hit(const R *c, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out, V
                     found = true;
                     best_t = t;
                     best_n = n;
+                    best_s = s;
                 }
             }
         }
@@ -298,6 +308,7 @@ MT_D bool cylinder_hit(const R *c, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out, V
                 found = true;
                 best_t = t;
                 best_n = n;
+                best_s = s;
             }
         }
     }
@@ -317,12 +328,19 @@ MT_D bool cylinder_hit(const R *c, V3<R> o, V3<R> d, R tmin, R tmax, R *t_out, V
                 found = true;
                 best_t = t;
                 best_n = n;
+                best_is_cap = 1;
+                best_cap = cap;
             }
         }
     }
     if (!found) return false;
     *t_out = best_t;
     *n_out = best_n;
+    if (part) {
+        part->is_cap = best_is_cap;
+        part->cap = best_cap;
+        part->s = best_s;
+    }
     return true;
 }
 
@@ -925,6 +943,8 @@ template <typename R> struct SurfaceHit {
     int prim;
     int material;
     int front_face;
+    int code;       // kind << 28 | slot (hit_uv)
+    R bu, bv;       // triangle barycentrics of the traversal hit (hit_uv)
 };
 
 // geo_store_hit (src/geometry.c:78-91): orient the unit normal against the ray.
@@ -946,6 +966,9 @@ MT_D void finish_hit(const DevScene<R> &S, V3<R> o, V3<R> d, const Hit<R> &h, Su
     int slot = h.code & 0x0FFFFFFF;
     out->prim = h.prim;
     out->material = __ldg(S.prim_info + h.prim).y;
+    out->code = h.code;
+    out->bu = h.u;
+    out->bv = h.v;
     V3<R> point = at(o, d, h.t);
     switch (kind) {
     case KIND_SPHERE: {
@@ -1022,6 +1045,124 @@ MT_D void finish_hit(const DevScene<R> &S, V3<R> o, V3<R> d, const Hit<R> &h, Su
 }
 
 // scene_intersect (src/scene.c:767-775) with the full hit record.
+// The reference's hit (u, v) for UV-mapped textures: sphere longitude /
+// latitude (src/geometry.c:359-366), plane tangent coordinates (:383-390),
+// box face coordinates (:463-476), cylinder cap disc or side angle / height
+// (:665-696), triangle barycentrics or interpolated vertex UVs (:526-534).
+// o, d: the ray of the hit (d unit); h: the traversal hit.
+template <typename R> MT_D V3<R> uv_tangent(V3<R> n, V3<R> *b)
+{
+    V3<R> up = (mfabs(n.y) > R(0.9)) ? v3(R(0), R(0), R(1)) : v3(R(0), R(1), R(0));
+    V3<R> t = normalize(cross(up, n));
+    *b = cross(n, t);
+    return t;
+}
+
+template <typename R>
+MT_NOINLINE void hit_uv(const DevScene<R> &S, V3<R> o, V3<R> d, const Hit<R> &h, R *u_out, R *v_out)
+{
+    const int kind = h.code >> 28;
+    const int slot = h.code & 0x0FFFFFFF;
+    const V3<R> point = at(o, d, h.t);
+    const R two_pi = R(2) * R(3.14159265358979323846);
+    R u = R(0), v = R(0);
+    switch (kind) {
+    case KIND_SPHERE: {
+        const R *s = S.spheres + 4 * (size_t)slot;
+        V3<R> n = scale(sub(point, v3(s[0], s[1], s[2])), R(1) / s[3]);
+        R phi = matan2(n.z, n.x);
+        R theta = masin(mfmax(R(-1), mfmin(R(1), n.y)));
+        u = R(0.5) + phi / two_pi;
+        v = R(0.5) + theta / R(3.14159265358979323846);
+        u = u - mfloor(u);
+        v = mfmax(R(0), mfmin(R(1), v));
+        break;
+    }
+    case KIND_PLANE: {
+        const R *p = S.planes + 6 * (size_t)slot;
+        V3<R> n = v3(p[3], p[4], p[5]), B;
+        V3<R> T = uv_tangent(n, &B);
+        V3<R> diff = sub(point, v3(p[0], p[1], p[2]));
+        u = dot(diff, T);
+        v = dot(diff, B);
+        u = u - mfloor(u);
+        v = v - mfloor(v);
+        break;
+    }
+    case KIND_BOX: {
+        const R *b = S.boxes + 6 * (size_t)slot;
+        R t;
+        int axis = -1, sign = 0;
+        box_t(b, o, d, h.t, h.t, &t, &axis, &sign);
+        const R lo[3] = {b[0] - b[3], b[1] - b[4], b[2] - b[5]};
+        const R hi[3] = {b[0] + b[3], b[1] + b[4], b[2] + b[5]};
+        const R dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        if (axis == 0) {
+            u = (dz > R(1e-12)) ? (point.z - lo[2]) / dz : R(0);
+            v = (dy > R(1e-12)) ? (point.y - lo[1]) / dy : R(0);
+        } else if (axis == 1) {
+            u = (dx > R(1e-12)) ? (point.x - lo[0]) / dx : R(0);
+            v = (dz > R(1e-12)) ? (point.z - lo[2]) / dz : R(0);
+        } else {
+            u = (dx > R(1e-12)) ? (point.x - lo[0]) / dx : R(0);
+            v = (dy > R(1e-12)) ? (point.y - lo[1]) / dy : R(0);
+        }
+        u = mfmax(R(0), mfmin(R(1), u));
+        v = mfmax(R(0), mfmin(R(1), v));
+        break;
+    }
+    case KIND_CYLINDER: {
+        const R *c = S.cyls + 8 * (size_t)slot;
+        R t;
+        V3<R> n;
+        CylPart<R> part;
+        part.is_cap = 0;
+        part.cap = 0;
+        part.s = R(0);
+        cylinder_hit(c, o, d, h.t, h.t, &t, &n, &part);
+        const V3<R> pa = v3(c[0], c[1], c[2]), pb = v3(c[3], c[4], c[5]);
+        const V3<R> A = sub(pb, pa);
+        const R hgt = length(A);
+        const V3<R> axis = scale(A, R(1) / hgt);
+        V3<R> B;
+        V3<R> T = uv_tangent(axis, &B);
+        if (part.is_cap) {
+            const V3<R> cap_center = part.cap == 0 ? pa : pb;
+            const R r_cap = part.cap == 0 ? c[6] : c[7];
+            V3<R> radial = sub(point, cap_center);
+            R rx = (r_cap > R(1e-12)) ? dot(radial, T) / (R(2) * r_cap) : R(0);
+            R ry = (r_cap > R(1e-12)) ? dot(radial, B) / (R(2) * r_cap) : R(0);
+            u = mfmax(R(0), mfmin(R(1), R(0.5) + rx));
+            v = mfmax(R(0), mfmin(R(1), R(0.5) + ry));
+        } else {
+            V3<R> axis_pt = add(pa, scale(axis, part.s * hgt));
+            V3<R> radial = sub(point, axis_pt);
+            R phi = matan2(dot(radial, B), dot(radial, T));
+            u = R(0.5) + phi / two_pi;
+            u = u - mfloor(u);
+            v = mfmax(R(0), mfmin(R(1), part.s));
+        }
+        break;
+    }
+    case KIND_TRIANGLE:
+    default: {
+        u = h.u;
+        v = h.v;
+        if (S.tri_uv) {
+            const R *q = S.tri_uv + 6 * (size_t)slot;
+            if (q[0] == q[0]) {  // not NaN: the triangle has vertex UVs
+                R w = R(1) - h.u - h.v;
+                u = w * q[0] + h.u * q[2] + h.v * q[4];
+                v = w * q[1] + h.u * q[3] + h.v * q[5];
+            }
+        }
+        break;
+    }
+    }
+    *u_out = u;
+    *v_out = v;
+}
+
 template <typename R>
 MT_D bool scene_intersect(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax, SurfaceHit<R> *out)
 {

@@ -172,6 +172,136 @@ MT_D bool pt_occluded_segment(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R 
     return true;
 }
 
+// pt_fog_segment (src/pathtrace.c:614-730): with fog.shadow_steps > 0 a
+// jittered march with a shadow segment toward the sun per step (god rays),
+// then the analytic remainder; otherwise the analytic fog_segment.
+template <typename R>
+MT_NOINLINE void pt_fog_segment(const DevScene<R> &S, V3<R> o, V3<R> d, R dist, uint32_t seed_key, int bounce,
+                                R *transmittance, V3<R> *inscatter)
+{
+    const DevFog<R> &fog = S.fog;
+    if (fog.shadow_steps <= 0) {
+        fog_segment(fog, S.sky, o, d, dist, transmittance, inscatter);
+        return;
+    }
+    int steps = fog.shadow_steps;
+    if (steps < 4) steps = 4;
+    if (steps > 128) steps = 128;
+    const bool is_sky = dist >= R(1e20);
+    const R lambda = fog.height_falloff;
+    R max_t;
+    if (is_sky) {
+        R top_y = (lambda > R(1e-4)) ? (fog.height + R(3) / lambda) : R(25);
+        if (o.y >= top_y && d.y >= R(0)) {
+            *transmittance = R(1);
+            *inscatter = v3(R(0), R(0), R(0));
+            return;
+        }
+        R dy = d.y;
+        if (dy > R(0.02)) {
+            max_t = (top_y - o.y) / dy;
+            if (max_t > R(40)) max_t = R(40);
+        } else {
+            max_t = R(40);
+        }
+    } else {
+        max_t = (dist > R(60)) ? R(60) : dist;
+    }
+    const R dt = max_t / R(steps);
+    const V3<R> sun_dir = mat3(S.sky.sun_dir);
+    R phase_hg = fog_phase_hg(fog, d, sun_dir);
+    if (phase_hg > R(6)) phase_hg = R(6);
+    const R phase = R(0.70) * phase_hg + R(0.30);
+    const V3<R> sun_glow_unit = scale(mat3(S.sky.sun_color), phase * fog.inscatter_strength);
+    R T_acc = R(1);
+    V3<R> acc = v3(R(0), R(0), R(0));
+    const R jitter = rand01<R>(seed_key, (uint32_t)bounce, 0xFE01u);
+    for (int i = 0; i < steps; ++i) {
+        R t = (R(i) + jitter) * dt;
+        V3<R> pos = add(o, scale(d, t));
+        R rho = fog.density;
+        if (lambda > R(1e-6)) {
+            R h_diff = pos.y - fog.height;
+            rho *= mexp(-lambda * h_diff);
+        }
+        if (fog.noise_amount > R(1e-4) && fog.noise_scale > R(1e-4)) rho *= fog_noise_mod(fog, pos);
+        if (rho < R(0)) rho = R(0);
+        R step_tau = rho * dt;
+        R step_T = mexp(-step_tau);
+        V3<R> atten;
+        bool in_shadow = pt_occluded_segment(S, pos, sun_dir, R(0.05), R(100), &atten);
+        if (!in_shadow) atten = scale(atten, cloud_transmittance(S.sky, pos, sun_dir));
+        V3<R> col = mat3(fog.color);
+        if (!in_shadow) col = add(col, mul(sun_glow_unit, atten));
+        V3<R> step_inscatter = scale(col, R(1) - step_T);
+        acc = add(acc, scale(step_inscatter, T_acc));
+        T_acc *= step_T;
+        if (T_acc < R(1e-4)) break;
+    }
+    if (dist > max_t) {
+        R rem_dist = is_sky ? R(1e30) : (dist - max_t);
+        V3<R> rem_o = add(o, scale(d, max_t));
+        R rem_T;
+        V3<R> rem_in;
+        fog_segment(fog, S.sky, rem_o, d, rem_dist, &rem_T, &rem_in);
+        acc = add(acc, scale(rem_in, T_acc));
+        T_acc *= rem_T;
+    }
+    *transmittance = T_acc;
+    *inscatter = acc;
+}
+
+// The march of pt_water_segment (src/pathtrace.c:748-795): underwater god
+// rays from sun shadow segments.
+template <typename R>
+MT_NOINLINE void pt_water_march(const DevScene<R> &S, int medium, V3<R> o, V3<R> d, R dist, uint32_t seed_key,
+                                int bounce, V3<R> *beta, V3<R> *radiance)
+{
+    const DevMaterial<R> &m = S.materials[medium];
+    int steps = S.fog.shadow_steps;
+    if (steps < 4) steps = 4;
+    if (steps > 16) steps = 16;
+    const R dt = dist / R(steps);
+    const V3<R> sun_dir = mat3(S.sky.sun_dir);
+    R cos_theta = dot(d, sun_dir);
+    const R g = R(0.72);
+    R denom = R(1) + g * g - R(2) * g * cos_theta;
+    if (denom < R(1e-4)) denom = R(1e-4);
+    R phase = (R(1) - g * g) / (denom * msqrt(denom));
+    if (phase > R(4.5)) phase = R(4.5);
+    const R jitter = rand01<R>(seed_key, (uint32_t)bounce, 0xAC31u);
+    const V3<R> step_T = v3(mexp(-m.absorption[0] * dt), mexp(-m.absorption[1] * dt), mexp(-m.absorption[2] * dt));
+    for (int i = 0; i < steps; ++i) {
+        R t = (R(i) + jitter) * dt;
+        V3<R> pos = add(o, scale(d, t));
+        V3<R> atten;
+        bool in_shadow = pt_occluded_segment(S, pos, sun_dir, R(0.02), R(100), &atten);
+        if (!in_shadow) atten = scale(atten, cloud_transmittance(S.sky, pos, sun_dir));
+        V3<R> ambient = scale(mat3(m.deep_color), R(0.40));
+        V3<R> sun_scat = v3(R(0), R(0), R(0));
+        if (!in_shadow) sun_scat = scale(mul(mat3(S.sky.sun_color), atten), phase * R(0.18));
+        V3<R> step_col = add(ambient, sun_scat);
+        V3<R> step_in = v3(step_col.x * (R(1) - step_T.x), step_col.y * (R(1) - step_T.y), step_col.z * (R(1) - step_T.z));
+        *radiance = add(*radiance, mul(*beta, step_in));
+        *beta = mul(*beta, step_T);
+    }
+}
+
+// pt_water_segment (src/pathtrace.c:737-795): a water medium with
+// fog.shadow_steps > 0 is marched; otherwise (and for other media) it is
+// pt_apply_medium.
+template <typename R>
+MT_D void pt_water_segment(const DevScene<R> &S, int medium, V3<R> o, V3<R> d, R dist, uint32_t seed_key, int bounce,
+                           V3<R> *beta, V3<R> *radiance)
+{
+    const DevMaterial<R> &m = S.materials[medium];
+    if (!m.is_water || S.fog.shadow_steps <= 0 || dist <= R(1e-4)) {
+        pt_apply_medium(m, dist, beta, radiance);
+        return;
+    }
+    pt_water_march(S, medium, o, d, dist, seed_key, bounce, beta, radiance);
+}
+
 // Distances a shadow segment travels through absorbing (Beer-Lambert)
 // materials, for the adjoint: up to two materials, `mat` -1 when unused.
 template <typename R> struct AbsorbPath {
@@ -239,8 +369,7 @@ MT_D V3<R> pt_nee_sun(const DevScene<R> &S, const DevMaterial<R> &mm, V3<R> P, V
     V3<R> so = add(P, scale(N, R(1e-3)));
     V3<R> atten;
     if (pt_occluded_segment(S, so, L, R(1e-3), R(1e30), &atten)) return zero;
-    // sky_cloud_transmittance is exactly 1 without volumetric clouds
-    // (src/material.c:418-421); volumetric clouds are rejected on upload.
+    atten = scale(atten, cloud_transmittance(S.sky, so, L));
     if (atten.x < R(1e-4) && atten.y < R(1e-4) && atten.z < R(1e-4)) return zero;
     R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
     R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
@@ -445,16 +574,30 @@ MT_D V3<R> pathtrace_radiance(const DevScene<R> &S, Ray3<R> primary, int max_dep
         SurfaceHit<R> h;
         if (!scene_intersect(S, r.o, r.d, R(1e-4), R(1e30), &h)) {
             if (medium >= 0) {
-                // pt_water_segment without volumetric steps == pt_apply_medium
-                // (src/pathtrace.c:737-747; fog shadow_steps is 0 on this path)
-                pt_apply_medium(S.materials[medium], R(5.0), &throughput, &radiance);
+                pt_water_segment(S, medium, r.o, r.d, R(5.0), seed_key, b, &throughput, &radiance);
                 medium = -1;
             }
             V3<R> sky_col = sky_sample(r.d, S.sky);
+            if (S.fog.density > R(0)) {
+                R T;
+                V3<R> ins;
+                if (b == 0) pt_fog_segment(S, r.o, r.d, R(1e30), seed_key, b, &T, &ins);
+                else fog_segment(S.fog, S.sky, r.o, r.d, R(1e30), &T, &ins);
+                sky_col = add(scale(sky_col, T), ins);
+            }
             radiance = add(radiance, mul(throughput, sky_col));
             break;
         }
-        if (medium >= 0) pt_apply_medium(S.materials[medium], h.t, &throughput, &radiance);
+        if (medium >= 0) {
+            pt_water_segment(S, medium, r.o, r.d, h.t, seed_key, b, &throughput, &radiance);
+        } else if (S.fog.density > R(0)) {
+            R T;
+            V3<R> ins;
+            if (b == 0) pt_fog_segment(S, r.o, r.d, h.t, seed_key, b, &T, &ins);
+            else fog_segment(S.fog, S.sky, r.o, r.d, h.t, &T, &ins);
+            radiance = add(radiance, mul(throughput, ins));
+            throughput = scale(throughput, T);
+        }
         if (h.material < 0 || h.material >= S.material_count) {
             radiance = add(radiance, mul(throughput, sky_sample(r.d, S.sky)));
             break;
@@ -471,7 +614,18 @@ MT_D V3<R> pathtrace_radiance(const DevScene<R> &S, Ray3<R> primary, int max_dep
         N = normalize(N);
         if (length_sq(N) <= R(0)) break;
         V3<R> V = neg(d);
-        const DevMaterial<R> &mm = m;  // TEXTURE_NONE: texture_albedo_uv is the identity
+        // texture-modulated albedo on a local copy (src/pathtrace.c:903-905)
+        DevMaterial<R> m_tex;
+        const DevMaterial<R> *mp = &m;
+        if (m.texture_kind != 0) {
+            m_tex = m;
+            V3<R> a = surface_albedo(S, m, r.o, unit_dir(r.d), h);
+            m_tex.albedo[0] = a.x;
+            m_tex.albedo[1] = a.y;
+            m_tex.albedo[2] = a.z;
+            mp = &m_tex;
+        }
+        const DevMaterial<R> &mm = *mp;
         if (b == 0 || last_bounce_specular) radiance = add(radiance, mul(throughput, mat3(mm.emissive)));
         if (b == 0 && length_sq(mat3(mm.atmosphere_glow)) > R(1e-6))
             radiance = add(radiance, mul(throughput, atmosphere_term(mm, N, V, mat3(S.sky.sun_dir))));
@@ -550,11 +704,27 @@ template <typename R> struct WhFrame {
     V3<R> P, N;          // shading point / normal
     V3<R> color;         // local (ambient + sun + emitters)
     V3<R> refl;          // reflection accumulator
+    V3<R> alb;           // the hit's (texture-modulated) albedo
     R t;                 // hit distance (refraction child: the exit distance)
     R F;                 // Schlick at cos_t
+    R fog_t;             // trace(): distance fog applies over (1e30 for the sky)
     int mat, prim, front;
     int depth, phase, gi, tir;
+    int traced;          // entered through trace(): fog_apply on return (src/render.c:842-863)
 };
+
+// The hit fields of a Whitted frame, with its albedo (src/render.c:620-621).
+template <typename R> MT_D void wh_set_hit(const DevScene<R> &S, WhFrame<R> &f, V3<R> o, V3<R> d, const SurfaceHit<R> &h)
+{
+    f.P = h.point;
+    f.N = h.normal;
+    f.t = h.t;
+    f.mat = h.material;
+    f.prim = h.prim;
+    f.front = h.front_face;
+    if (h.material >= 0 && h.material < S.material_count)
+        f.alb = surface_albedo(S, S.materials[h.material], o, unit_dir(d), h);
+}
 
 template <typename R>
 MT_D V3<R> emissive_direct(const DevScene<R> &S, const DevMaterial<R> &mm, V3<R> P, V3<R> N, V3<R> V, int self_prim,
@@ -607,7 +777,12 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
     st[0].d = ray.d;
     st[0].depth = 0;
     st[0].phase = WH_TRACE;
+    st[0].traced = 0;
     sp = 1;
+    // a frame's result, with trace()'s fog when it entered through trace()
+    auto fogged = [&](const WhFrame<R> &fr, V3<R> c) {
+        return (fr.traced && S.fog.density > R(0)) ? fog_apply(S.fog, S.sky, fr.o, fr.d, fr.fog_t, c) : c;
+    };
     int guard = 0;
     while (sp > 0) {
         if (++guard > (1 << 24)) {
@@ -628,17 +803,15 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
             // The hit point and facing use the normalised direction (inside
             // scene_intersect); everything else sees the ray's own direction,
             // as src/render.c:842-863 passes `r` through unchanged.
+            f.traced = 1;
             if (!scene_intersect(S, f.o, f.d, R(1e-4), R(1e30), &h)) {
-                ret = sky_sample(f.d, S.sky);
+                f.fog_t = R(1e30);
+                ret = fogged(f, sky_sample(f.d, S.sky));
                 --sp;
                 continue;
             }
-            f.P = h.point;
-            f.N = h.normal;
-            f.t = h.t;
-            f.mat = h.material;
-            f.prim = h.prim;
-            f.front = h.front_face;
+            f.fog_t = h.t;
+            wh_set_hit(S, f, f.o, f.d, h);
         }
         // fall through: shade the hit
         case WH_HIT: {
@@ -648,11 +821,21 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
                 continue;
             }
             if (f.mat < 0 || f.mat >= S.material_count) {
-                ret = sky_sample(f.d, S.sky);
+                ret = fogged(f, sky_sample(f.d, S.sky));
                 --sp;
                 continue;
             }
-            const DevMaterial<R> &m = S.materials[f.mat];
+            const DevMaterial<R> &m0 = S.materials[f.mat];
+            DevMaterial<R> m_tex;
+            const DevMaterial<R> *mp = &m0;
+            if (m0.texture_kind != 0) {
+                m_tex = m0;
+                m_tex.albedo[0] = f.alb.x;
+                m_tex.albedo[1] = f.alb.y;
+                m_tex.albedo[2] = f.alb.z;
+                mp = &m_tex;
+            }
+            const DevMaterial<R> &m = *mp;
             if (m.is_water) f.N = water_normal(f.P.x, f.P.z, R(0));
             if (dot(f.N, f.d) > R(0)) f.N = neg(f.N);
             V3<R> V = neg(f.d);
@@ -776,12 +959,8 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
                         c.d = rd;
                         c.depth = f.depth + 1;
                         c.phase = WH_HIT;
-                        c.P = h2.point;
-                        c.N = h2.normal;
-                        c.t = h2.t;
-                        c.mat = h2.material;
-                        c.prim = h2.prim;
-                        c.front = h2.front_face;
+                        c.traced = 0;  // trace_hit directly: no fog (src/render.c:786-790)
+                        wh_set_hit(S, c, ro, rd, h2);
                         ++sp;
                         continue;
                     }
@@ -796,7 +975,7 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
                     out = add(out, mat3(m.emissive));
                 if (f.depth == 0 && length_sq(mat3(m.atmosphere_glow)) > R(1e-6))
                     out = add(out, atmosphere_term(m, f.N, V, sun_dir));
-                ret = out;
+                ret = fogged(f, out);
                 --sp;
                 continue;
             }
@@ -808,7 +987,7 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
             V3<R> out = lerp(f.color, surface, m.transparency);
             if (m.pbr && (m.emissive[0] != R(0) || m.emissive[1] != R(0) || m.emissive[2] != R(0)))
                 out = add(out, mat3(m.emissive));
-            ret = out;
+            ret = fogged(f, out);
             --sp;
             continue;
         }

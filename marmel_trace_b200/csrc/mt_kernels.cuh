@@ -15,7 +15,7 @@ namespace mt {
 // row-major order, so a warp covers 32 horizontally adjacent pixels whose
 // primary rays are coherent.
 template <typename R, int MODE>
-__global__ void __launch_bounds__(128) k_render(const DevScene<R> S, const DevCamera<R> cam, int w, int h,
+__global__ void __launch_bounds__(128) k_render(const __grid_constant__ DevScene<R> S, const DevCamera<R> cam, int w, int h,
                                                 int spp_total, int s0, int s1, int depth, int out_kind, void *out)
 {
     int pix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(128) k_render(const DevScene<R> S, const DevCa
 }
 
 template <typename R>
-__global__ void k_intersect(const DevScene<R> S, int n, const double *o, const double *d, double tmin, double tmax,
+__global__ void k_intersect(const __grid_constant__ DevScene<R> S, int n, const double *o, const double *d, double tmin, double tmax,
                             int *prim, double *t, double *normal, int *front, int *mat)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -89,7 +89,7 @@ __global__ void k_intersect(const DevScene<R> S, int n, const double *o, const d
 }
 
 template <typename R>
-__global__ void k_occluded(const DevScene<R> S, int n, const double *o, const double *d, double tmin, double tmax,
+__global__ void k_occluded(const __grid_constant__ DevScene<R> S, int n, const double *o, const double *d, double tmin, double tmax,
                            int *occ)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -100,7 +100,7 @@ __global__ void k_occluded(const DevScene<R> S, int n, const double *o, const do
 }
 
 template <typename R>
-__global__ void k_radiance(const DevScene<R> S, int n, const double *o, const double *d, int depth,
+__global__ void k_radiance(const __grid_constant__ DevScene<R> S, int n, const double *o, const double *d, int depth,
                            const unsigned *seeds, double *out, int mode)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -115,7 +115,7 @@ __global__ void k_radiance(const DevScene<R> S, int n, const double *o, const do
 }
 
 template <typename R>
-__global__ void k_primary(const DevScene<R> S, const DevCamera<R> cam, int w, int h, int spp, int mode, double *out)
+__global__ void k_primary(const __grid_constant__ DevScene<R> S, const DevCamera<R> cam, int w, int h, int spp, int mode, double *out)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long n = (long long)w * h * spp;
@@ -218,7 +218,7 @@ MT_D Ray3<R> adaptive_primary(const DevCamera<R> &cam, int w, int h, int n0, int
 // One pass (adaptive_region, src/render.c:1174-1240). `list` holds the active
 // pixels (count on the device); NULL means every pixel (pass 0).
 template <typename R>
-__global__ void __launch_bounds__(128) k_adaptive_pass(const DevScene<R> S, const DevCamera<R> cam, int w, int h,
+__global__ void __launch_bounds__(128) k_adaptive_pass(const __grid_constant__ DevScene<R> S, const DevCamera<R> cam, int w, int h,
                                                        int n0, int nmax, int batch, int depth, const int *list,
                                                        const int *count, double *sums, int *nsamp)
 {

@@ -64,7 +64,13 @@ template <typename R> struct DevMaterial {
     int32_t is_water;
     int32_t beer_lambert;
     int32_t pbr;
-    int32_t pad;
+    int32_t texture_kind;   // TextureKind (src/material.h:33-42)
+    R texture_scale;        // as given; <= 0 means 1 (texture_scale_or_default)
+    R texture_color_a[3];
+    R texture_color_b[3];
+    const unsigned char *texture_rgb;  // image texture: width x height sRGB RGB bytes, top row first
+    int32_t texture_width;
+    int32_t texture_height;
 };
 
 template <typename R> struct DevSky {
@@ -81,8 +87,25 @@ template <typename R> struct DevSky {
     R cloud_softness;
     R cloud_sharpness;
     R sun_radius;
+    R cloud_thickness;   // > 1e-4: volumetric slab (src/material.c:493-557)
+    R cloud_density;     // <= 0 means 0.08
+    int32_t cloud_steps;
     int32_t cloud_octaves;
     uint32_t seed;
+};
+
+// FogParams (src/material.h:199-209).
+template <typename R> struct DevFog {
+    R density;   // 0: no fog
+    R color[3];
+    R height;
+    R height_falloff;
+    R inscatter_strength;
+    R sun_anisotropy;
+    R noise_scale;
+    R noise_amount;
+    int32_t shadow_steps;  // > 0: marched at bounce 0 with sun shadow rays
+    int32_t pad;
 };
 
 template <typename R> struct DevLight {
@@ -132,6 +155,7 @@ template <typename R> struct DevScene {
     const R *planes;         // point, axis
     const int *plane_prims;  // prim_index of each plane
     const int *tri_prim;     // prim_index of each triangle slot (FP64 path)
+    const R *tri_uv;         // 6 per triangle slot (ua va ub vb uc vc) when some triangle has UVs; NaN first = none
     const int2 *prim_info;   // {code, material} per prim_index
     const DevMaterial<R> *materials;
     int node_count;
@@ -148,6 +172,7 @@ template <typename R> struct DevScene {
     R water_level;
     DevOcean<R> ocean;
     DevSky<R> sky;
+    DevFog<R> fog;
     DevLight<R> lights[kMaxLights];
     unsigned *err;               // device error word
     DevCounters *counters;       // NULL when counting is off

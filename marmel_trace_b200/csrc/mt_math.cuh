@@ -12,6 +12,9 @@
 
 #define MT_HD __host__ __device__ __forceinline__
 #define MT_D __device__ __forceinline__
+// Rare, large paths (textures, fog, volumetric media) stay out of line, so the
+// common path of the kernels that can reach them keeps its registers.
+#define MT_NOINLINE __device__ __noinline__
 
 namespace mt {
 
@@ -39,6 +42,10 @@ MT_D float msin(float x) { return sinf(x); }
 MT_D double msin(double x) { return sin(x); }
 MT_D float mtan(float x) { return tanf(x); }
 MT_D double mtan(double x) { return tan(x); }
+MT_D float matan2(float y, float x) { return atan2f(y, x); }
+MT_D double matan2(double y, double x) { return atan2(y, x); }
+MT_D float masin(float x) { return asinf(x); }
+MT_D double masin(double x) { return asin(x); }
 MT_D bool misfinite(float x) { return isfinite(x); }
 MT_D bool misfinite(double x) { return isfinite(x); }
 MT_D void msincos(float x, float *s, float *c) { sincosf(x, s, c); }

@@ -94,9 +94,67 @@ template <typename R> MT_D R noise_fbm2(R x, R y, int octaves, uint32_t seed)
     return noise_clamp(sum / norm, R(-1), R(1));
 }
 
+template <typename R> MT_D R noise_rand_signed(int x, int y, int z, uint32_t seed)
+{
+    return noise_rand01<R>(x, y, z, seed) * R(2) - R(1);
+}
+
+// noise_perlin3 (src/noise.c:189-246)
+template <typename R> MT_D R noise_perlin3(R x, R y, R z, uint32_t seed)
+{
+    R fx = mfloor(x), fy = mfloor(y), fz = mfloor(z);
+    int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+    R rx = x - fx, ry = y - fy, rz = z - fz;
+    R u = noise_fade(rx), v = noise_fade(ry), w = noise_fade(rz);
+    R dotv[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        int cx = ix + (i & 1), cy = iy + ((i >> 1) & 1), cz = iz + ((i >> 2) & 1);
+        R gx = noise_rand_signed<R>(cx, cy, cz, seed);
+        R gy = noise_rand_signed<R>(cx, cy, cz, seed ^ 0x68bc21ebu);
+        R gz = noise_rand_signed<R>(cx, cy, cz, seed ^ 0x02e5be93u);
+        R len = msqrt(gx * gx + gy * gy + gz * gz);
+        if (len < R(1e-12)) {
+            gx = R(1);
+            gy = R(0);
+            gz = R(0);
+        } else {
+            gx /= len;
+            gy /= len;
+            gz /= len;
+        }
+        R dx = rx - R(i & 1), dy = ry - R((i >> 1) & 1), dz = rz - R((i >> 2) & 1);
+        dotv[i] = gx * dx + gy * dy + gz * dz;
+    }
+    R x00 = noise_lerp(dotv[0], dotv[1], u);
+    R x10 = noise_lerp(dotv[2], dotv[3], u);
+    R x01 = noise_lerp(dotv[4], dotv[5], u);
+    R x11 = noise_lerp(dotv[6], dotv[7], u);
+    R y0 = noise_lerp(x00, x10, v);
+    R y1 = noise_lerp(x01, x11, v);
+    R val = noise_lerp(y0, y1, w);
+    return noise_clamp(val * R(1.1547005383792515), R(-1), R(1));
+}
+
+// noise_fbm3 with lacunarity 2 and gain 0.5, the only values its callers use
+// (src/noise.c:296-317)
+template <typename R> MT_D R noise_fbm3(R x, R y, R z, int octaves, uint32_t seed)
+{
+    int n = octaves <= 0 ? 1 : octaves;
+    R amp = R(1), freq = R(1), sum = R(0), norm = R(0);
+    for (int i = 0; i < n; ++i) {
+        sum += amp * noise_perlin3(x * freq, y * freq, z * freq, seed);
+        norm += amp;
+        amp *= R(0.5);
+        freq *= R(2);
+    }
+    if (norm <= R(0)) return R(0);
+    return noise_clamp(sum / norm, R(-1), R(1));
+}
+
 // ------------------------------------------------------------------
-// Sky (sky_sample, src/material.c:473-600,956: gradient, sun glow, planar
-// clouds; the volumetric/star/nebula/galaxy branches are rejected on upload)
+// Sky (sky_sample, src/material.c:473-600,956: gradient, sun glow, volumetric
+// or planar clouds; the star / nebula / galaxy terms are rejected on upload)
 // ------------------------------------------------------------------
 template <typename R> MT_D R smoothstep(R e0, R e1, R x)
 {
@@ -112,6 +170,138 @@ template <typename R> MT_D R pow_nonneg(R base, R e)
     return mpow(base, e);
 }
 
+template <typename R> MT_D void basis(V3<R> n, V3<R> *t, V3<R> *b);
+
+// eval_cloud_density_at (src/material.c:376-408)
+template <typename R> MT_D R cloud_density_at(const DevSky<R> &sky, V3<R> p)
+{
+    if (sky.cloud_thickness <= R(1e-4)) return R(0);
+    R y_bot = sky.cloud_height;
+    R y_top = y_bot + sky.cloud_thickness;
+    if (p.y < y_bot || p.y > y_top) return R(0);
+    R h_rel = (p.y - y_bot) / sky.cloud_thickness;
+    R vert_profile = smoothstep(R(0), R(0.12), h_rel) * smoothstep(R(1), R(0.60), h_rel);
+    if (vert_profile <= R(0)) return R(0);
+    int octaves = sky.cloud_octaves;
+    if (octaves < 1) octaves = 1;
+    if (octaves > 6) octaves = 6;
+    R sx = p.x * sky.cloud_scale;
+    R sy = (p.y - y_bot) * (sky.cloud_scale * R(1.5));
+    R sz = p.z * sky.cloud_scale;
+    R raw = noise_fbm3(sx, sy, sz, octaves, sky.seed);
+    R d0 = mat_clamp01(R(0.5) * (raw + R(1)));
+    R d = d0 * vert_profile;
+    R a = sky.cloud_coverage - sky.cloud_softness;
+    R b = sky.cloud_coverage + sky.cloud_softness;
+    R alpha = smoothstep(a, b, d);
+    if (alpha <= R(0)) return R(0);
+    alpha = pow_nonneg(alpha, sky.cloud_sharpness);
+    R mult = (sky.cloud_density > R(0)) ? sky.cloud_density : R(0.08);
+    return alpha * mult;
+}
+
+// sky_cloud_transmittance (src/material.c:410-466): grey transmittance of
+// the cloud slab from pos along dir, with the crepuscular shaft modulation.
+template <typename R> MT_NOINLINE R cloud_transmittance_march(const DevSky<R> &sky, V3<R> pos, V3<R> dir)
+{
+    if (dir.y <= R(1e-4)) return R(1);
+    R y_bot = sky.cloud_height;
+    R y_top = y_bot + sky.cloud_thickness;
+    R t0 = (y_bot - pos.y) / dir.y;
+    R t1 = (y_top - pos.y) / dir.y;
+    R t_start = (t0 > R(0)) ? t0 : R(0);
+    R t_end = t1;
+    if (t_end <= t_start) return R(1);
+    R slab_dist = t_end - t_start;
+    if (slab_dist > R(3000)) slab_dist = R(3000);
+    int steps = sky.cloud_steps / 2;
+    if (steps < 4) steps = 4;
+    if (steps > 16) steps = 16;
+    R dt = slab_dist / R(steps);
+    R tau = R(0);
+    for (int i = 0; i < steps; ++i) {
+        R t = t_start + (R(i) + R(0.5)) * dt;
+        V3<R> p = add(pos, scale(dir, t));
+        R rho = cloud_density_at(sky, p);
+        tau += rho * dt;
+        if (tau > R(15)) {
+            tau = R(15);
+            break;
+        }
+    }
+    R T = mexp(-tau);
+    V3<R> u_dir, v_dir;
+    basis(mat3(sky.sun_dir), &u_dir, &v_dir);
+    R u = dot(pos, u_dir);
+    R v = dot(pos, v_dir);
+    const R shaft_scale = R(0.22);
+    R raw_shaft = noise_fbm2(u * shaft_scale, v * shaft_scale, 3, sky.seed ^ 0x9E3779B9u);
+    R shaft = smoothstep(R(-0.25), R(0.35), raw_shaft);
+    R beam_factor = R(0.12) + R(0.88) * shaft;
+    T *= beam_factor;
+    return T;
+}
+
+template <typename R> MT_D R cloud_transmittance(const DevSky<R> &sky, V3<R> pos, V3<R> dir)
+{
+    if (sky.cloud_thickness <= R(1e-4)) return R(1);
+    return cloud_transmittance_march(sky, pos, dir);
+}
+
+// The volumetric slab of sky_sample (src/material.c:493-556): the cloud march
+// blended over `base`.
+template <typename R> MT_NOINLINE V3<R> sky_clouds_volumetric(V3<R> dir, const DevSky<R> &sky, V3<R> base, R cos_sun)
+{
+    if (!(dir.y > R(0.01))) return base;
+    const V3<R> sun_color = mat3(sky.sun_color);
+    R y_bot = sky.cloud_height;
+    R y_top = y_bot + sky.cloud_thickness;
+    R t0 = y_bot / dir.y;
+    R t1 = y_top / dir.y;
+    R slab_dist = t1 - t0;
+    if (slab_dist > R(3500)) slab_dist = R(3500);
+    int steps = sky.cloud_steps;
+    if (steps < 4) steps = 4;
+    if (steps > 64) steps = 64;
+    R dt = slab_dist / R(steps);
+    V3<R> cloud_albedo = v3(R(0.96), R(0.97), R(0.98));
+    V3<R> sky_ambient = lerp(mat3(sky.horizon_color), mat3(sky.zenith_color), R(0.55));
+    V3<R> ambient_col = scale(mul(cloud_albedo, sky_ambient), R(0.60));
+    R lit = (cos_sun > R(0)) ? cos_sun : R(0);
+    R silver = R(0.50) * pow_nonneg(mfmax(R(0), cos_sun), R(14));
+    R T_acc = R(1);
+    V3<R> cloud_inscatter = v3(R(0), R(0), R(0));
+    V3<R> sun_dir = mat3(sky.sun_dir);
+    for (int i = 0; i < steps; ++i) {
+        R tt = t0 + (R(i) + R(0.5)) * dt;
+        V3<R> p = scale(dir, tt);
+        R rho = cloud_density_at(sky, p);
+        if (rho <= R(1e-5)) continue;
+        R sun_tau = R(0);
+        if (sun_dir.y > R(0.02)) {
+            R t_sun_top = (y_top - p.y) / sun_dir.y;
+            if (t_sun_top > R(0)) {
+                R dt_sun = t_sun_top / R(4);
+                for (int k = 0; k < 4; ++k) {
+                    V3<R> p_sun = add(p, scale(sun_dir, (R(k) + R(0.5)) * dt_sun));
+                    sun_tau += cloud_density_at(sky, p_sun) * dt_sun;
+                }
+            }
+        }
+        R T_sun = mexp(-sun_tau) + R(0.25) * mexp(-sun_tau * R(0.30));
+        V3<R> sun_lit = scale(sun_color, (R(0.35) * lit + silver) * T_sun);
+        V3<R> step_col = add(ambient_col, mul(cloud_albedo, sun_lit));
+        R step_tau = rho * dt;
+        R step_T = mexp(-step_tau);
+        cloud_inscatter = add(cloud_inscatter, scale(step_col, (R(1) - step_T) * T_acc));
+        T_acc *= step_T;
+        if (T_acc < R(0.005)) break;
+    }
+    R horizon_fade = smoothstep(R(0.01), R(0.08), dir.y);
+    V3<R> combined = add(scale(base, T_acc), cloud_inscatter);
+    return lerp(base, combined, horizon_fade);
+}
+
 template <typename R> MT_D V3<R> sky_sample(V3<R> dir, const DevSky<R> &sky)
 {
     R h = mat_clamp01(dir.y);
@@ -123,7 +313,10 @@ template <typename R> MT_D V3<R> sky_sample(V3<R> dir, const DevSky<R> &sky)
         R glow = pow_nonneg(cos_sun, sky.sun_glow_exponent) * sky.sun_glow_strength;
         base = add(base, scale(sun_color, glow));
     }
-    if (dir.y > R(0.03)) {
+    if (sky.cloud_thickness > R(1e-4)) {
+        base = sky_clouds_volumetric(dir, sky, base, cos_sun);
+    } else if (dir.y > R(0.03)) {
+        // planar clouds (src/material.c:557-595)
         R tt = sky.cloud_height / dir.y;
         R px = dir.x * tt;
         R pz = dir.z * tt;
@@ -148,6 +341,241 @@ template <typename R> MT_D V3<R> sky_sample(V3<R> dir, const DevSky<R> &sky)
     if (!(base.y >= R(0))) base.y = R(0);
     if (!(base.z >= R(0))) base.z = R(0);
     return base;
+}
+
+// ------------------------------------------------------------------
+// Fog (fog_segment / fog_apply, src/material.c:963-1053)
+// ------------------------------------------------------------------
+// The fBm turbulence factor of fog density at p (src/material.c:1000-1011,
+// src/pathtrace.c:674-684).
+template <typename R> MT_D R fog_noise_mod(const DevFog<R> &fog, V3<R> p)
+{
+    R n = noise_fbm3(p.x * fog.noise_scale, p.y * fog.noise_scale, p.z * fog.noise_scale, 3, 1337u);
+    R turb = R(0.5) * (n + R(1));
+    if (turb < R(0)) turb = R(0);
+    if (turb > R(1)) turb = R(1);
+    return (R(1) - fog.noise_amount) + fog.noise_amount * turb * R(2);
+}
+
+// Henyey-Greenstein phase toward the sun with g clamped to +-0.95.
+template <typename R> MT_D R fog_phase_hg(const DevFog<R> &fog, V3<R> dir, V3<R> sun_dir)
+{
+    R g = fog.sun_anisotropy;
+    if (g < R(-0.95)) g = R(-0.95);
+    if (g > R(0.95)) g = R(0.95);
+    R cos_theta = dot(dir, sun_dir);
+    R denom = R(1) + g * g - R(2) * g * cos_theta;
+    if (denom < R(1e-4)) denom = R(1e-4);
+    return (R(1) - g * g) / (denom * msqrt(denom));
+}
+
+template <typename R>
+MT_NOINLINE void fog_segment(const DevFog<R> &fog, const DevSky<R> &sky, V3<R> o, V3<R> d, R dist, R *transmittance,
+                             V3<R> *inscatter)
+{
+    *transmittance = R(1);
+    *inscatter = v3(R(0), R(0), R(0));
+    if (fog.density <= R(0) || dist <= R(1e-7)) return;
+    R rho0 = fog.density;
+    R lambda = (fog.height_falloff > R(0)) ? fog.height_falloff : R(0);
+    R y0 = o.y - fog.height;
+    R dy = d.y;
+    R tau = R(0);
+    bool is_sky = dist >= R(1e20);
+    if (lambda <= R(1e-6)) {
+        tau = is_sky ? R(1e6) : (rho0 * dist);
+    } else {
+        R base_density = rho0 * mexp(-lambda * y0);
+        if (is_sky) {
+            tau = (dy > R(1e-5)) ? base_density / (lambda * dy) : R(1e6);
+        } else if (mfabs(dy) < R(1e-5)) {
+            tau = base_density * dist;
+        } else {
+            R term = (R(1) - mexp(-lambda * dy * dist)) / (lambda * dy);
+            tau = base_density * term;
+        }
+    }
+    if (tau < R(0)) tau = R(0);
+    if (fog.noise_amount > R(1e-4) && fog.noise_scale > R(1e-4)) {
+        R eval_dist = is_sky ? R(20) : (dist > R(50) ? R(50) : dist * R(0.5));
+        tau *= fog_noise_mod(fog, add(o, scale(d, eval_dist)));
+    }
+    R T = mexp(-tau);
+    if (T < R(0)) T = R(0);
+    if (T > R(1)) T = R(1);
+    V3<R> inscatter_col = mat3(fog.color);
+    if (fog.inscatter_strength > R(0)) {
+        R phase = fog_phase_hg(fog, d, mat3(sky.sun_dir));
+        inscatter_col = add(inscatter_col, scale(mat3(sky.sun_color), phase * fog.inscatter_strength));
+    }
+    *transmittance = T;
+    *inscatter = scale(inscatter_col, R(1) - T);
+}
+
+template <typename R>
+MT_D V3<R> fog_apply(const DevFog<R> &fog, const DevSky<R> &sky, V3<R> o, V3<R> d, R dist, V3<R> surface)
+{
+    if (fog.density <= R(0)) return surface;
+    R T;
+    V3<R> inscatter;
+    fog_segment(fog, sky, o, d, dist, &T, &inscatter);
+    return add(scale(surface, T), inscatter);
+}
+
+// ------------------------------------------------------------------
+// Textures (texture_albedo_uv, src/texture.c:269-327)
+// ------------------------------------------------------------------
+template <typename R> MT_D R texture_scale_or_default(const DevMaterial<R> &m)
+{
+    R s = m.texture_scale;
+    return (s > R(0)) ? s : R(1);
+}
+
+template <typename R> MT_D V3<R> texture_planet_earth(const DevMaterial<R> &m, V3<R> p)
+{
+    R s = R(1) / texture_scale_or_default(m);
+    V3<R> q = scale(p, s);
+    R elev = noise_fbm3(q.x * R(1.6), q.y * R(1.6), q.z * R(1.6), 7, 42u);
+    V3<R> surf;
+    if (elev < R(0)) {
+        R t = mat_clamp01((elev + R(0.25)) / R(0.25));
+        surf = lerp(v3(R(0.02), R(0.05), R(0.20)), v3(R(0.04), R(0.18), R(0.35)), t);
+    } else {
+        R t = mat_clamp01(elev / R(0.45));
+        const V3<R> land_low = v3(R(0.12), R(0.22), R(0.08)), land_mid = v3(R(0.26), R(0.24), R(0.14));
+        const V3<R> land_arid = v3(R(0.42), R(0.35), R(0.20)), snow = v3(R(0.88), R(0.90), R(0.94));
+        if (t < R(0.35)) surf = lerp(land_low, land_mid, t / R(0.35));
+        else if (t < R(0.70)) surf = lerp(land_mid, land_arid, (t - R(0.35)) / R(0.35));
+        else surf = lerp(land_arid, snow, (t - R(0.70)) / R(0.30));
+    }
+    R warp = noise_fbm3(q.x * R(2.2) + R(7.3), q.y * R(2.2) + R(7.3), q.z * R(2.2) + R(7.3), 4, 101u);
+    R c_noise = noise_fbm3(q.x * R(2.6) + warp * R(0.4), q.y * R(2.6) + warp * R(0.4), q.z * R(2.6) + warp * R(0.4),
+                           6, 999u);
+    R c_cov = smoothstep(R(0.02), R(0.38), c_noise);
+    V3<R> result = lerp(surf, v3(R(0.92), R(0.94), R(0.96)), c_cov * R(0.88));
+    return mul(mat3(m.albedo), result);
+}
+
+template <typename R> MT_D V3<R> texture_planet_moon(const DevMaterial<R> &m, V3<R> p)
+{
+    R s = R(1) / texture_scale_or_default(m);
+    V3<R> q = scale(p, s);
+    R maria = noise_fbm3(q.x * R(1.2), q.y * R(1.2), q.z * R(1.2), 5, 77u);
+    R crater = noise_fbm3(q.x * R(4.5), q.y * R(4.5), q.z * R(4.5), 6, 555u);
+    R micro = noise_fbm3(q.x * R(16), q.y * R(16), q.z * R(16), 4, 888u);
+    R m_blend = mat_clamp01((maria + R(0.12)) / R(0.38));
+    V3<R> base = lerp(v3(R(0.075), R(0.075), R(0.072)), v3(R(0.165), R(0.160), R(0.150)), m_blend);
+    R detail = R(1) + R(0.32) * crater + R(0.14) * micro;
+    V3<R> result = scale(base, detail);
+    if (crater > R(0.40)) {
+        R ray_t = mat_clamp01((crater - R(0.40)) / R(0.25));
+        result = lerp(result, v3(R(0.250), R(0.245), R(0.235)), ray_t * R(0.75));
+    }
+    return mul(mat3(m.albedo), result);
+}
+
+// Exact sRGB byte to linear (src/texture.c:57-61).
+template <typename R> MT_D R srgb_to_linear(unsigned char byte)
+{
+    R c = R(byte) / R(255);
+    return (c <= R(0.04045)) ? (c / R(12.92)) : mpow((c + R(0.055)) / R(1.055), R(2.4));
+}
+
+// texture_image_sample (src/texture.c:212-263): wrapped bilinear lookup.
+template <typename R> MT_D V3<R> texture_image_sample(const DevMaterial<R> &m, R u, R v)
+{
+    const int w = m.texture_width, h = m.texture_height;
+    u = u - mfloor(u);
+    v = v - mfloor(v);
+    R px = u * R(w) - R(0.5);
+    R py = (R(1) - v) * R(h) - R(0.5);
+    int x0 = (int)mfloor(px), y0 = (int)mfloor(py);
+    int x1 = x0 + 1, y1 = y0 + 1;
+    R fx = px - R(x0), fy = py - R(y0);
+    x0 = ((x0 % w) + w) % w;
+    x1 = ((x1 % w) + w) % w;
+    y0 = ((y0 % h) + h) % h;
+    y1 = ((y1 % h) + h) % h;
+    const unsigned char *p00 = m.texture_rgb + ((size_t)y0 * w + x0) * 3;
+    const unsigned char *p10 = m.texture_rgb + ((size_t)y0 * w + x1) * 3;
+    const unsigned char *p01 = m.texture_rgb + ((size_t)y1 * w + x0) * 3;
+    const unsigned char *p11 = m.texture_rgb + ((size_t)y1 * w + x1) * 3;
+    R w00 = (R(1) - fx) * (R(1) - fy);
+    R w10 = fx * (R(1) - fy);
+    R w01 = (R(1) - fx) * fy;
+    R w11 = fx * fy;
+    R c[3];
+    for (int k = 0; k < 3; ++k)
+        c[k] = w00 * srgb_to_linear<R>(p00[k]) + w10 * srgb_to_linear<R>(p10[k]) + w01 * srgb_to_linear<R>(p01[k]) +
+               w11 * srgb_to_linear<R>(p11[k]);
+    return v3(c[0], c[1], c[2]);
+}
+
+// Parity bit of floor(x) (as the reference's long long cast, & 1).
+template <typename R> MT_D int floor_parity(R x) { return (int)(((long long)mfloor(x)) & 1); }
+
+// Albedo of material m at world point p with hit (u, v).
+template <typename R> MT_NOINLINE V3<R> texture_albedo_uv(const DevMaterial<R> &m, V3<R> p, R u, R v)
+{
+    switch (m.texture_kind) {
+    case 1: {  // TEXTURE_CHECKER
+        R inv_scale = R(1) / texture_scale_or_default(m);
+        int parity = (floor_parity(p.x * inv_scale) + floor_parity(p.y * inv_scale) + floor_parity(p.z * inv_scale)) & 1;
+        return mul(mat3(m.albedo), parity ? mat3(m.texture_color_a) : mat3(m.texture_color_b));
+    }
+    case 2: {  // TEXTURE_STRIPES
+        R s = texture_scale_or_default(m);
+        R wave = R(0.5) * (R(1) + msin(p.y * s * (R(2) * R(3.14159265358979323846))));
+        return mul(mat3(m.albedo), (wave >= R(0.5)) ? mat3(m.texture_color_a) : mat3(m.texture_color_b));
+    }
+    case 3:
+        return texture_planet_earth(m, p);
+    case 4:
+        return texture_planet_moon(m, p);
+    case 5: {  // TEXTURE_NOISE (src/texture.c:154-162)
+        R s = R(1) / texture_scale_or_default(m);
+        V3<R> q = scale(p, s);
+        R n = noise_fbm3(q.x, q.y, q.z, 6, 1337u);
+        R t = mat_clamp01(R(0.5) * (n + R(1)));
+        return mul(mat3(m.albedo), lerp(mat3(m.texture_color_a), mat3(m.texture_color_b), t));
+    }
+    case 7: {  // TEXTURE_UV_CHECKER
+        R s = texture_scale_or_default(m);
+        int parity = (floor_parity(u * s) + floor_parity(v * s)) & 1;
+        return mul(mat3(m.albedo), parity ? mat3(m.texture_color_a) : mat3(m.texture_color_b));
+    }
+    case 6:  // TEXTURE_IMAGE
+        if (m.texture_rgb) {
+            R s = (m.texture_scale > R(0)) ? m.texture_scale : R(1);
+            return mul(mat3(m.albedo), texture_image_sample(m, u * s, v * s));
+        }
+        return mat3(m.albedo);
+    default:
+        return mat3(m.albedo);
+    }
+}
+
+// True for the kinds whose albedo reads the hit's (u, v).
+MT_HD bool texture_uses_uv(int kind) { return kind == 6 || kind == 7; }
+
+// The albedo a surface hit shades with: texture_albedo_uv at the hit point
+// and the hit's (u, v) (src/pathtrace.c:903-905, src/render.c:620-621).
+// o, du: the ray of the hit with its unit direction.
+template <typename R>
+MT_D V3<R> surface_albedo(const DevScene<R> &S, const DevMaterial<R> &m, V3<R> o, V3<R> du, const SurfaceHit<R> &h)
+{
+    if (m.texture_kind == 0) return mat3(m.albedo);
+    R u = R(0), v = R(0);
+    if (texture_uses_uv(m.texture_kind)) {
+        Hit<R> th;
+        th.t = h.t;
+        th.u = h.bu;
+        th.v = h.bv;
+        th.prim = h.prim;
+        th.code = h.code;
+        hit_uv(S, o, du, th, &u, &v);
+    }
+    return texture_albedo_uv(m, h.point, u, v);
 }
 
 // sky_basis / sampling_basis: least-aligned world axis, Gram-Schmidt

@@ -133,7 +133,7 @@ MT_D int warp_append(int *counter, bool want)
 // generate: primary rays of a batch (pt_render_pixel, src/pathtrace.c:1053-1086)
 // ------------------------------------------------------------------
 template <typename R>
-__global__ void k_wf_generate(const DevScene<R> S, const WfParams<R> *P, int batch, int batch_spp, int n_paths,
+__global__ void k_wf_generate(const __grid_constant__ DevScene<R> S, const WfParams<R> *P, int batch, int batch_spp, int n_paths,
                               WfPath<R> *paths, WfRay<R> *rays, WfCounters *C, R *nee, WfAdj<R> A)
 {
     const WfParams<R> p = *P;
@@ -186,7 +186,7 @@ __global__ void k_wf_generate(const DevScene<R> S, const WfParams<R> *P, int bat
 // extend: nearest hit (scene_intersect, src/scene.c:767 -> src/bvh.c:557)
 // ------------------------------------------------------------------
 template <typename R, int W>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend(const DevScene<R> S, const WfRay<R> *rays, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays, const WfCounters *C,
                                                    int which, WfHit<R> *hits)
 {
     const int n = C->ray_count[which];
@@ -255,7 +255,7 @@ MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> 
 // When the bounce's extend results were sorted by material (C->sorted), the
 // kernel reads the sorted copies instead.
 template <typename R, bool ADJ>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
                                                   WfCounters *C, int which, int b, int max_depth, WfPath<R> *paths,
                                                   R *nee, WfRay<R> *rays_out, WfShadow<R> *sq, WfAdj<R> A,
                                                   const WfRay<R> *sorted_rays, const WfHit<R> *sorted_hits)
@@ -283,6 +283,10 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
         V3<R> next_o = zero, next_d = zero;
         int mat = -1, vflags = 0;
         bool shade_hit = false, do_sun = false, cont = false;
+        // the material the hit shades with: a local copy with the texture's
+        // albedo (src/pathtrace.c:903-905), else the scene's
+        DevMaterial<R> m_tex;
+        const DevMaterial<R> *msh = S.materials;
         if (active) {
             const WfRay<R> r = rays_in[q];
             const WfHit<R> hh = hits[q];
@@ -307,15 +311,24 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
             const V3<R> ro = v3(r.o[0], r.o[1], r.o[2]);
             const V3<R> d = v3(r.d[0], r.d[1], r.d[2]);
             if (hh.prim < 0) {
-                // escaped: medium fallback depth then the sky (src/pathtrace.c:837-857)
+                // escaped: medium fallback depth then the sky, through the fog
+                // (src/pathtrace.c:837-857)
                 if (st.medium >= 0) {
                     const V3<R> beta_in = throughput;
-                    pt_apply_medium(S.materials[st.medium], R(5.0), &throughput, &radiance);
+                    pt_water_segment(S, st.medium, ro, d, R(5.0), st.seed_key, b, &throughput, &radiance);
                     if constexpr (ADJ)
                         medium_grad(ctx, S.materials[st.medium], st.medium, R(5.0), beta_in, sub(Lp, radiance), adj);
                     st.medium = -1;
                 }
-                radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
+                V3<R> sky_col = sky_sample(d, S.sky);
+                if (S.fog.density > R(0)) {
+                    R T;
+                    V3<R> ins;
+                    if (b == 0) pt_fog_segment(S, ro, d, R(1e30), st.seed_key, b, &T, &ins);
+                    else fog_segment(S.fog, S.sky, ro, d, R(1e30), &T, &ins);
+                    sky_col = add(scale(sky_col, T), ins);
+                }
+                radiance = add(radiance, mul(throughput, sky_col));
                 if constexpr (ADJ) sky_sun_grad(ctx, d, S.sky, mul(adj, throughput));
             } else {
                 Hit<R> th;
@@ -328,15 +341,31 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
                 finish_hit(S, ro, unit_dir(d), th, &h);
                 if (st.medium >= 0) {
                     const V3<R> beta_in = throughput;
-                    pt_apply_medium(S.materials[st.medium], h.t, &throughput, &radiance);
+                    pt_water_segment(S, st.medium, ro, d, h.t, st.seed_key, b, &throughput, &radiance);
                     if constexpr (ADJ)
                         medium_grad(ctx, S.materials[st.medium], st.medium, h.t, beta_in, sub(Lp, radiance), adj);
+                } else if (S.fog.density > R(0)) {
+                    R T;
+                    V3<R> ins;
+                    if (b == 0) pt_fog_segment(S, ro, d, h.t, st.seed_key, b, &T, &ins);
+                    else fog_segment(S.fog, S.sky, ro, d, h.t, &T, &ins);
+                    radiance = add(radiance, mul(throughput, ins));
+                    throughput = scale(throughput, T);
                 }
                 if (h.material < 0 || h.material >= S.material_count) {
                     radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
                     if constexpr (ADJ) sky_sun_grad(ctx, d, S.sky, mul(adj, throughput));
                 } else {
                     const DevMaterial<R> &m = S.materials[h.material];
+                    msh = S.materials + h.material;
+                    if (m.texture_kind != 0) {
+                        m_tex = m;
+                        const V3<R> a = surface_albedo(S, m, ro, unit_dir(d), h);
+                        m_tex.albedo[0] = a.x;
+                        m_tex.albedo[1] = a.y;
+                        m_tex.albedo[2] = a.z;
+                        msh = &m_tex;
+                    }
                     P = h.point;
                     N = h.normal;
                     if (m.is_water) {
@@ -371,9 +400,9 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
                         int refracted = 0, sampled_specular = 0;
                         bool ok;
                         if (m.pbr)
-                            ok = pt_sample_pbr(m, N, d, V, u1, u2, u_lobe, &wi, &w, &sampled_specular);
+                            ok = pt_sample_pbr(*msh, N, d, V, u1, u2, u_lobe, &wi, &w, &sampled_specular);
                         else
-                            ok = pt_sample_legacy(m, N, d, V, h.front_face, u1, u2, u_lobe, u_glass, &wi, &w,
+                            ok = pt_sample_legacy(*msh, N, d, V, h.front_face, u1, u2, u_lobe, u_glass, &wi, &w,
                                                   &refracted, &sampled_specular);
                         if (ok) {
                             st.last_specular = sampled_specular;
@@ -429,7 +458,7 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
                                 so = add(P, scale(N, R(1e-3)));
                                 R lt_t;
                                 if (light_sphere_t(S, lt.prim, so, wi, R(1e-3), R(1e30), &lt_t)) {
-                                    V3<R> lit = shade(S.materials[mat], N, wi, V, mat3(lt.emissive));
+                                    V3<R> lit = shade(*msh, N, wi, V, mat3(lt.emissive));
                                     contrib = mul(beta, scale(lit, Omega));
                                     tmax = lt_t - R(1e-3);
                                     want = true;
@@ -453,7 +482,7 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const DevScene<R> S, c
                     so = add(P, scale(N, R(1e-3)));
                     R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
                     R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
-                    V3<R> lit = shade(S.materials[mat], N, L, V, mat3(S.sky.sun_color));
+                    V3<R> lit = shade(*msh, N, L, V, mat3(S.sky.sun_color));
                     contrib = mul(beta, scale(lit, Omega));
                     want = true;
                 }
@@ -557,7 +586,7 @@ MT_D int warp_add_by_key(int *counters, int key, bool want)
 }
 
 template <typename R>
-__global__ void k_wf_sort_count(const DevScene<R> S, WfCounters *C, int which, const WfRay<R> *rays,
+__global__ void k_wf_sort_count(const __grid_constant__ DevScene<R> S, WfCounters *C, int which, const WfRay<R> *rays,
                                 const WfHit<R> *hits, int *keys, int *buckets, int threshold)
 {
     const int n = C->ray_count[which];
@@ -728,7 +757,7 @@ MT_D void shadow_result(const WfShadow<R> &s, bool occ, V3<R> atten, const Absor
 template <typename R, bool ADJ, int W, bool PASS>
 // (binary tree: at most 72 registers, so 7 blocks of 128 fit an SM; the
 // pass-through instantiation would otherwise take 80 and run 6)
-__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? 7 : 1) k_wf_shadow(const DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? 7 : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
                                                    R *nee, R *att, int *occ_cache, int wh, int b, const int *walk)
 {
     const int n = walk ? C->walk_count : C->shadow_count;
@@ -755,6 +784,8 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? 7 : 1) k_wf_shadow(const
             else
                 occ = scene_any<R, W>(S, ray_pre(o, unit_dir(d)), R(1e-3), s.tmax);
         }
+        // the sun through volumetric clouds (pt_nee_sun, src/pathtrace.c:545-546)
+        if (!occ && s.li == kMaxLights) atten = scale(atten, cloud_transmittance(S.sky, o, d));
         shadow_result<R, ADJ>(s, occ, atten, ab, nee, att);
     }
 }
@@ -762,7 +793,7 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? 7 : 1) k_wf_shadow(const
 // First pass of bounce 0 (scenes without pass-through materials): the cached
 // occluder of every connection; misses go to `walk` (warp-aggregated appends).
 template <typename R, bool ADJ>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const DevScene<R> S, const WfShadow<R> *sq,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq,
                                                          WfCounters *C, R *nee, R *att, int *occ_cache, int wh,
                                                          int b, int *walk)
 {
@@ -827,7 +858,7 @@ MT_D int fetch_round(int *counter, int n, bool idle, bool busy_lane, bool *more)
 }
 
 template <typename R, int W>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend_dyn(const DevScene<R> S, const WfRay<R> *rays, WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend_dyn(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays, WfCounters *C,
                                                        int which, WfHit<R> *hits)
 {
     const int n = C->ray_count[which];
@@ -866,7 +897,7 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend_dyn(const DevScene<R>
 // Shadow rays of a scene without pass-through materials: a pure any-hit
 // query per connection (see k_wf_shadow).
 template <typename R, bool ADJ, int W>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_dyn(const DevScene<R> S, const WfShadow<R> *sq, WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_dyn(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, WfCounters *C,
                                                        R *nee, R *att)
 {
     const int n = C->shadow_count;
@@ -888,17 +919,14 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_dyn(const DevScene<R>
         if (q >= 0) {
             if (tv.node == kEmpty || !trav_step<R, true, W>(S, tv, stk, stride, &unused, cnt)) {
                 const WfShadow<R> &s = sq[q];
-                const bool lit = !tv.found;
-                const size_t at = ((size_t)s.slot * kNeeSlots + s.li) * 3;
-                nee[at] = lit ? s.contrib[0] : R(0);
-                nee[at + 1] = lit ? s.contrib[1] : R(0);
-                nee[at + 2] = lit ? s.contrib[2] : R(0);
-                if constexpr (ADJ) {
-                    R *rec = att + ((size_t)s.slot * kNeeSlots + s.li) * kAttStride;
-                    for (int k = 0; k < kAttStride; ++k) rec[k] = R(0);
-                    if (lit) rec[0] = rec[1] = rec[2] = R(1);
-                    rec[5] = rec[6] = R(-1);
-                }
+                V3<R> atten = v3(R(1), R(1), R(1));
+                if (!tv.found && s.li == kMaxLights)
+                    atten = scale(atten, cloud_transmittance(S.sky, v3(s.o[0], s.o[1], s.o[2]),
+                                                             v3(s.d[0], s.d[1], s.d[2])));
+                AbsorbPath<R> ab;
+                ab.mat[0] = ab.mat[1] = -1;
+                ab.dist[0] = ab.dist[1] = R(0);
+                shadow_result<R, ADJ>(s, tv.found, atten, ab, nee, att);
                 q = -1;
             }
         }
@@ -912,7 +940,7 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_dyn(const DevScene<R>
 // src/pathtrace.c:1020-1027) and the per-pixel sum in sample order
 // ------------------------------------------------------------------
 template <typename R>
-__global__ void k_wf_finalize(const DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, R *sample_buf)
+__global__ void k_wf_finalize(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, R *sample_buf)
 {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_paths; q += gridDim.x * blockDim.x) {
         const WfPath<R> st = paths[q];
@@ -931,7 +959,7 @@ __global__ void k_wf_finalize(const DevScene<R> S, int n_paths, const WfPath<R> 
 // Adjoint replay: the vertex each path still holds (its last) takes its
 // gradient terms against the radiance the path ends with.
 template <typename R>
-__global__ void k_wf_finalize_adj(const DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
+__global__ void k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
 {
     __shared__ float adj_g[kAdjMaxParams];
     const AdjCtx ctx = make_adj_ctx(adj_g, S.material_count);

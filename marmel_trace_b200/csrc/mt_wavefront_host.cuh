@@ -262,6 +262,9 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
     const size_t smem_w = W == 2 ? smem : (size_t)S.wide_stack_depth * block * sizeof(int);
     const int Ws = S.has_passthrough ? 2 : W;
     const size_t smem_s = Ws == 2 ? smem : smem_w;
+    // marched media (fog or water with fog.shadow_steps > 0) cast shadow
+    // segments from the shade stage: it then needs the binary-tree stack
+    const size_t smem_shade = S.fog.shadow_steps > 0 ? smem : 0;
     int ev = 0;
     auto tic = [&]() {
         if (prof) cudaEventRecord(st->kev[ev & 63], s);
@@ -311,10 +314,10 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             }
             tic();
             if (replay) {
-                k_wf_shade<R, true><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
-                                                        rays[which ^ 1], sq, A, nullptr, nullptr);
+                k_wf_shade<R, true><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
+                                                                 rays[which ^ 1], sq, A, nullptr, nullptr);
             } else {
-                k_wf_shade<R, false><<<g, block, 0, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
+                k_wf_shade<R, false><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
                                                          rays[which ^ 1], sq, none,
                                                          sort ? (const WfRay<R> *)st->sorted_rays : nullptr,
                                                          (const WfHit<R> *)st->sorted_hits);

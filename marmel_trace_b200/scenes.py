@@ -29,8 +29,15 @@ from .api import SceneDesc, default_sky, normalize
 
 def material(albedo=(0.0, 0.0, 0.0), specular=(0.0, 0.0, 0.0), shininess=0.0, reflectivity=0.0, transparency=0.0,
              ior=1.0, absorption=(0.0, 0.0, 0.0), deep_color=(0.0, 0.0, 0.0), metallic=0.0, roughness=0.0,
-             emissive=(0.0, 0.0, 0.0), pbr=0, is_water=0, beer_lambert=0) -> np.ndarray:
+             emissive=(0.0, 0.0, 0.0), pbr=0, is_water=0, beer_lambert=0, texture_kind=0, texture_scale=1.0,
+             texture_color_a=(1.0, 1.0, 1.0), texture_color_b=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """One material row; the texture fields default as material_texture_defaults
+    does (src/material.h:48-51)."""
     m = np.zeros(1, MATERIAL_DTYPE)
+    m["texture_kind"] = texture_kind
+    m["texture_scale"] = texture_scale
+    m["texture_color_a"] = texture_color_a
+    m["texture_color_b"] = texture_color_b
     m["albedo"] = albedo
     m["specular"] = specular
     m["shininess"] = shininess
@@ -314,6 +321,78 @@ def water_scene(seed: int = 6, n_spheres: int = 16) -> SceneDesc:
     set_sphere(prims[3 + n_spheres], (2.0, 4.0, -1.0), 0.6, 2)
     return SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=default_sky(),
                      camera=dict(eye=(0.0, 5.0, -14.0), target=(0.0, -1.5, 0.0), up=(0.0, 1.0, 0.0), vfov=50.0))
+
+
+# ---------------------------------------------------------------------
+# Scene content beyond the benchmark configurations: textures, fog,
+# volumetric clouds (the reference's texture_albedo_uv, fog_segment /
+# pt_fog_segment and the volumetric sky)
+# ---------------------------------------------------------------------
+def checker_image(h: int = 6, w: int = 8, seed: int = 9) -> np.ndarray:
+    """A small random sRGB image (h, w, 3) uint8 for TEXTURE_IMAGE."""
+    return np.random.default_rng(seed).integers(0, 256, (h, w, 3), dtype=np.uint8)
+
+
+def feature_scene(fog: str | None = None, clouds: bool = False, seed: int = 11) -> SceneDesc:
+    """Ground plane (3D checker), spheres with the procedural kinds (stripes,
+    earth, moon, noise), UV checker and image textures on a sphere, a box, a
+    tapered cylinder, a tilted plane and two UV-mapped triangles, a glass
+    sphere and an emissive light, under the default sky.
+    fog: None, "analytic" (height fog with noise) or "marched"
+    (fog.shadow_steps = 6: sun shadow segments through the medium).
+    clouds: a volumetric cloud slab (cloud_thickness 40 at height 60)."""
+    rng = np.random.default_rng(seed)
+    K = {"checker": 1, "stripes": 2, "earth": 3, "moon": 4, "noise": 5, "image": 6, "uv": 7}
+    mats = [material(albedo=(0.8, 0.8, 0.8), texture_kind=K["checker"], texture_scale=1.5,
+                     texture_color_a=(0.9, 0.85, 0.8), texture_color_b=(0.2, 0.25, 0.3))]
+    kinds = ["stripes", "earth", "moon", "noise", "uv", "image"]
+    for k in kinds:
+        mats.append(material(albedo=tuple(rng.uniform(0.6, 1.0, 3)), texture_kind=K[k], texture_scale=float(
+            rng.uniform(0.6, 2.0)), texture_color_a=tuple(rng.uniform(0.2, 1.0, 3)),
+            texture_color_b=tuple(rng.uniform(0.0, 0.6, 3)), roughness=0.6, pbr=int(k in ("earth", "noise"))))
+    mats.append(glass_material())
+    mats.append(light_material((1.0, 0.9, 0.8), 10.0))
+    uv_mat, img_mat = 1 + kinds.index("uv"), 1 + kinds.index("image")
+    prims = prims_array(15)
+    # the ground lies inside a checker cell (cells of 1.5 from y = 0): on a
+    # cell boundary the 3D checker's parity would follow the sign of the hit
+    # point's rounding error, in the reference as well
+    set_plane(prims[0], (0.0, 0.2, 0.0), (0.0, 1.0, 0.0), 0)
+    for i in range(6):
+        set_sphere(prims[1 + i], (-6.0 + 2.4 * i, 1.0, 1.0 + 0.8 * (i % 2)), 1.0, 1 + i)
+    set_sphere(prims[7], (0.5, 0.7, -2.5), 0.7, 1 + len(kinds))          # glass
+    set_sphere(prims[8], (3.0, 5.0, -3.0), 0.5, 2 + len(kinds))          # light
+    b = prims[9]
+    b["kind"], b["material"] = PRIM_BOX, uv_mat
+    b["v"][:6] = (-3.5, 0.8, -2.0, 0.8, 0.8, 0.8)
+    c = prims[10]
+    c["kind"], c["material"] = PRIM_CYLINDER, img_mat
+    c["v"][:8] = (3.5, 0.0, -1.5, 3.2, 2.2, -1.6, 0.9, 0.5)
+    for k, (tri, uv) in enumerate(((((-2.0, 0.21, -5.0), (2.0, 0.21, -5.0), (2.0, 3.0, -6.0)), (0, 0, 2, 0, 2, 2)),
+                                   (((-2.0, 0.21, -5.0), (2.0, 3.0, -6.0), (-2.0, 3.0, -6.0)), (0, 0, 2, 2, 0, 2)))):
+        t = prims[11 + k]
+        t["kind"], t["material"], t["has_uv"] = PRIM_TRIANGLE, img_mat, 1
+        t["v"] = np.array(tri, np.float64).ravel()
+        t["uv"] = uv
+    # a tilted plane far below the ground, seen through the glass sphere,
+    # carries the UV checker so planes exercise their (u, v) too
+    set_plane(prims[13], (0.0, -50.0, 0.0), (0.1, 1.0, 0.05), uv_mat)
+    t = prims[14]
+    t["kind"], t["material"] = PRIM_TRIANGLE, uv_mat  # barycentric (u, v)
+    t["v"] = np.array(((4.0, 0.21, 3.0), (7.0, 0.21, 3.0), (5.5, 2.5, 4.0)), np.float64).ravel()
+    sky = default_sky(sun_dir=normalize((0.3, 0.8, 0.5)))
+    if clouds:
+        sky.update(cloud_thickness=40.0, cloud_height=60.0, cloud_scale=0.02, cloud_coverage=0.45, cloud_steps=16)
+    d = SceneDesc(prims=prims, materials=np.array(mats, MATERIAL_DTYPE), sky=sky,
+                  camera=dict(eye=(0.0, 4.0, -12.0), target=(0.0, 1.5, 0.0), up=(0.0, 1.0, 0.0), vfov=55.0),
+                  images={img_mat: checker_image()})
+    if fog == "analytic":
+        d.fog_density = 0.04
+        d.fog = dict(height=0.5, height_falloff=0.15, noise_scale=0.3, noise_amount=0.4)
+    elif fog == "marched":
+        d.fog_density = 0.05
+        d.fog = dict(height_falloff=0.1, shadow_steps=6)
+    return d
 
 
 # ---------------------------------------------------------------------

@@ -160,9 +160,22 @@ class RefScene:
             cloud_height=s.cloud_height, cloud_scale=s.cloud_scale, cloud_coverage=s.cloud_coverage,
             cloud_softness=s.cloud_softness, cloud_sharpness=s.cloud_sharpness, cloud_octaves=s.cloud_octaves,
             cloud_thickness=s.cloud_thickness, seed=s.seed, sun_radius=s.sun_radius,
+            cloud_density=s.cloud_density, cloud_steps=s.cloud_steps,
         )
+        fog = dict(color=tuple(d.fog_color), height=d.fog_height, height_falloff=d.fog_height_falloff,
+                   inscatter_strength=d.fog_inscatter_strength, sun_anisotropy=d.fog_sun_anisotropy,
+                   noise_scale=d.fog_noise_scale, noise_amount=d.fog_noise_amount, shadow_steps=d.fog_shadow_steps)
+        # image textures: copy the bytes the reference scene owns
+        images = {}
+        for i in range(m):
+            addr = int(mats[i]["texture_rgb"])
+            if addr:
+                h, w = int(mats[i]["texture_height"]), int(mats[i]["texture_width"])
+                images[i] = np.ctypeslib.as_array((C.c_uint8 * (h * w * 3)).from_address(addr)).reshape(h, w, 3).copy()
+                mats[i]["texture_rgb"] = 0
         desc = SceneDesc(prims=prims, materials=mats, sky=sky, water_level=d.water_level,
-                         water_material=d.water_material, fog_density=d.fog_density)
+                         water_material=d.water_material, fog_density=d.fog_density, fog=fog,
+                         images=images or None)
         return desc, Camera(cam)
 
     def lights(self):

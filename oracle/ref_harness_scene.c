@@ -130,9 +130,18 @@ void *mtref_from_desc(const mt_scene_desc *d, const mt_camera *cam)
     s->sky.star_intensity = d->sky.star_intensity;
     s->sky.nebula_intensity = d->sky.nebula_intensity;
     s->sky.galaxy_intensity = d->sky.galaxy_intensity;
+    s->sky.cloud_density = d->sky.cloud_density;
+    s->sky.cloud_steps = d->sky.cloud_steps;
     fog_default_params(&s->fog);
     s->fog.density = d->fog_density;
     s->fog.shadow_steps = d->fog_shadow_steps;
+    s->fog.color = dv3(d->fog_color);
+    s->fog.height = d->fog_height;
+    s->fog.height_falloff = d->fog_height_falloff;
+    s->fog.inscatter_strength = d->fog_inscatter_strength;
+    s->fog.sun_anisotropy = d->fog_sun_anisotropy;
+    s->fog.noise_scale = d->fog_noise_scale;
+    s->fog.noise_amount = d->fog_noise_amount;
     s->has_ocean = d->ocean.enabled;
     if (d->ocean.enabled) {
         s->ocean_params.enabled = 1;
@@ -167,6 +176,29 @@ void *mtref_from_desc(const mt_scene_desc *d, const mt_camera *cam)
             o->emissive = dv3(m->emissive);
             o->pbr = m->pbr;
             o->texture_kind = m->texture_kind;
+            o->texture_scale = m->texture_scale;
+            o->texture_color_a = dv3(m->texture_color_a);
+            o->texture_color_b = dv3(m->texture_color_b);
+            if (m->texture_rgb && m->texture_width > 0 && m->texture_height > 0) {
+                /* an image texture, owned by the Scene's texture table */
+                ImageTexture *img = texture_image_create(m->texture_width, m->texture_height);
+                if (!img) goto fail;
+                memcpy(img->rgb, m->texture_rgb, (size_t)m->texture_width * (size_t)m->texture_height * 3u);
+                if (s->texture_count == s->texture_capacity) {
+                    int cap = s->texture_capacity ? 2 * s->texture_capacity : 4;
+                    SceneTexture *t = (SceneTexture *)realloc(s->textures, (size_t)cap * sizeof *t);
+                    if (!t) {
+                        texture_image_free(img);
+                        goto fail;
+                    }
+                    s->textures = t;
+                    s->texture_capacity = cap;
+                }
+                s->textures[s->texture_count].path = NULL;
+                s->textures[s->texture_count].image = img;
+                s->texture_count++;
+                o->texture_image = img;
+            }
             o->bump_strength = m->bump_strength;
             o->bump_scale = 1.0;
             o->atmosphere_glow = dv3(m->atmosphere_glow);
@@ -187,9 +219,17 @@ void *mtref_from_desc(const mt_scene_desc *d, const mt_camera *cam)
             q = prim_box(dv3(p->v), dv3(p->v + 3), p->material);
             break;
         case MT_PRIM_TRIANGLE:
-            if (p->smooth)
+            if (p->smooth && p->has_uv)
+                q = prim_triangle_smooth_uv(dv3(p->v), dv3(p->v + 3), dv3(p->v + 6), dv3(p->n), dv3(p->n + 3),
+                                            dv3(p->n + 6), vec3(p->uv[0], p->uv[1], 0.0),
+                                            vec3(p->uv[2], p->uv[3], 0.0), vec3(p->uv[4], p->uv[5], 0.0),
+                                            p->material);
+            else if (p->smooth)
                 q = prim_triangle_smooth(dv3(p->v), dv3(p->v + 3), dv3(p->v + 6),
                                          dv3(p->n), dv3(p->n + 3), dv3(p->n + 6), p->material);
+            else if (p->has_uv)
+                q = prim_triangle_uv(dv3(p->v), dv3(p->v + 3), dv3(p->v + 6), vec3(p->uv[0], p->uv[1], 0.0),
+                                     vec3(p->uv[2], p->uv[3], 0.0), vec3(p->uv[4], p->uv[5], 0.0), p->material);
             else
                 q = prim_triangle(dv3(p->v), dv3(p->v + 3), dv3(p->v + 6), p->material);
             break;

@@ -56,20 +56,50 @@ def test_argument_codes_without_scene(mtlib):
 
 
 def test_unsupported_content_is_rejected(mtlib):
-    d = scenes.spheres_scene()
-    for mutate in ("fog", "texture", "csg", "clouds"):
+    """CSG / SDF primitives, bump maps and the star / nebula / galaxy sky
+    terms stay off the GPU path (MT_ERR_UNSUPPORTED, no CPU fallback)."""
+    for mutate in ("csg", "bump", "stars"):
         dd = scenes.spheres_scene()
-        if mutate == "fog":
-            dd.fog_density = 0.1
-        elif mutate == "texture":
-            dd.materials["texture_kind"][1] = 1
-        elif mutate == "csg":
+        if mutate == "csg":
             dd.prims["kind"][3] = 5
-        else:
-            dd.sky["cloud_thickness"] = 10.0
+        elif mutate == "bump":
+            dd.materials["bump_strength"][1] = 0.5
         cd = dd.c_desc()
+        if mutate == "stars":
+            cd.sky.star_intensity = 1.0
         h = C.c_void_p()
         assert mtlib.mt_scene_create(C.byref(cd), None, C.byref(h)) == _capi.MT_ERR_UNSUPPORTED
+
+
+def test_feature_fields_reach_the_descriptor(mtlib):
+    """Fog, clouds and image textures travel through mt_scene_desc; an image
+    pointer without an image size is an argument error (before any device
+    work)."""
+    dd = scenes.feature_scene(fog="marched", clouds=True)
+    cd = dd.c_desc()
+    assert cd.fog_shadow_steps == 6 and cd.sky.cloud_thickness == 40.0 and cd.fog_density > 0
+    img = [i for i in range(len(dd.materials)) if dd.materials["texture_kind"][i] == _capi.TEXTURE_IMAGE][0]
+    assert dd.materials["texture_rgb"][img] != 0 and dd.materials["texture_width"][img] == 8
+    bad = scenes.spheres_scene()
+    bad.materials["texture_rgb"][1] = 1  # a pointer with no image size
+    h = C.c_void_p()
+    assert mtlib.mt_scene_create(C.byref(bad.c_desc()), None, C.byref(h)) == _capi.MT_ERR_INVALID
+
+
+def test_feature_scene_round_trips_through_the_reference(oracle):
+    """The reference scene built from the descriptor exports the same fog,
+    cloud, texture and UV fields back (harness + binding)."""
+    d = scenes.feature_scene(fog="analytic", clouds=True)
+    rs = oracle.RefScene.from_desc(d)
+    d2, _ = rs.export()
+    assert np.array_equal(d.prims, d2.prims)
+    for f in ("texture_kind", "texture_scale", "texture_color_a", "texture_color_b", "albedo"):
+        assert np.array_equal(d.materials[f], d2.materials[f]), f
+    for k, v in d.fog.items():
+        assert np.allclose(d2.fog[k], v), k
+    assert d2.sky["cloud_thickness"] == 40.0 and d2.sky["cloud_steps"] == 16
+    (i, img), = d.images.items()
+    assert np.array_equal(d2.images[i], img)
 
 
 def test_camera_matches_reference(oracle):
