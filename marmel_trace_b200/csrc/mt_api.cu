@@ -401,6 +401,9 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     S->has_passthrough = 0;
     for (int i = 0; i < d->material_count; ++i)
         if (d->materials[i].is_water || d->materials[i].transparency > 0.8) S->has_passthrough = 1;
+    S->has_extras = d->fog_density > 0.0 || d->fog_shadow_steps > 0 || d->sky.cloud_thickness > 1e-4;
+    for (int i = 0; i < d->material_count; ++i)
+        if (d->materials[i].texture_kind != MT_TEXTURE_NONE) S->has_extras = 1;
     S->water_level = (R)d->water_level;
     S->ocean.enabled = d->ocean.enabled;
     S->ocean.seed = d->ocean.seed;

@@ -302,7 +302,9 @@ template <typename R> MT_NOINLINE V3<R> sky_clouds_volumetric(V3<R> dir, const D
     return lerp(base, combined, horizon_fade);
 }
 
-template <typename R> MT_D V3<R> sky_sample(V3<R> dir, const DevSky<R> &sky)
+// VOL = false: a caller that knows the sky has no volumetric slab (the
+// branch is then compiled out).
+template <typename R, bool VOL = true> MT_D V3<R> sky_sample(V3<R> dir, const DevSky<R> &sky)
 {
     R h = mat_clamp01(dir.y);
     R t = pow_nonneg(h, sky.gradient_gamma);
@@ -313,8 +315,8 @@ template <typename R> MT_D V3<R> sky_sample(V3<R> dir, const DevSky<R> &sky)
         R glow = pow_nonneg(cos_sun, sky.sun_glow_exponent) * sky.sun_glow_strength;
         base = add(base, scale(sun_color, glow));
     }
-    if (sky.cloud_thickness > R(1e-4)) {
-        base = sky_clouds_volumetric(dir, sky, base, cos_sun);
+    if (VOL && sky.cloud_thickness > R(1e-4)) {
+        if constexpr (VOL) base = sky_clouds_volumetric(dir, sky, base, cos_sun);
     } else if (dir.y > R(0.03)) {
         // planar clouds (src/material.c:557-595)
         R tt = sky.cloud_height / dir.y;

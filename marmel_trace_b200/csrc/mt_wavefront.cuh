@@ -254,7 +254,11 @@ MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> 
 //
 // When the bounce's extend results were sorted by material (C->sorted), the
 // kernel reads the sorted copies instead.
-template <typename R, bool ADJ>
+//
+// EXTRAS: the scene has fog, marched media, volumetric clouds or a textured
+// material (DevScene::has_extras). Without them those paths are compiled out:
+// their out-of-line calls would otherwise constrain the kernel's registers.
+template <typename R, bool ADJ, bool EXTRAS>
 __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
                                                   WfCounters *C, int which, int b, int max_depth, WfPath<R> *paths,
                                                   R *nee, WfRay<R> *rays_out, WfShadow<R> *sq, WfAdj<R> A,
@@ -315,13 +319,16 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const __grid_constant_
                 // (src/pathtrace.c:837-857)
                 if (st.medium >= 0) {
                     const V3<R> beta_in = throughput;
-                    pt_water_segment(S, st.medium, ro, d, R(5.0), st.seed_key, b, &throughput, &radiance);
+                    if constexpr (EXTRAS)
+                        pt_water_segment(S, st.medium, ro, d, R(5.0), st.seed_key, b, &throughput, &radiance);
+                    else
+                        pt_apply_medium(S.materials[st.medium], R(5.0), &throughput, &radiance);
                     if constexpr (ADJ)
                         medium_grad(ctx, S.materials[st.medium], st.medium, R(5.0), beta_in, sub(Lp, radiance), adj);
                     st.medium = -1;
                 }
-                V3<R> sky_col = sky_sample(d, S.sky);
-                if (S.fog.density > R(0)) {
+                V3<R> sky_col = sky_sample<R, EXTRAS>(d, S.sky);
+                if (EXTRAS && S.fog.density > R(0)) {
                     R T;
                     V3<R> ins;
                     if (b == 0) pt_fog_segment(S, ro, d, R(1e30), st.seed_key, b, &T, &ins);
@@ -341,10 +348,13 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const __grid_constant_
                 finish_hit(S, ro, unit_dir(d), th, &h);
                 if (st.medium >= 0) {
                     const V3<R> beta_in = throughput;
-                    pt_water_segment(S, st.medium, ro, d, h.t, st.seed_key, b, &throughput, &radiance);
+                    if constexpr (EXTRAS)
+                        pt_water_segment(S, st.medium, ro, d, h.t, st.seed_key, b, &throughput, &radiance);
+                    else
+                        pt_apply_medium(S.materials[st.medium], h.t, &throughput, &radiance);
                     if constexpr (ADJ)
                         medium_grad(ctx, S.materials[st.medium], st.medium, h.t, beta_in, sub(Lp, radiance), adj);
-                } else if (S.fog.density > R(0)) {
+                } else if (EXTRAS && S.fog.density > R(0)) {
                     R T;
                     V3<R> ins;
                     if (b == 0) pt_fog_segment(S, ro, d, h.t, st.seed_key, b, &T, &ins);
@@ -353,12 +363,12 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const __grid_constant_
                     throughput = scale(throughput, T);
                 }
                 if (h.material < 0 || h.material >= S.material_count) {
-                    radiance = add(radiance, mul(throughput, sky_sample(d, S.sky)));
+                    radiance = add(radiance, mul(throughput, sky_sample<R, EXTRAS>(d, S.sky)));
                     if constexpr (ADJ) sky_sun_grad(ctx, d, S.sky, mul(adj, throughput));
                 } else {
                     const DevMaterial<R> &m = S.materials[h.material];
                     msh = S.materials + h.material;
-                    if (m.texture_kind != 0) {
+                    if (EXTRAS && m.texture_kind != 0) {
                         m_tex = m;
                         const V3<R> a = surface_albedo(S, m, ro, unit_dir(d), h);
                         m_tex.albedo[0] = a.x;

@@ -314,13 +314,20 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             }
             tic();
             if (replay) {
-                k_wf_shade<R, true><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
-                                                                 rays[which ^ 1], sq, A, nullptr, nullptr);
+                // the adjoint rejects every scene extra
+                k_wf_shade<R, true, false><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth,
+                                                                        paths, nee, rays[which ^ 1], sq, A, nullptr,
+                                                                        nullptr);
             } else {
-                k_wf_shade<R, false><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth, paths, nee,
-                                                         rays[which ^ 1], sq, none,
-                                                         sort ? (const WfRay<R> *)st->sorted_rays : nullptr,
-                                                         (const WfHit<R> *)st->sorted_hits);
+                const WfRay<R> *srays = sort ? (const WfRay<R> *)st->sorted_rays : nullptr;
+                if (S.has_extras)
+                    k_wf_shade<R, false, true><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth,
+                                                                            paths, nee, rays[which ^ 1], sq, none,
+                                                                            srays, (const WfHit<R> *)st->sorted_hits);
+                else
+                    k_wf_shade<R, false, false><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth,
+                                                                             paths, nee, rays[which ^ 1], sq, none,
+                                                                             srays, (const WfHit<R> *)st->sorted_hits);
             }
             toc(1);
             tic();
