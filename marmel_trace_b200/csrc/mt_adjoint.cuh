@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(128) k_adjoint(const __grid_constant__ DevScen
             for (int s = s0; s < s1; ++s) {
                 Ray3<R> ray = pt_primary(S, cam, w, h, x, y, s);
                 uint32_t seed_key = hash3((uint32_t)x, (uint32_t)y, (uint32_t)s);
-                V3<R> L = pathtrace_radiance(S, ray, depth, seed_key);
+                V3<R> L = pathtrace_radiance<R, false>(S, ray, depth, seed_key);  // no extras: rejected on entry
                 pathtrace_adjoint(S, ray, depth, seed_key, L, adj, ctx);
             }
         }

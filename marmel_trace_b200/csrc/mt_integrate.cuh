@@ -356,7 +356,8 @@ MT_D bool pt_occluded_segment_abs(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin
 }
 
 // pt_nee_sun (src/pathtrace.c:534-556)
-template <typename R>
+// EXTRAS = false: the scene has no volumetric clouds (DevScene::has_extras).
+template <typename R, bool EXTRAS = true>
 MT_D V3<R> pt_nee_sun(const DevScene<R> &S, const DevMaterial<R> &mm, V3<R> P, V3<R> N, V3<R> V, V3<R> throughput,
                       uint32_t seed_key, int bounce)
 {
@@ -369,7 +370,7 @@ MT_D V3<R> pt_nee_sun(const DevScene<R> &S, const DevMaterial<R> &mm, V3<R> P, V
     V3<R> so = add(P, scale(N, R(1e-3)));
     V3<R> atten;
     if (pt_occluded_segment(S, so, L, R(1e-3), R(1e30), &atten)) return zero;
-    atten = scale(atten, cloud_transmittance(S.sky, so, L));
+    if constexpr (EXTRAS) atten = scale(atten, cloud_transmittance(S.sky, so, L));
     if (atten.x < R(1e-4) && atten.y < R(1e-4) && atten.z < R(1e-4)) return zero;
     R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
     R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
@@ -554,7 +555,9 @@ template <typename R> MT_D V3<R> atmosphere_term(const DevMaterial<R> &mm, V3<R>
 }
 
 // pathtrace_radiance (src/pathtrace.c:800-1028) without fog (rejected on upload)
-template <typename R>
+// EXTRAS = false: the scene has no fog, marched media, clouds or textures
+// (DevScene::has_extras); those paths are then compiled out.
+template <typename R, bool EXTRAS = true>
 MT_D V3<R> pathtrace_radiance(const DevScene<R> &S, Ray3<R> primary, int max_depth, uint32_t seed_key)
 {
     V3<R> radiance = v3(R(0), R(0), R(0));
@@ -574,11 +577,12 @@ MT_D V3<R> pathtrace_radiance(const DevScene<R> &S, Ray3<R> primary, int max_dep
         SurfaceHit<R> h;
         if (!scene_intersect(S, r.o, r.d, R(1e-4), R(1e30), &h)) {
             if (medium >= 0) {
-                pt_water_segment(S, medium, r.o, r.d, R(5.0), seed_key, b, &throughput, &radiance);
+                if constexpr (EXTRAS) pt_water_segment(S, medium, r.o, r.d, R(5.0), seed_key, b, &throughput, &radiance);
+                else pt_apply_medium(S.materials[medium], R(5.0), &throughput, &radiance);
                 medium = -1;
             }
-            V3<R> sky_col = sky_sample(r.d, S.sky);
-            if (S.fog.density > R(0)) {
+            V3<R> sky_col = sky_sample<R, EXTRAS>(r.d, S.sky);
+            if (EXTRAS && S.fog.density > R(0)) {
                 R T;
                 V3<R> ins;
                 if (b == 0) pt_fog_segment(S, r.o, r.d, R(1e30), seed_key, b, &T, &ins);
@@ -589,8 +593,9 @@ MT_D V3<R> pathtrace_radiance(const DevScene<R> &S, Ray3<R> primary, int max_dep
             break;
         }
         if (medium >= 0) {
-            pt_water_segment(S, medium, r.o, r.d, h.t, seed_key, b, &throughput, &radiance);
-        } else if (S.fog.density > R(0)) {
+            if constexpr (EXTRAS) pt_water_segment(S, medium, r.o, r.d, h.t, seed_key, b, &throughput, &radiance);
+            else pt_apply_medium(S.materials[medium], h.t, &throughput, &radiance);
+        } else if (EXTRAS && S.fog.density > R(0)) {
             R T;
             V3<R> ins;
             if (b == 0) pt_fog_segment(S, r.o, r.d, h.t, seed_key, b, &T, &ins);
@@ -599,7 +604,7 @@ MT_D V3<R> pathtrace_radiance(const DevScene<R> &S, Ray3<R> primary, int max_dep
             throughput = scale(throughput, T);
         }
         if (h.material < 0 || h.material >= S.material_count) {
-            radiance = add(radiance, mul(throughput, sky_sample(r.d, S.sky)));
+            radiance = add(radiance, mul(throughput, sky_sample<R, EXTRAS>(r.d, S.sky)));
             break;
         }
         const DevMaterial<R> &m = S.materials[h.material];
@@ -617,7 +622,7 @@ MT_D V3<R> pathtrace_radiance(const DevScene<R> &S, Ray3<R> primary, int max_dep
         // texture-modulated albedo on a local copy (src/pathtrace.c:903-905)
         DevMaterial<R> m_tex;
         const DevMaterial<R> *mp = &m;
-        if (m.texture_kind != 0) {
+        if (EXTRAS && m.texture_kind != 0) {
             m_tex = m;
             V3<R> a = surface_albedo(S, m, r.o, unit_dir(r.d), h);
             m_tex.albedo[0] = a.x;
@@ -632,7 +637,7 @@ MT_D V3<R> pathtrace_radiance(const DevScene<R> &S, Ray3<R> primary, int max_dep
         if (S.light_count > 0)
             radiance = add(radiance, pt_nee_emissive(S, mm, P, N, V, throughput, h.prim, seed_key, b));
         if (b == 0 || (b == 1 && medium >= 0 && last_bounce_specular))
-            radiance = add(radiance, pt_nee_sun(S, mm, P, N, V, throughput, seed_key, b));
+            radiance = add(radiance, pt_nee_sun<R, EXTRAS>(S, mm, P, N, V, throughput, seed_key, b));
         uint32_t kb = hash3(seed_key ^ PT_KEY, (uint32_t)b, 0u);
         R u1 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_A);
         R u2 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_B);
@@ -714,7 +719,8 @@ template <typename R> struct WhFrame {
 };
 
 // The hit fields of a Whitted frame, with its albedo (src/render.c:620-621).
-template <typename R> MT_D void wh_set_hit(const DevScene<R> &S, WhFrame<R> &f, V3<R> o, V3<R> d, const SurfaceHit<R> &h)
+template <typename R, bool EXTRAS>
+MT_D void wh_set_hit(const DevScene<R> &S, WhFrame<R> &f, V3<R> o, V3<R> d, const SurfaceHit<R> &h)
 {
     f.P = h.point;
     f.N = h.normal;
@@ -722,8 +728,9 @@ template <typename R> MT_D void wh_set_hit(const DevScene<R> &S, WhFrame<R> &f, 
     f.mat = h.material;
     f.prim = h.prim;
     f.front = h.front_face;
-    if (h.material >= 0 && h.material < S.material_count)
-        f.alb = surface_albedo(S, S.materials[h.material], o, unit_dir(d), h);
+    if constexpr (EXTRAS)
+        if (h.material >= 0 && h.material < S.material_count)
+            f.alb = surface_albedo(S, S.materials[h.material], o, unit_dir(d), h);
 }
 
 template <typename R>
@@ -763,7 +770,8 @@ MT_D V3<R> emissive_direct(const DevScene<R> &S, const DevMaterial<R> &mm, V3<R>
     return scale(sum, R(1) / R(16));
 }
 
-template <typename R>
+// EXTRAS = false: the scene has no fog, clouds or textures (DevScene::has_extras).
+template <typename R, bool EXTRAS = true>
 MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint32_t seed_key)
 {
     WhFrame<R> st[kWhittedFrames];
@@ -781,7 +789,7 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
     sp = 1;
     // a frame's result, with trace()'s fog when it entered through trace()
     auto fogged = [&](const WhFrame<R> &fr, V3<R> c) {
-        return (fr.traced && S.fog.density > R(0)) ? fog_apply(S.fog, S.sky, fr.o, fr.d, fr.fog_t, c) : c;
+        return (EXTRAS && fr.traced && S.fog.density > R(0)) ? fog_apply(S.fog, S.sky, fr.o, fr.d, fr.fog_t, c) : c;
     };
     int guard = 0;
     while (sp > 0) {
@@ -806,12 +814,12 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
             f.traced = 1;
             if (!scene_intersect(S, f.o, f.d, R(1e-4), R(1e30), &h)) {
                 f.fog_t = R(1e30);
-                ret = fogged(f, sky_sample(f.d, S.sky));
+                ret = fogged(f, sky_sample<R, EXTRAS>(f.d, S.sky));
                 --sp;
                 continue;
             }
             f.fog_t = h.t;
-            wh_set_hit(S, f, f.o, f.d, h);
+            wh_set_hit<R, EXTRAS>(S, f, f.o, f.d, h);
         }
         // fall through: shade the hit
         case WH_HIT: {
@@ -821,14 +829,14 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
                 continue;
             }
             if (f.mat < 0 || f.mat >= S.material_count) {
-                ret = fogged(f, sky_sample(f.d, S.sky));
+                ret = fogged(f, sky_sample<R, EXTRAS>(f.d, S.sky));
                 --sp;
                 continue;
             }
             const DevMaterial<R> &m0 = S.materials[f.mat];
             DevMaterial<R> m_tex;
             const DevMaterial<R> *mp = &m0;
-            if (m0.texture_kind != 0) {
+            if (EXTRAS && m0.texture_kind != 0) {
                 m_tex = m0;
                 m_tex.albedo[0] = f.alb.x;
                 m_tex.albedo[1] = f.alb.y;
@@ -960,11 +968,11 @@ MT_D V3<R> whitted_trace(const DevScene<R> &S, Ray3<R> ray, int max_depth, uint3
                         c.depth = f.depth + 1;
                         c.phase = WH_HIT;
                         c.traced = 0;  // trace_hit directly: no fog (src/render.c:786-790)
-                        wh_set_hit(S, c, ro, rd, h2);
+                        wh_set_hit<R, EXTRAS>(S, c, ro, rd, h2);
                         ++sp;
                         continue;
                     }
-                    V3<R> inner = sky_sample(rd, S.sky);
+                    V3<R> inner = sky_sample<R, EXTRAS>(rd, S.sky);
                     ret = (m.is_water || m.beer_lambert) ? water_attenuate(m, inner, R(5.0)) : inner;
                     finish = true;
                 }

@@ -14,7 +14,9 @@ namespace mt {
 // (src/pathtrace.c:1053-1095, src/render.c:929-966). The image is read in
 // row-major order, so a warp covers 32 horizontally adjacent pixels whose
 // primary rays are coherent.
-template <typename R, int MODE>
+// EXTRAS: the scene has fog, marched media, clouds or textures
+// (DevScene::has_extras); without them those paths are compiled out.
+template <typename R, int MODE, bool EXTRAS>
 __global__ void __launch_bounds__(128) k_render(const __grid_constant__ DevScene<R> S, const DevCamera<R> cam, int w, int h,
                                                 int spp_total, int s0, int s1, int depth, int out_kind, void *out)
 {
@@ -27,11 +29,11 @@ __global__ void __launch_bounds__(128) k_render(const __grid_constant__ DevScene
         if (MODE == RENDER_PT) {
             Ray3<R> ray = pt_primary(S, cam, w, h, x, y, s);
             uint32_t seed_key = hash3((uint32_t)x, (uint32_t)y, (uint32_t)s);
-            acc = add(acc, pathtrace_radiance(S, ray, depth, seed_key));
+            acc = add(acc, pathtrace_radiance<R, EXTRAS>(S, ray, depth, seed_key));
         } else {
             Ray3<R> ray = wh_primary(cam, w, h, spp_total, x, y, s);
             uint32_t seed_key = hash3((uint32_t)x, (uint32_t)y, (uint32_t)s);
-            acc = add(acc, whitted_trace(S, ray, depth, seed_key));
+            acc = add(acc, whitted_trace<R, EXTRAS>(S, ray, depth, seed_key));
         }
     }
     if (S.counters && s1 > s0) atomicAdd(&S.counters->primary_rays, (unsigned long long)(s1 - s0));
@@ -148,12 +150,16 @@ cudaError_t launch_render(const DevScene<R> &S, const DevCamera<R> &cam, int w, 
     if (block <= 0) block = 128;
     if (block > 128) block = 128;  // __launch_bounds__(128)
     long long n = (long long)w * h;
-    if (mode == RENDER_PT)
-        k_render<R, RENDER_PT><<<grid_for(n, block), block, stack_smem(S, block), stream>>>(S, cam, w, h, spp_total, s0, s1, depth,
-                                                                         out_kind, out);
+    const int g = grid_for(n, block);
+    const size_t sm = stack_smem(S, block);
+    if (mode == RENDER_PT && S.has_extras)
+        k_render<R, RENDER_PT, true><<<g, block, sm, stream>>>(S, cam, w, h, spp_total, s0, s1, depth, out_kind, out);
+    else if (mode == RENDER_PT)
+        k_render<R, RENDER_PT, false><<<g, block, sm, stream>>>(S, cam, w, h, spp_total, s0, s1, depth, out_kind, out);
+    else if (S.has_extras)
+        k_render<R, RENDER_WHITTED, true><<<g, block, sm, stream>>>(S, cam, w, h, spp_total, s0, s1, depth, out_kind, out);
     else
-        k_render<R, RENDER_WHITTED><<<grid_for(n, block), block, stack_smem(S, block), stream>>>(S, cam, w, h, spp_total, s0, s1,
-                                                                              depth, out_kind, out);
+        k_render<R, RENDER_WHITTED, false><<<g, block, sm, stream>>>(S, cam, w, h, spp_total, s0, s1, depth, out_kind, out);
     return cudaGetLastError();
 }
 
@@ -217,7 +223,7 @@ MT_D Ray3<R> adaptive_primary(const DevCamera<R> &cam, int w, int h, int n0, int
 
 // One pass (adaptive_region, src/render.c:1174-1240). `list` holds the active
 // pixels (count on the device); NULL means every pixel (pass 0).
-template <typename R>
+template <typename R, bool EXTRAS>
 __global__ void __launch_bounds__(128) k_adaptive_pass(const __grid_constant__ DevScene<R> S, const DevCamera<R> cam, int w, int h,
                                                        int n0, int nmax, int batch, int depth, const int *list,
                                                        const int *count, double *sums, int *nsamp)
@@ -236,7 +242,7 @@ __global__ void __launch_bounds__(128) k_adaptive_pass(const __grid_constant__ D
         const int s = n + k;
         Ray3<R> ray = adaptive_primary(cam, w, h, n0, x, y, s);
         uint32_t seed_key = hash3((uint32_t)x, (uint32_t)y, (uint32_t)s);
-        V3<R> c = whitted_trace(S, ray, depth, seed_key);
+        V3<R> c = whitted_trace<R, EXTRAS>(S, ray, depth, seed_key);
         const double cx = (double)c.x, cy = (double)c.y, cz = (double)c.z;
         sr += cx;
         sg += cy;
@@ -311,8 +317,12 @@ cudaError_t launch_adaptive_pass(const DevScene<R> &S, const DevCamera<R> &cam, 
                                  cudaStream_t stream)
 {
     long long n = (long long)w * h;
-    k_adaptive_pass<R><<<grid_for(n, 128), 128, stack_smem(S, 128), stream>>>(S, cam, w, h, n0, nmax, batch, depth,
-                                                                              list, count, sums, nsamp);
+    if (S.has_extras)
+        k_adaptive_pass<R, true><<<grid_for(n, 128), 128, stack_smem(S, 128), stream>>>(S, cam, w, h, n0, nmax, batch,
+                                                                                        depth, list, count, sums, nsamp);
+    else
+        k_adaptive_pass<R, false><<<grid_for(n, 128), 128, stack_smem(S, 128), stream>>>(S, cam, w, h, n0, nmax, batch,
+                                                                                         depth, list, count, sums, nsamp);
     return cudaGetLastError();
 }
 
