@@ -134,7 +134,7 @@ MT_D int warp_append(int *counter, bool want)
 // ------------------------------------------------------------------
 template <typename R>
 __global__ void k_wf_generate(const __grid_constant__ DevScene<R> S, const WfParams<R> *P, int batch, int batch_spp, int n_paths,
-                              WfPath<R> *paths, WfRay<R> *rays, WfCounters *C, R *nee, WfAdj<R> A)
+                              WfPath<R> *paths, WfRay<R> *rays, WfCounters *C, R *nee, WfAdj<R> A, bool zero_nee)
 {
     const WfParams<R> p = *P;
     const int n_round = (n_paths + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x) * (gridDim.x * blockDim.x);
@@ -162,7 +162,8 @@ __global__ void k_wf_generate(const __grid_constant__ DevScene<R> S, const WfPar
             if (ray.o.y < w_h && S.water_material < S.material_count) st.medium = S.water_material;
         }
         V3<R> d = normalize(ray.d);
-        for (int k = 0; k < kNeeSlots * 3; ++k) nee[(size_t)q * kNeeSlots * 3 + k] = R(0);
+        if (zero_nee)
+            for (int k = 0; k < kNeeSlots * 3; ++k) nee[(size_t)q * kNeeSlots * 3 + k] = R(0);
         if (A.verts) {  // adjoint replay: no vertex pending, no NEE transmittance yet
             A.verts[q].mat = -1;
             for (int k = 0; k < kNeeSlots * kAttStride; ++k) A.att[(size_t)q * kNeeSlots * kAttStride + k] = R(0);

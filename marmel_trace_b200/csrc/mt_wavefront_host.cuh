@@ -46,6 +46,12 @@ struct WavefrontState {
     // (a batch lane renders several, so it turns this off)
     void *occ_cache = nullptr;
     bool occ_cache_on = true;
+    // the NEE slots hold zeros between windows: they are zeroed at
+    // allocation, and every slot a shadow connection writes is gathered (and
+    // zeroed) by the next shade or by finalize; a state whose buffers are
+    // carved from shared memory of changing layout leaves this false and has
+    // k_wf_generate zero them
+    bool nee_clean = false;
     void *walk = nullptr;      // shadow rays left to walk after the occluder-cache pass
     int grid = 0;              // persistent grid (blocks) of the stage kernels
     cudaEvent_t kev[64];       // per-kernel timing events (profiling mode)
@@ -95,6 +101,7 @@ inline void wf_free(WavefrontState *st)
     st->cap_paths = 0;
     st->acc_pixels = 0;
     st->sort_bucket_cap = 0;
+    st->nee_clean = false;
 }
 
 // Batch size of a window of `spp` samples over `wh` pixels: the largest
@@ -136,6 +143,8 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
     WF_CK(cudaMalloc(&st->rays[1], n_paths * sizeof(WfRay<R>)), "cudaMalloc(rays)");
     WF_CK(cudaMalloc(&st->hits, n_paths * sizeof(WfHit<R>)), "cudaMalloc(hits)");
     WF_CK(cudaMalloc(&st->nee, n_paths * kNeeSlots * 3 * sizeof(R)), "cudaMalloc(nee)");
+    WF_CK(cudaMemset(st->nee, 0, n_paths * kNeeSlots * 3 * sizeof(R)), "cudaMemset(nee)");
+    st->nee_clean = true;
     WF_CK(cudaMalloc(&st->shadow, (nshadow ? nshadow : 1) * sizeof(WfShadow<R>)), "cudaMalloc(shadow)");
     WF_CK(cudaMalloc(&st->sample_buf, n_paths * 3 * sizeof(R)), "cudaMalloc(samples)");
     WF_CK(cudaMalloc(&st->acc, wh * 3 * sizeof(R)), "cudaMalloc(acc)");
@@ -288,7 +297,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         WF_CK(cudaMemsetAsync(C, 0, sizeof(WfCounters), s), "memset(counters)");
         tic();
         k_wf_generate<R><<<g, block, 0, s>>>(S, P, batch, batch_spp, n_paths, paths, rays[0], C, nee,
-                                             replay ? A : none);
+                                             replay ? A : none, replay || !st->nee_clean);
         toc(3);
         int which = 0;
         for (int b = 0; b <= depth; ++b) {
