@@ -950,17 +950,25 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_dyn(const __grid_cons
 // finalize + reduce: per-sample radiance (final clamp of
 // src/pathtrace.c:1020-1027) and the per-pixel sum in sample order
 // ------------------------------------------------------------------
+// The final radiance of path q: its last bounce's NEE gathered, then the
+// reference's final NaN -> 0 and negative clamp (src/pathtrace.c:1020-1027).
+template <typename R> MT_D V3<R> finalize_path(const DevScene<R> &S, const WfPath<R> *paths, R *nee, size_t q)
+{
+    const WfPath<R> st = paths[q];
+    V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
+    gather_nee(S, nee + q * kNeeSlots * 3, &radiance);
+    if (!finite3(radiance)) radiance = v3(R(0), R(0), R(0));
+    if (radiance.x < R(0)) radiance.x = R(0);
+    if (radiance.y < R(0)) radiance.y = R(0);
+    if (radiance.z < R(0)) radiance.z = R(0);
+    return radiance;
+}
+
 template <typename R>
 __global__ void k_wf_finalize(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, R *sample_buf)
 {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_paths; q += gridDim.x * blockDim.x) {
-        const WfPath<R> st = paths[q];
-        V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
-        gather_nee(S, nee + (size_t)q * kNeeSlots * 3, &radiance);
-        if (!finite3(radiance)) radiance = v3(R(0), R(0), R(0));
-        if (radiance.x < R(0)) radiance.x = R(0);
-        if (radiance.y < R(0)) radiance.y = R(0);
-        if (radiance.z < R(0)) radiance.z = R(0);
+        const V3<R> radiance = finalize_path(S, paths, nee, (size_t)q);
         sample_buf[3 * (size_t)q] = radiance.x;
         sample_buf[3 * (size_t)q + 1] = radiance.y;
         sample_buf[3 * (size_t)q + 2] = radiance.z;
@@ -989,16 +997,23 @@ __global__ void k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_p
 }
 
 template <typename R>
-__global__ void k_wf_reduce(const WfParams<R> *P, int batch_spp, int first_batch, int last_batch,
-                            const R *sample_buf, R *acc)
+__global__ void k_wf_reduce(const __grid_constant__ DevScene<R> S, const WfParams<R> *P, int batch_spp, int first_batch,
+                            int last_batch, const R *sample_buf, R *acc, const WfPath<R> *paths, R *nee)
 {
     const WfParams<R> p = *P;
     for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < p.wh; pix += gridDim.x * blockDim.x) {
         V3<R> a = v3(R(0), R(0), R(0));
         if (!first_batch) a = v3(acc[3 * (size_t)pix], acc[3 * (size_t)pix + 1], acc[3 * (size_t)pix + 2]);
         for (int j = 0; j < batch_spp; ++j) {
-            const R *sb = sample_buf + 3 * ((size_t)j * p.wh + pix);
-            a = add(a, v3(sb[0], sb[1], sb[2]));
+            const size_t q = (size_t)j * p.wh + pix;
+            if (paths) {
+                // fused with finalize: the same per-path radiance, summed in
+                // sample order without the round trip through sample_buf
+                a = add(a, finalize_path(S, paths, nee, q));
+            } else {
+                const R *sb = sample_buf + 3 * q;
+                a = add(a, v3(sb[0], sb[1], sb[2]));
+            }
         }
         if (!last_batch) {
             acc[3 * (size_t)pix] = a.x;

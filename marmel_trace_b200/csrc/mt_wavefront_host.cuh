@@ -355,9 +355,12 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         int rc = bounces(batch, false);
         if (rc) return rc;
         tic();
-        k_wf_finalize<R><<<g, block, 0, s>>>(S, n_paths, paths, nee, sample_buf);
-        if (!adjoint)
-            k_wf_reduce<R><<<g, block, 0, s>>>(P, batch_spp, batch == 0, batch == n_batches - 1, sample_buf, acc);
+        if (adjoint) {
+            k_wf_finalize<R><<<g, block, 0, s>>>(S, n_paths, paths, nee, sample_buf);
+        } else {
+            // one thread per pixel finalises its batch_spp paths and sums them
+            k_wf_reduce<R><<<g, block, 0, s>>>(S, P, batch_spp, batch == 0, batch == n_batches - 1, nullptr, acc, paths, nee);
+        }
         toc(3);
         if (adjoint) {
             if ((rc = bounces(batch, true))) return rc;
