@@ -612,6 +612,7 @@ template <typename R> struct Trav {
     int sp;     // stack entries in use
     bool found;
     int any_code;  // any hit: the tree primitive that blocked (kind << 28 | slot), -1 for a plane
+    int any_leaf;  // any hit: the leaf (leaf_code) holding that primitive, -1 for a plane
 };
 
 // Nearest hit (ANY = false) or any hit (ANY = true) in [tmin, tmax].
@@ -633,6 +634,7 @@ MT_D void trav_init(const DevScene<R> &S, Trav<R> &tv, const RayPre<R> &rp, R tm
     tv.found = false;
     tv.sp = 0;
     tv.any_code = -1;
+    tv.any_leaf = -1;
     for (int i = 0; i < S.plane_count; ++i) {
         R t;
         ++c.ntest;
@@ -675,6 +677,7 @@ MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, T
                 if (ANY) {
                     tv.found = true;
                     tv.any_code = (KIND_TRIANGLE << 28) | (first + i);
+                    tv.any_leaf = node;
                     break;
                 }
                 int pi = tri_prim_index(S, first + i);
@@ -701,6 +704,7 @@ MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, T
                 if (ANY) {
                     tv.found = true;
                     tv.any_code = ref.y;
+                    tv.any_leaf = node;
                     break;
                 }
                 if (!tv.found || t < best->t || (t == best->t && ref.x < best->prim)) {
@@ -898,16 +902,34 @@ template <typename R, int W = 2> MT_D bool scene_any(const DevScene<R> &S, const
     return traverse<R, true, W>(S, rp, tmin, tmax, &dummy);
 }
 
-// Any hit that first tries the primitive in *cache (kind << 28 | slot, -1
-// none) -- a hit there is a hit of the query, so the answer is the same --
-// and otherwise walks the tree and leaves the blocking primitive in *cache.
+// Any hit among the primitives of one leaf (leaf_code; -1: none). Every
+// primitive is tested against the same [tmin, tmax] as in the walk, so a hit
+// here is a hit of the whole any-hit query.
+template <typename R> MT_D bool leaf_occluded(const DevScene<R> &S, int node, const RayPre<R> &rp, R tmin, R tmax)
+{
+    const int leaf = ~node, first = leaf >> 4, count = leaf & 7;
+    if ((leaf >> 3) & 1) {
+        for (int i = 0; i < count; ++i)
+            if (tri_occ(S, first + i, rp, tmin, tmax)) return true;
+    } else {
+        for (int i = 0; i < count; ++i)
+            if (prim_occluded(S, __ldg(S.refs + first + i).y, rp, tmin, tmax)) return true;
+    }
+    return false;
+}
+
+// Any hit that first tries the leaf in *cache (leaf_code, -1 none) -- a hit
+// there is a hit of the query, so the answer is the same -- and otherwise
+// walks the tree and leaves the blocking leaf in *cache. Caching the leaf
+// rather than the one primitive catches the neighbouring primitives of a
+// blocker, which nearby connections often meet instead.
 // test_cached = false: the caller has already tested *cache and it missed.
 template <typename R, int W = 2>
 MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, int *cache,
                            bool test_cached = true)
 {
     const int c = *cache;
-    if (test_cached && c >= 0 && prim_occluded(S, c, rp, tmin, tmax)) {
+    if (test_cached && c != -1 && leaf_occluded(S, c, rp, tmin, tmax)) {
         if (S.counters) count_add(&S.counters->any_prim_tests, 1ull);
         return true;
     }
@@ -921,7 +943,7 @@ MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R 
         }
     }
     trav_count_flush<R, true>(S, cnt);
-    if (tv.found && tv.any_code >= 0 && tv.any_code != c) *cache = tv.any_code;
+    if (tv.found && tv.any_leaf != -1 && tv.any_leaf != c) *cache = tv.any_leaf;
     return tv.found;
 }
 

@@ -694,9 +694,9 @@ __global__ void k_wf_sort_scatter(const WfCounters *C, int which, const WfRay<R>
 //
 // In a scene without pass-through materials the stage runs in two passes
 // over the occluder cache, which holds for each connection's entry (see
-// occ_entry) the primitive that last blocked a connection there:
-// k_wf_shadow_cache tests every connection's cached primitive (a hit there is
-// a hit of the any-hit query, so the answer cannot change), resolves the
+// occ_entry) the BVH leaf that last blocked a connection there:
+// k_wf_shadow_cache tests the primitives of every connection's cached leaf (a
+// hit there is a hit of the any-hit query, so the answer cannot change), resolves the
 // blocked ones and appends the others to `walk`; k_wf_shadow then walks the
 // tree for `walk` only and stores each blocker it finds (scene_any_cached).
 // Cache hits (one primitive test) and walks (the whole tree) therefore do not
@@ -821,8 +821,8 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const __grid_co
             if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
             const int c = *occ_entry(S, occ_cache, wh, b, s);
             const bool blocked =
-                c >= 0 && prim_occluded(S, c, ray_pre(v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2]))),
-                                        R(1e-3), s.tmax);
+                c != -1 && leaf_occluded(S, c, ray_pre(v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2]))),
+                                         R(1e-3), s.tmax);
             if (blocked) {
                 if (S.counters) atomicAdd(&S.counters->any_prim_tests, 1ull);
                 shadow_result<R, ADJ>(s, true, v3(R(1), R(1), R(1)), ab, nee, att);
