@@ -22,7 +22,9 @@
 
 namespace mt {
 
-template <typename R> struct WfRay {
+// 16-byte aligned records (and 8 for paths) so that a record moves in vector
+// loads and stores, not one instruction per word.
+template <typename R> struct alignas(16) WfRay {
     R o[3];
     R d[3];
     int slot;
@@ -35,7 +37,7 @@ template <typename R> struct WfHit {
     int code;
 };
 
-template <typename R> struct WfPath {
+template <typename R> struct alignas(8) WfPath {
     R throughput[3];
     R radiance[3];
     uint32_t seed_key;
@@ -44,7 +46,7 @@ template <typename R> struct WfPath {
     int pad;
 };
 
-template <typename R> struct WfShadow {
+template <typename R> struct alignas(16) WfShadow {
     R o[3];
     R d[3];
     R tmax;
@@ -259,8 +261,11 @@ MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> 
 // EXTRAS: the scene has fog, marched media, volumetric clouds or a textured
 // material (DevScene::has_extras). Without them those paths are compiled out:
 // their out-of-line calls would otherwise constrain the kernel's registers.
+// The FP32 forward kernel is held to 7 blocks of 128 per SM (72 registers):
+// left alone the compiler takes 79 and the SM runs 6 blocks, which measured
+// 22.2 vs 27.0 ms of shading per 16-spp torus-field frame.
 template <typename R, bool ADJ, bool EXTRAS>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shade(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
+__global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRAS) ? 7 : 0) k_wf_shade(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
                                                   WfCounters *C, int which, int b, int max_depth, WfPath<R> *paths,
                                                   R *nee, WfRay<R> *rays_out, WfShadow<R> *sq, WfAdj<R> A,
                                                   const WfRay<R> *sorted_rays, const WfHit<R> *sorted_hits)
