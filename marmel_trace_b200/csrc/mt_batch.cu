@@ -253,9 +253,9 @@ int mt_batch_render(mt_batch *b, int32_t n, const mt_batch_item *items, void *st
                 DevScene<float> S = *mt_scene_dev_f32(items[i].scene);
                 S.counters = nullptr;
                 const WfParams<float> *P = (const WfParams<float> *)b->params + i;
-                // the occluder cache holds primitive codes of one scene
-                ce = cudaMemsetAsync(b->st[l]->occ_cache, 0xFF,
-                                     (b->st[l]->acc_pixels * kNeeSlots + kOccHash) * sizeof(int), b->streams[l]);
+                // the occluder cache holds BVH leaves of one scene
+                ce = cudaMemsetAsync(b->st[l]->occ_cache, 0xFF, occ_cache_ints(b->st[l]->acc_pixels) * sizeof(int),
+                                     b->streams[l]);
                 if (ce != cudaSuccess) break;
                 erc = wf_enqueue<float>(b->st[l], S, items[i].width, items[i].height, bspp[i], nbat[i],
                                         items[i].depth, b->streams[l], false, 128, false, false, P, kBatchSortThreshold);

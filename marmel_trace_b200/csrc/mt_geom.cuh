@@ -924,12 +924,26 @@ template <typename R> MT_D bool leaf_occluded(const DevScene<R> &S, int node, co
 // rather than the one primitive catches the neighbouring primitives of a
 // blocker, which nearby connections often meet instead.
 // test_cached = false: the caller has already tested *cache and it missed.
-template <typename R, int W = 2>
+// The entry holds the WAYS most recent blocking leaves, newest first; all are
+// tried before the walk (occ_ways_occluded).
+template <typename R, int WAYS>
+MT_D bool occ_ways_occluded(const DevScene<R> &S, const int *cache, const RayPre<R> &rp, R tmin, R tmax)
+{
+#pragma unroll
+    for (int k = 0; k < WAYS; ++k) {
+        const int c = cache[k];
+        if (c == -1) return false;  // entries fill from the front
+        if (leaf_occluded(S, c, rp, tmin, tmax)) return true;
+    }
+    return false;
+}
+
+template <typename R, int W = 2, int WAYS = 1>
 MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, int *cache,
                            bool test_cached = true)
 {
-    const int c = *cache;
-    if (test_cached && c != -1 && leaf_occluded(S, c, rp, tmin, tmax)) {
+    const int c = cache[0];
+    if (test_cached && occ_ways_occluded<R, WAYS>(S, cache, rp, tmin, tmax)) {
         if (S.counters) count_add(&S.counters->any_prim_tests, 1ull);
         return true;
     }
@@ -943,7 +957,11 @@ MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R 
         }
     }
     trav_count_flush<R, true>(S, cnt);
-    if (tv.found && tv.any_leaf != -1 && tv.any_leaf != c) *cache = tv.any_leaf;
+    if (tv.found && tv.any_leaf != -1 && tv.any_leaf != c) {
+#pragma unroll
+        for (int k = WAYS - 1; k > 0; --k) cache[k] = cache[k - 1];
+        cache[0] = tv.any_leaf;
+    }
     return tv.found;
 }
 

@@ -150,8 +150,8 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
     WF_CK(cudaMalloc(&st->acc, wh * 3 * sizeof(R)), "cudaMalloc(acc)");
     WF_CK(cudaMalloc(&st->params, sizeof(WfParams<R>)), "cudaMalloc(params)");
     WF_CK(cudaMalloc((void **)&st->counters, sizeof(WfCounters)), "cudaMalloc(counters)");
-    WF_CK(cudaMalloc(&st->occ_cache, (wh * kNeeSlots + kOccHash) * sizeof(int)), "cudaMalloc(occluder cache)");
-    WF_CK(cudaMemset(st->occ_cache, 0xFF, (wh * kNeeSlots + kOccHash) * sizeof(int)), "cudaMemset(occluder cache)");
+    WF_CK(cudaMalloc(&st->occ_cache, occ_cache_ints(wh) * sizeof(int)), "cudaMalloc(occluder cache)");
+    WF_CK(cudaMemset(st->occ_cache, 0xFF, occ_cache_ints(wh) * sizeof(int)), "cudaMemset(occluder cache)");
     WF_CK(cudaMalloc(&st->walk, (nshadow ? nshadow : 1) * sizeof(int)), "cudaMalloc(shadow walk list)");
     if (!st->h_params) WF_CK(cudaMallocHost(&st->h_params, 256), "cudaMallocHost(params)");
     st->cap_paths = n_paths;

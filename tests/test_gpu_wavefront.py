@@ -182,3 +182,24 @@ def test_autotune_keeps_the_image(mtlib):
     assert rep["chosen"]["bvh_width"] in (2, 4, 8) and rep["chosen"]["block"] in (64, 128)
     assert torch.equal(_acc_image(g, cam, W, H, 4, DEPTH), ref)
     g.release()
+
+
+def test_warm_occluder_cache_keeps_the_image(mtlib):
+    """The occluder cache persists across calls on one scene, so a second
+    render of the same samples starts with every entry holding a blocking leaf
+    from the first; a hit there must give the same answer as the walk, so both
+    images are bit-identical (and equal to the cache-less dynamic-fetch kernels)."""
+    d = scenes.torus_field_scene(n_instances=256, area=30.0)
+    W, H, SPP, DEPTH = 120, 80, 4, 8
+    cam = d.make_camera(W, H)
+    g = mt.GpuScene(d, precision="fp32", integrator="wavefront")
+    cold = _acc_image(g, cam, W, H, SPP, DEPTH, s0=100)
+    warm = _acc_image(g, cam, W, H, SPP, DEPTH, s0=100)
+    other = _acc_image(g, cam, W, H, SPP, DEPTH, s0=200)  # different samples through the same entries
+    again = _acc_image(g, cam, W, H, SPP, DEPTH, s0=100)
+    g.release()
+    gd = mt.GpuScene(d, precision="fp32", integrator="wavefront", traversal=2)
+    nocache = _acc_image(gd, cam, W, H, SPP, DEPTH, s0=100)
+    gd.release()
+    assert torch.equal(cold, warm) and torch.equal(cold, again) and torch.equal(cold, nocache)
+    assert not torch.equal(cold, other)
