@@ -149,10 +149,10 @@ def build_scene():
 
 # DRAM bytes (read + write) per path sample of the stage kernels, from an ncu
 # launch list of this workload (4-spp frames, 2M-slot queue; summarised under
-# profiles/): the shadow stage (cache pass 20.59 + 3.63 GB, walk 17.63 + 3.98
-# GB) and the extend kernel (5.74 + 0.44 GB) over 7 frames of 4 x 2,073,600
+# profiles/): the shadow stage (cache pass 29.44 + 4.20 GB, walk 18.29 + 3.39
+# GB) and the extend kernel (5.73 + 0.43 GB) over 7 frames of 4 x 2,073,600
 # samples.
-TRAFFIC_BYTES_PER_SAMPLE = {"shadow": 45.84e9 / (7 * 4 * 2073600), "extend": 6.18e9 / (7 * 4 * 2073600)}
+TRAFFIC_BYTES_PER_SAMPLE = {"shadow": 55.32e9 / (7 * 4 * 2073600), "extend": 6.16e9 / (7 * 4 * 2073600)}
 
 
 def traversal_bytes(st, kind: str, width: int = 2) -> float:
