@@ -1007,25 +1007,17 @@ __global__ void k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_p
     adj_block_end(adj_g, A.P);
 }
 
+// Per pixel: each of its batch_spp paths finalised (finalize_path) and summed
+// in sample order, without a round trip through a per-sample buffer.
 template <typename R>
 __global__ void k_wf_reduce(const __grid_constant__ DevScene<R> S, const WfParams<R> *P, int batch_spp, int first_batch,
-                            int last_batch, const R *sample_buf, R *acc, const WfPath<R> *paths, R *nee)
+                            int last_batch, R *acc, const WfPath<R> *paths, R *nee)
 {
     const WfParams<R> p = *P;
     for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < p.wh; pix += gridDim.x * blockDim.x) {
         V3<R> a = v3(R(0), R(0), R(0));
         if (!first_batch) a = v3(acc[3 * (size_t)pix], acc[3 * (size_t)pix + 1], acc[3 * (size_t)pix + 2]);
-        for (int j = 0; j < batch_spp; ++j) {
-            const size_t q = (size_t)j * p.wh + pix;
-            if (paths) {
-                // fused with finalize: the same per-path radiance, summed in
-                // sample order without the round trip through sample_buf
-                a = add(a, finalize_path(S, paths, nee, q));
-            } else {
-                const R *sb = sample_buf + 3 * q;
-                a = add(a, v3(sb[0], sb[1], sb[2]));
-            }
-        }
+        for (int j = 0; j < batch_spp; ++j) a = add(a, finalize_path(S, paths, nee, (size_t)j * p.wh + pix));
         if (!last_batch) {
             acc[3 * (size_t)pix] = a.x;
             acc[3 * (size_t)pix + 1] = a.y;

@@ -146,7 +146,6 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
     WF_CK(cudaMemset(st->nee, 0, n_paths * kNeeSlots * 3 * sizeof(R)), "cudaMemset(nee)");
     st->nee_clean = true;
     WF_CK(cudaMalloc(&st->shadow, (nshadow ? nshadow : 1) * sizeof(WfShadow<R>)), "cudaMalloc(shadow)");
-    WF_CK(cudaMalloc(&st->sample_buf, n_paths * 3 * sizeof(R)), "cudaMalloc(samples)");
     WF_CK(cudaMalloc(&st->acc, wh * 3 * sizeof(R)), "cudaMalloc(acc)");
     WF_CK(cudaMalloc(&st->params, sizeof(WfParams<R>)), "cudaMalloc(params)");
     WF_CK(cudaMalloc((void **)&st->counters, sizeof(WfCounters)), "cudaMalloc(counters)");
@@ -162,9 +161,14 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
 // The adjoint replay's per-path buffers, sized to the reserved path slots.
 template <typename R> int wf_reserve_adj(WavefrontState *st)
 {
-    if (st->adj_verts) return 0;
-    WF_CK(cudaMalloc(&st->adj_verts, st->cap_paths * sizeof(AdjVertex<R>)), "cudaMalloc(adjoint vertices)");
-    WF_CK(cudaMalloc(&st->adj_att, st->cap_paths * kNeeSlots * kAttStride * sizeof(R)), "cudaMalloc(adjoint nee)");
+    // each buffer on its own, so that a failed allocation is retried next call
+    // each sample's primal radiance (k_wf_finalize), the replay's target
+    if (!st->sample_buf)
+        WF_CK(cudaMalloc(&st->sample_buf, st->cap_paths * 3 * sizeof(R)), "cudaMalloc(samples)");
+    if (!st->adj_verts)
+        WF_CK(cudaMalloc(&st->adj_verts, st->cap_paths * sizeof(AdjVertex<R>)), "cudaMalloc(adjoint vertices)");
+    if (!st->adj_att)
+        WF_CK(cudaMalloc(&st->adj_att, st->cap_paths * kNeeSlots * kAttStride * sizeof(R)), "cudaMalloc(adjoint nee)");
     return 0;
 }
 
@@ -359,7 +363,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             k_wf_finalize<R><<<g, block, 0, s>>>(S, n_paths, paths, nee, sample_buf);
         } else {
             // one thread per pixel finalises its batch_spp paths and sums them
-            k_wf_reduce<R><<<g, block, 0, s>>>(S, P, batch_spp, batch == 0, batch == n_batches - 1, nullptr, acc, paths, nee);
+            k_wf_reduce<R><<<g, block, 0, s>>>(S, P, batch_spp, batch == 0, batch == n_batches - 1, acc, paths, nee);
         }
         toc(3);
         if (adjoint) {
