@@ -929,11 +929,22 @@ template <typename R> MT_D bool leaf_occluded(const DevScene<R> &S, int node, co
 template <typename R, int WAYS>
 MT_D bool occ_ways_occluded(const DevScene<R> &S, const int *cache, const RayPre<R> &rp, R tmin, R tmax)
 {
+    int c[WAYS];
+    if constexpr (WAYS == 4) {
+        // a four-way entry is 16 bytes at a 16-byte boundary: one load
+        const int4 e = *reinterpret_cast<const int4 *>(cache);
+        c[0] = e.x;
+        c[1] = e.y;
+        c[2] = e.z;
+        c[3] = e.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < WAYS; ++k) c[k] = cache[k];
+    }
 #pragma unroll
     for (int k = 0; k < WAYS; ++k) {
-        const int c = cache[k];
-        if (c == -1) return false;  // entries fill from the front
-        if (leaf_occluded(S, c, rp, tmin, tmax)) return true;
+        if (c[k] == -1) return false;  // entries fill from the front
+        if (leaf_occluded(S, c[k], rp, tmin, tmax)) return true;
     }
     return false;
 }
@@ -958,9 +969,14 @@ MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R 
     }
     trav_count_flush<R, true>(S, cnt);
     if (tv.found && tv.any_leaf != -1 && tv.any_leaf != c) {
+        if constexpr (WAYS == 4) {
+            const int4 e = *reinterpret_cast<const int4 *>(cache);
+            *reinterpret_cast<int4 *>(cache) = make_int4(tv.any_leaf, e.x, e.y, e.z);
+        } else {
 #pragma unroll
-        for (int k = WAYS - 1; k > 0; --k) cache[k] = cache[k - 1];
-        cache[0] = tv.any_leaf;
+            for (int k = WAYS - 1; k > 0; --k) cache[k] = cache[k - 1];
+            cache[0] = tv.any_leaf;
+        }
     }
     return tv.found;
 }
