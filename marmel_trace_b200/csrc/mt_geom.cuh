@@ -918,14 +918,9 @@ template <typename R> MT_D bool leaf_occluded(const DevScene<R> &S, int node, co
     return false;
 }
 
-// Any hit that first tries the leaf in *cache (leaf_code, -1 none) -- a hit
-// there is a hit of the query, so the answer is the same -- and otherwise
-// walks the tree and leaves the blocking leaf in *cache. Caching the leaf
-// rather than the one primitive catches the neighbouring primitives of a
-// blocker, which nearby connections often meet instead.
-// test_cached = false: the caller has already tested *cache and it missed.
-// The entry holds the WAYS most recent blocking leaves, newest first; all are
-// tried before the walk (occ_ways_occluded).
+// Any hit among the leaves of an occluder-cache entry: WAYS leaf codes, newest
+// first, -1 for an empty way (entries fill from the front, and nothing but
+// leaf codes and -1 is ever stored).
 template <typename R, int WAYS>
 MT_D bool occ_ways_occluded(const DevScene<R> &S, const int *cache, const RayPre<R> &rp, R tmin, R tmax)
 {
@@ -949,6 +944,12 @@ MT_D bool occ_ways_occluded(const DevScene<R> &S, const int *cache, const RayPre
     return false;
 }
 
+// Any hit that first tries the leaves in the entry `cache` (occ_ways_occluded)
+// -- a hit there is a hit of the query, so the answer is the same -- and
+// otherwise walks the tree and pushes the blocking leaf to the front of the
+// entry. Caching leaves rather than single primitives catches the
+// neighbouring primitives of a blocker, which nearby connections often meet
+// instead. test_cached = false: the caller has already tested the entry.
 template <typename R, int W = 2, int WAYS = 1>
 MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, int *cache,
                            bool test_cached = true)
