@@ -921,6 +921,43 @@ template <typename R> MT_D bool leaf_occluded(const DevScene<R> &S, int node, co
 // Any hit among the leaves of an occluder-cache entry: WAYS leaf codes, newest
 // first, -1 for an empty way (entries fill from the front, and nothing but
 // leaf codes and -1 is ever stored).
+// Returns the way whose leaf blocks the ray, or -1. MOVE: a hit past the
+// first way moves that leaf to the front (the entry is only an ordered set of
+// candidates, so reordering it changes no answer).
+template <typename R, int WAYS, bool MOVE = false>
+MT_D int occ_ways_hit(const DevScene<R> &S, int *cache, const RayPre<R> &rp, R tmin, R tmax)
+{
+    int c[WAYS];
+    if constexpr (WAYS == 4) {
+        const int4 e = *reinterpret_cast<const int4 *>(cache);
+        c[0] = e.x;
+        c[1] = e.y;
+        c[2] = e.z;
+        c[3] = e.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < WAYS; ++k) c[k] = cache[k];
+    }
+#pragma unroll
+    for (int k = 0; k < WAYS; ++k) {
+        if (c[k] == -1) return -1;
+        if (leaf_occluded(S, c[k], rp, tmin, tmax)) {
+            if constexpr (MOVE && WAYS == 4) {
+                if (k > 0) {
+                    int4 m;
+                    m.x = c[k];
+                    m.y = c[0];
+                    m.z = k > 1 ? c[1] : c[2];
+                    m.w = k > 2 ? c[2] : c[3];
+                    *reinterpret_cast<int4 *>(cache) = m;
+                }
+            }
+            return k;
+        }
+    }
+    return -1;
+}
+
 template <typename R, int WAYS>
 MT_D bool occ_ways_occluded(const DevScene<R> &S, const int *cache, const RayPre<R> &rp, R tmin, R tmax)
 {

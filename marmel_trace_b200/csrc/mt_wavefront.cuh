@@ -704,7 +704,8 @@ __global__ void k_wf_sort_scatter(const WfCounters *C, int which, const WfRay<R>
 // leaves (a hit there is a hit of the any-hit query, so the answer cannot
 // change), resolves the blocked ones and appends the others to `walk`;
 // k_wf_shadow then walks the tree for `walk` only and pushes each blocking leaf
-// it finds to the front of the entry (scene_any_cached). Cache hits (a few
+// it finds to the front of the entry (scene_any_cached); a probe that hits a
+// later way moves that leaf to the front (occ_ways_hit). Cache hits (a few
 // primitive tests) and walks (the whole tree) therefore do not share warps.
 
 // Occluder cache entry of a connection. At bounce 0, per pixel and NEE slot:
@@ -831,9 +832,10 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const __grid_co
         if (q < n) {
             const WfShadow<R> s = sq[q];
             if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
-            const bool blocked = occ_ways_occluded<R, kOccWays>(
-                S, occ_entry(S, occ_cache, wh, b, s),
-                ray_pre(v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2]))), R(1e-3), s.tmax);
+            const bool blocked =
+                occ_ways_hit<R, kOccWays, true>(
+                    S, occ_entry(S, occ_cache, wh, b, s),
+                    ray_pre(v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2]))), R(1e-3), s.tmax) >= 0;
             if (blocked) {
                 if (S.counters) atomicAdd(&S.counters->any_prim_tests, 1ull);
                 shadow_result<R, ADJ>(s, true, v3(R(1), R(1), R(1)), ab, nee, att);
