@@ -42,6 +42,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -89,11 +90,14 @@ class ClockSampler:
     def __init__(self, device: int, tag: str = ""):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}{tag}.csv"
+        # the raw samples (MT_CLOCKS_DIR, else the system temp folder); the
+        # JSON line carries their summary
+        out = Path(os.environ.get("MT_CLOCKS_DIR") or tempfile.gettempdir())
+        self.path = out / f"clocks_{os.getpid()}{tag}.csv"
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
