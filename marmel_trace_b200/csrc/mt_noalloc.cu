@@ -10,17 +10,31 @@
 // queues and path state live in one fixed array owned by this file instead
 // of in buffers allocated on demand.
 //
-// The array (kScratchBytes, 12 MiB) is a file-scope __device__ variable, so
-// every GPU that loads the library holds it until the process exits, whether
-// or not this entry point is called. It bounds one call to kMaxPixels pixels
-// (one sample of every pixel per batch). Larger images are rejected with
-// MT_ERR_INVALID.
+// The array (kScratchBytes, 12 MiB) is a file-scope __device__ variable. A
+// GPU holds it from the moment this file's device code is loaded on it until
+// the process exits. CUDA loads modules lazily by default (CUDA 12.2 and
+// later), so that moment is the first call of this entry point on the device
+// (its cudaGetSymbolAddress), not the library's load; with
+// CUDA_MODULE_LOADING=EAGER it is the process's first CUDA call. A caller
+// whose pool later takes the whole device budget must therefore make one
+// call on each device (a warm-up) before the pool reserves its memory, or
+// run with CUDA_MODULE_LOADING=EAGER. If the array cannot be loaded, the
+// call returns MT_ERR_OOM with error text. The array bounds one call to
+// kMaxPixels pixels (one sample of every pixel per batch); larger images are
+// rejected with MT_ERR_INVALID.
 //
 // Host code cannot use the array's name as a device address (on the host it
 // names a host-side stand-in). The first call on each device therefore looks
 // up the array's device address with cudaGetSymbolAddress while that device
 // is current, and caches it. Make that first call on a device before
 // capturing any stream.
+//
+// The call's parameter block (camera, window, output) is written into the
+// array by a one-thread kernel that receives it by value, so no host buffer
+// has to outlive the call.
+//
+// Renders through this entry point are not counted by mt_set_counting /
+// mt_get_stats.
 //
 // All calls share the one array and it keeps the last call's contents. Every
 // value a call reads is written earlier by the same call: the queue counters
@@ -31,6 +45,8 @@
 #include <mutex>
 
 #include "mt_wavefront_host.cuh"
+
+void mt_set_last_error_text(const char *msg);
 
 namespace {
 
@@ -45,6 +61,16 @@ unsigned char *g_scratch_ptr[kMaxDevices] = {nullptr};
 int g_grid[kMaxDevices] = {0};
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Store the call's parameter block (passed by value in the launch) into the
+// scratch array.
+__global__ void k_noalloc_params(const mt::WfParams<float> p, mt::WfParams<float> *dst) { *dst = p; }
+
+int fail_text(int code, const char *msg)
+{
+    mt_set_last_error_text(msg);
+    return code;
+}
 
 // Carve the wavefront buffers for `n_paths` paths / `wh` pixels out of the
 // scratch array; returns the bytes used.
@@ -76,7 +102,6 @@ size_t carve(unsigned char *base, size_t n_paths, size_t wh, int light_count, mt
 const mt::DevScene<float> *mt_scene_dev_f32(const mt_scene *scene);
 int mt_scene_precision(const mt_scene *scene);
 int mt_scene_device(const mt_scene *scene);
-void mt_set_last_error_text(const char *msg);
 
 extern "C" int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_camera *cam, int width, int height,
                                                    int spp_begin, int spp_end, int max_depth, float *accum_dev,
@@ -96,8 +121,10 @@ extern "C" int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_cam
         return MT_ERR_UNSUPPORTED;
     }
     const int dev = mt_scene_device(scene);
-    if (dev < 0 || dev >= kMaxDevices) return MT_ERR_INVALID;
-    if (cudaSetDevice(dev) != cudaSuccess) return MT_ERR_NO_DEVICE;
+    if (dev < 0 || dev >= kMaxDevices)
+        return fail_text(MT_ERR_INVALID, "mt_render_accumulate_device_noalloc: device index out of range");
+    if (cudaSetDevice(dev) != cudaSuccess)
+        return fail_text(MT_ERR_NO_DEVICE, "mt_render_accumulate_device_noalloc: cudaSetDevice failed");
 
     const DevScene<float> &S = *mt_scene_dev_f32(scene);
     {
@@ -106,7 +133,11 @@ extern "C" int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_cam
         std::lock_guard<std::mutex> lock(g_setup_mutex);
         if (!g_scratch_ptr[dev]) {
             void *p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MT_ERR_LAUNCH;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();  // clear the (non-sticky) error of the failed lookup
+                return fail_text(MT_ERR_OOM, "mt_render_accumulate_device_noalloc: could not load the 12 MiB "
+                                             "scratch array on this device (device memory exhausted?)");
+            }
             int sms = 0, per_sm = 0;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_extend<float, 2>, 128,
@@ -118,7 +149,9 @@ extern "C" int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_cam
 
     const int wh = width * height;
     WavefrontState st;  // a view of the scratch array: nothing here is allocated
-    if (carve(g_scratch_ptr[dev], (size_t)wh, (size_t)wh, S.light_count, &st) > kScratchBytes) return MT_ERR_INVALID;
+    if (carve(g_scratch_ptr[dev], (size_t)wh, (size_t)wh, S.light_count, &st) > kScratchBytes)
+        return fail_text(MT_ERR_INVALID, "mt_render_accumulate_device_noalloc: the buffers of this image do not "
+                                         "fit the scratch array");
     st.grid = g_grid[dev];
 
     WfParams<float> hp;
@@ -141,8 +174,17 @@ extern "C" int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_cam
     hp.spp_window = spp_end - spp_begin;
     hp.out_kind = accumulate ? OUT_ADD_F32 : OUT_SUM_F32;
     cudaStream_t s = (cudaStream_t)stream;
-    // Pageable source: the copy is staged before cudaMemcpyAsync returns.
-    if (cudaMemcpyAsync(st.params, &hp, sizeof hp, cudaMemcpyHostToDevice, s) != cudaSuccess) return MT_ERR_LAUNCH;
+    k_noalloc_params<<<1, 1, 0, s>>>(hp, (WfParams<float> *)st.params);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::string msg = std::string("mt_render_accumulate_device_noalloc: parameter kernel: ") + cudaGetErrorString(e);
+        return fail_text(MT_ERR_LAUNCH, msg.c_str());
+    }
     // One sample of every pixel per batch: n_paths == pixels.
-    return wf_enqueue<float>(&st, S, width, height, 1, spp_end - spp_begin, max_depth, s, false, 128);
+    int rc = wf_enqueue<float>(&st, S, width, height, 1, spp_end - spp_begin, max_depth, s, false, 128);
+    if (rc) {
+        std::string msg = std::string("mt_render_accumulate_device_noalloc: ") + wavefront_last_error();
+        return fail_text(rc, msg.c_str());
+    }
+    return 0;
 }
