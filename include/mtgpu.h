@@ -236,6 +236,8 @@ typedef struct {
     int32_t device;          /* CUDA device ordinal                             */
     int32_t traversal;       /* wavefront traversal kernels: MT_TRAVERSAL_*     */
     int32_t bvh_builder;     /* MT_BVH_BUILDER_*                                */
+    int32_t occluder_cache;  /* wavefront shadow stage: 0 = library default (on),
+                                -1 = off (every connection walks the tree)      */
 } mt_options;
 
 /* Where the scene's BVH is built. Both run the reference's binned-SAH
@@ -363,14 +365,19 @@ int mt_render_accumulate_device(mt_scene *scene, const mt_camera *cam, int width
  * entry point has no counterpart in the reference.
  *
  * It allocates nothing. Its queues and path state live in one fixed 12 MiB
- * __device__ array inside the library, which every GPU that loads the library
- * holds until the process exits. Limits: width * height <= 16384 pixels per
- * call (MT_ERR_INVALID beyond), FP32 scenes only (MT_ERR_UNSUPPORTED). The
- * caller passes the scene, the camera and the device output buffer
- * `accum_dev` (width * height * 3 floats). The first call on a device looks
- * up the array's device address; make it before capturing any stream. All
- * calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.
+ * __device__ array inside the library. A GPU holds the array from the load of
+ * the library's module on it until the process exits; modules load lazily by
+ * default (CUDA 12.2 and later), so that is the first call of this entry point
+ * on the device. A caller whose pool later takes the whole device budget makes
+ * one call per device first (a warm-up), or runs with
+ * CUDA_MODULE_LOADING=EAGER; if the array cannot be loaded the call returns
+ * MT_ERR_OOM. Limits: width * height <= 16384 pixels per call (MT_ERR_INVALID
+ * beyond), FP32 scenes only (MT_ERR_UNSUPPORTED). The caller passes the scene,
+ * the camera and the device output buffer `accum_dev` (width * height * 3
+ * floats). The first call on a device looks up the array's device address;
+ * make it before capturing any stream. All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. Renders
+ * through this entry point are not counted by mt_set_counting.
  */
 int mt_render_accumulate_device_noalloc(mt_scene *scene, const mt_camera *cam, int width, int height,
                                         int spp_begin, int spp_end, int max_depth, float *accum_dev,
@@ -505,6 +512,31 @@ int mt_intersect(mt_scene *scene, int n, const double *origins, const double *di
 /* Batched any-hit test (scene_occluded, src/scene.c:777-811): 1 = blocked. */
 int mt_occluded(mt_scene *scene, int n, const double *origins, const double *dirs,
                 double tmin, double tmax, int32_t *occluded_out);
+
+/*
+ * Query log of the wavefront integrator (parity harness; no counterpart in the
+ * reference, whose traversal calls are plain function calls a test can make
+ * itself). While enabled, the FP32 wavefront stages record every traversal
+ * query they answer during path-traced renders of this scene: each extension
+ * ray with its nearest hit (scene_intersect over [1e-4, 1e30],
+ * src/pathtrace.c:829-834) and each shadow connection with its answer
+ * (pt_occluded_segment over [1e-3, tmax], src/pathtrace.c:504-532), whether
+ * the occluder cache or the tree walk answered it. A test then puts the same
+ * queries to the reference.
+ *
+ * mt_trace_log_enable keeps the first `capacity` records of later renders
+ * (capacity 0 turns the log off and frees it); it resets the count.
+ * mt_trace_log_read copies min(count, capacity) records of 12 floats:
+ *   o.xyz, d.xyz (unit), t, result, kind, bounce, light, 0
+ * kind 0 (extension): t = hit distance, result = prim index or -1;
+ * kind 1 (shadow): t = tmax, result = 1 when occluded, bounce (-1: not
+ * recorded), light = NEE slot (lights 0..7, 8 = the sun).
+ * result, kind, bounce and light are int32 bit patterns. *count receives the
+ * number of queries seen since the last enable (it may exceed capacity).
+ * FP32 scenes only (MT_ERR_UNSUPPORTED otherwise).
+ */
+int mt_trace_log_enable(mt_scene *scene, int32_t capacity);
+int mt_trace_log_read(mt_scene *scene, float *records, int32_t capacity, int64_t *count);
 
 /* Primary rays exactly as pt_render_pixel draws them (src/pathtrace.c:1057-1082):
  * for every (x, y, s), origin + direction (doubles, 6 per ray) in

@@ -170,6 +170,7 @@ class MtOptions(C.Structure):
         ("device", C.c_int32),
         ("traversal", C.c_int32),
         ("bvh_builder", C.c_int32),
+        ("occluder_cache", C.c_int32),
     ]
 
 
@@ -257,6 +258,8 @@ SIGNATURES = {
     "mt_whitted_trace": (I, [P, I, P, P, I, P, P]),
     "mt_intersect": (I, [P, I, P, P, D, D, P, P, P, P, P]),
     "mt_occluded": (I, [P, I, P, P, D, D, P]),
+    "mt_trace_log_enable": (I, [P, I]),
+    "mt_trace_log_read": (I, [P, P, I, P]),
     "mt_primary_rays": (I, [P, P, I, I, I, I, P]),
     "mt_scene_param_count": (I, [P]),
     "mt_scene_get_material_params": (I, [P, P, I]),

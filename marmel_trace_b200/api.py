@@ -331,6 +331,31 @@ class GpuScene:
         check(self.lib.mt_occluded(self.h, len(o), ptr(o), ptr(d), tmin, tmax, ptr(occ)), "mt_occluded")
         return occ
 
+    def trace_log_enable(self, capacity: int):
+        """Record the wavefront stages' traversal queries (mt_trace_log_enable)."""
+        check(self.lib.mt_trace_log_enable(self.h, int(capacity)), "mt_trace_log_enable")
+
+    def trace_log_read(self, capacity: int):
+        """(records, seen): the logged queries as a structured array with
+        fields o (3), d (3), t, result, kind, bounce, light, and the number of
+        queries seen since the log was enabled."""
+        raw = np.zeros((max(int(capacity), 1), 12), np.float32)
+        seen = C.c_int64()
+        check(self.lib.mt_trace_log_read(self.h, ptr(raw), int(capacity), C.byref(seen)), "mt_trace_log_read")
+        n = min(seen.value, int(capacity))
+        raw = raw[:n]
+        ints = raw.view(np.int32)
+        rec = np.zeros(n, dtype=[("o", np.float32, 3), ("d", np.float32, 3), ("t", np.float32), ("result", np.int32),
+                                 ("kind", np.int32), ("bounce", np.int32), ("light", np.int32)])
+        rec["o"] = raw[:, 0:3]
+        rec["d"] = raw[:, 3:6]
+        rec["t"] = raw[:, 6]
+        rec["result"] = ints[:, 7]
+        rec["kind"] = ints[:, 8]
+        rec["bounce"] = ints[:, 9]
+        rec["light"] = ints[:, 10]
+        return rec, seen.value
+
     def primary_rays(self, cam: Camera, w: int, h: int, spp: int, mode: str = "pathtrace") -> np.ndarray:
         out = np.zeros((h * w * spp, 6), np.float64)
         m = capi.MODE_PATHTRACE if mode == "pathtrace" else capi.MODE_WHITTED

@@ -95,6 +95,10 @@ struct mt_scene {
     unsigned *d_err = nullptr;
     DevCounters *d_counters = nullptr;
     bool counting = false;
+    // wavefront query log (mt_trace_log_enable): records and their count
+    float4 *d_trace = nullptr;
+    unsigned *d_trace_n = nullptr;
+    int trace_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     mt_stats stats;
     WavefrontState *wf = nullptr;
@@ -543,6 +547,9 @@ int render_dev(mt_scene *sc, const mt_camera *cam, int w, int h, int spp_total, 
     DevScene<R> S = dev_scene<R>(sc);
     S.counters = sc->counting ? sc->d_counters : nullptr;
     if (sc->opts.integrator == MT_INTEGRATOR_WAVEFRONT && mode == RENDER_PT) {
+        S.trace_rec = sc->d_trace;
+        S.trace_count = sc->d_trace_n;
+        S.trace_cap = sc->trace_cap;
         int rc = wavefront_render(sc->wf, S, dc, w, h, s0, s1, depth, out_kind, dout, stream, &sc->opts,
                                      timed ? sc->ev0 : nullptr, timed ? sc->ev1 : nullptr, &sc->stats.launches);
         if (rc) return fail(rc, "wavefront render failed: %s", wavefront_last_error());
@@ -727,6 +734,8 @@ void mt_scene_release(mt_scene *sc)
     cudaSetDevice(sc->opts.device);
     if (sc->wf) wavefront_destroy(sc->wf);
     for (void *p : sc->allocs) cudaFree(p);
+    if (sc->d_trace) cudaFree(sc->d_trace);
+    if (sc->d_trace_n) cudaFree(sc->d_trace_n);
     if (sc->ev0) cudaEventDestroy(sc->ev0);
     if (sc->ev1) cudaEventDestroy(sc->ev1);
     delete sc;
@@ -1238,6 +1247,45 @@ int mt_occluded(mt_scene *sc, int n, const double *o, const double *d, double tm
     CK(cudaDeviceSynchronize(), "occluded kernel");
     CK(cudaMemcpy(occ, dOcc.p, n * sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
     return check_err_word(sc);
+}
+
+int mt_trace_log_enable(mt_scene *sc, int32_t capacity)
+{
+    if (!sc) return fail(MT_ERR_NULL, "NULL pointer");
+    if (capacity < 0) return fail(MT_ERR_INVALID, "negative capacity");
+    if (sc->opts.precision != MT_PRECISION_FP32) return fail(MT_ERR_UNSUPPORTED, "the query log is FP32 only");
+    int rc = set_device(sc);
+    if (rc) return rc;
+    CK(cudaDeviceSynchronize(), "synchronize");
+    if (sc->d_trace) cudaFree(sc->d_trace);
+    if (sc->d_trace_n) cudaFree(sc->d_trace_n);
+    sc->d_trace = nullptr;
+    sc->d_trace_n = nullptr;
+    sc->trace_cap = 0;
+    if (capacity == 0) return 0;
+    CK(cudaMalloc((void **)&sc->d_trace, (size_t)capacity * 3 * sizeof(float4)), "cudaMalloc(query log)");
+    CK(cudaMalloc((void **)&sc->d_trace_n, sizeof(unsigned)), "cudaMalloc(query log count)");
+    CK(cudaMemset(sc->d_trace_n, 0, sizeof(unsigned)), "cudaMemset(query log count)");
+    sc->trace_cap = capacity;
+    return 0;
+}
+
+int mt_trace_log_read(mt_scene *sc, float *records, int32_t capacity, int64_t *count)
+{
+    if (!sc || !count) return fail(MT_ERR_NULL, "NULL pointer");
+    if (!sc->d_trace) return fail(MT_ERR_INVALID, "the query log is not enabled");
+    int rc = set_device(sc);
+    if (rc) return rc;
+    CK(cudaDeviceSynchronize(), "synchronize");
+    unsigned n = 0;
+    CK(cudaMemcpy(&n, sc->d_trace_n, sizeof n, cudaMemcpyDeviceToHost), "cudaMemcpy(query log count)");
+    *count = (int64_t)n;
+    int64_t keep = (int64_t)n < (int64_t)sc->trace_cap ? (int64_t)n : (int64_t)sc->trace_cap;
+    if (keep > capacity) keep = capacity;
+    if (keep > 0 && records)
+        CK(cudaMemcpy(records, sc->d_trace, (size_t)keep * 3 * sizeof(float4), cudaMemcpyDeviceToHost),
+           "cudaMemcpy(query log)");
+    return 0;
 }
 
 int mt_primary_rays(mt_scene *sc, const mt_camera *cam, int w, int h, int spp, int mode, double *out)

@@ -177,6 +177,11 @@ template <typename R> struct DevScene {
     DevLight<R> lights[kMaxLights];
     unsigned *err;               // device error word
     DevCounters *counters;       // NULL when counting is off
+    // Query log of the wavefront stages (mt_trace_log_enable; NULL when off):
+    // 3 float4 per query, appended at trace_count, the first trace_cap kept.
+    float4 *trace_rec;
+    unsigned *trace_count;
+    int trace_cap;
 };
 
 template <typename R> struct DevCamera {

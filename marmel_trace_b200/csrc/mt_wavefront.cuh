@@ -131,6 +131,24 @@ MT_D int warp_append(int *counter, bool want)
     return base + __popc(ballot & ((1u << lane) - 1u));
 }
 
+// Query log (mt_trace_log_enable): one record of 3 float4 per traversal
+// query the stages answer, so a test can put the same query to the oracle:
+//   (o.x, o.y, o.z, d.x) (d.y, d.z, t, result) (kind, bounce, light, 0)
+// kind 0: extension ray, t = hit distance, result = prim index (-1: miss);
+// kind 1: shadow connection over [1e-3, t = tmax], result = 1 if occluded.
+// result / kind / bounce / light are int bit patterns. Records past
+// trace_cap are counted but not kept.
+template <typename R>
+MT_D void trace_put(const DevScene<R> &S, V3<R> o, V3<R> d, R t, int result, int kind, int b, int li)
+{
+    const unsigned at = atomicAdd(S.trace_count, 1u);
+    if (at >= (unsigned)S.trace_cap) return;
+    float4 *r = S.trace_rec + 3 * (size_t)at;
+    r[0] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)d.x);
+    r[1] = make_float4((float)d.y, (float)d.z, (float)t, __int_as_float(result));
+    r[2] = make_float4(__int_as_float(kind), __int_as_float(b), __int_as_float(li), 0.0f);
+}
+
 // ------------------------------------------------------------------
 // generate: primary rays of a batch (pt_render_pixel, src/pathtrace.c:1053-1086)
 // ------------------------------------------------------------------
@@ -214,6 +232,7 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend(const __grid_constant
             out.code = 0;
         }
         hits[q] = out;
+        if (S.trace_rec) trace_put(S, o, d, out.t, out.prim, 0, 0, 0);
     }
     if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->extension_rays, (unsigned long long)n);
 }
@@ -811,13 +830,16 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? 7 : 1) k_wf_shadow(const
         // the sun through volumetric clouds (pt_nee_sun, src/pathtrace.c:545-546)
         if (!occ && s.li == kMaxLights) atten = scale(atten, cloud_transmittance(S.sky, o, d));
         shadow_result<R, ADJ>(s, occ, atten, ab, nee, att);
+        if (S.trace_rec) trace_put(S, o, unit_dir(d), s.tmax, occ ? 1 : 0, 1, b, s.li);
     }
 }
 
 // First pass of bounce 0 (scenes without pass-through materials): the cached
 // occluder of every connection; misses go to `walk` (warp-aggregated appends).
+// Held to 64 registers (8 blocks of 128 per SM), as it compiles without the
+// query log.
 template <typename R, bool ADJ>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq,
+__global__ void __launch_bounds__(kWfMaxBlock, 8) k_wf_shadow_cache(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq,
                                                          WfCounters *C, R *nee, R *att, int *occ_cache, int wh,
                                                          int b, int *walk)
 {
@@ -839,6 +861,9 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_cache(const __grid_co
             if (blocked) {
                 if (S.counters) atomicAdd(&S.counters->any_prim_tests, 1ull);
                 shadow_result<R, ADJ>(s, true, v3(R(1), R(1), R(1)), ab, nee, att);
+                if (S.trace_rec)
+                    trace_put(S, v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2])), s.tmax, 1, 1, b,
+                              s.li);
             } else {
                 miss = true;
             }
@@ -951,6 +976,9 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_shadow_dyn(const __grid_cons
                 ab.mat[0] = ab.mat[1] = -1;
                 ab.dist[0] = ab.dist[1] = R(0);
                 shadow_result<R, ADJ>(s, tv.found, atten, ab, nee, att);
+                if (S.trace_rec)
+                    trace_put(S, v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2])), s.tmax, tv.found ? 1 : 0, 1, -1,
+                              s.li);
                 q = -1;
             }
         }

@@ -432,6 +432,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     cudaStreamSynchronize(stream);  // the pinned block may still be in use by a previous copy
     memcpy(st->h_params, &hp, sizeof hp);
     WF_CK(cudaMemcpyAsync(st->params, st->h_params, sizeof hp, cudaMemcpyHostToDevice, stream), "params copy");
+    // the occluder cache can be switched off per scene (mt_options.occluder_cache)
+    st->occ_cache_on = !(opts && opts->occluder_cache < 0);
     // the bounce-0 shadow stage is two kernels when it uses the occluder cache
     const int cache_pass = st->occ_cache_on && st->occ_cache && st->walk && !S.has_passthrough &&
                            !(opts && opts->traversal == MT_TRAVERSAL_DYNAMIC);
@@ -447,9 +449,9 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         char key[256];
         // the scene travels by value in the captured kernel parameters, so
         // its identity, counters and parameter version are part of the key
-        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d:%d:%d:%d", (int)sizeof(R), w, h, batch_spp, n_batches,
-                 depth, (const void *)S.nodes, (const void *)S.counters, S.version, (int)dyn, block, sort_threshold,
-                 S.bvh_width);
+        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d:%d:%d:%d:%p:%d", (int)sizeof(R), w, h, batch_spp,
+                 n_batches, depth, (const void *)S.nodes, (const void *)S.counters, S.version, (int)dyn, block,
+                 sort_threshold, S.bvh_width, (const void *)S.trace_rec, (int)st->occ_cache_on);
         if (!exec || exec_key != key) {
             if (exec) cudaGraphExecDestroy(exec);
             exec = nullptr;

@@ -34,14 +34,14 @@ def clip_params(p: torch.Tensor, n_mat: int) -> torch.Tensor:
 
 
 def run(steps: int = 200, width: int = 512, height: int = 512, spp: int = 32, depth: int = 6, lr: float = 0.02,
-        seed: int = 4, target_spp: int = 256, log_every: int = 20) -> dict:
+        seed: int = 4, target_spp: int = 256, log_every: int = 20, device: int = 0) -> dict:
     d = scenes.adjoint_scene(seed=seed)
     n_mat = len(d.materials)
     truth = scenes.material_params(d)
-    tgt = DiffRenderer(d, width, height, target_spp, depth)
+    tgt = DiffRenderer(d, width, height, target_spp, depth, device=device)
     target = tgt.render(s0=10_000_000).detach()
     tgt.release()
-    r = DiffRenderer(d, width, height, spp, depth)
+    r = DiffRenderer(d, width, height, spp, depth, device=device)
     rng = np.random.default_rng(seed + 1000)
     p0 = truth + rng.normal(0.0, 0.15, truth.shape)
     params = clip_params(torch.tensor(p0, dtype=torch.float64, device="cuda"), n_mat).requires_grad_(True)

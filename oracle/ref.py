@@ -53,6 +53,8 @@ _SIG = {
     "mtref_whitted_linear": (I, [P, I, I, I, I, P, I]),
     "mtref_bvh_export": (I, [P, P, P, P, P, P, P, P, P]),
     "mtref_bvh_count": (I, [P, I, P, P, D, D, P, P, P]),
+    "mtref_queries": (I, [P, I, I, P, P, P, P, P, P, I]),
+    "mtref_bvh_count_batch": (I, [P, I, I, P, P, P, P, P, I]),
     "mtdual_param_count": (I, [P]),
     "mtdual_pathtrace_grad": (I, [P, I, I, I, I, I, P, D, P, I, P, P]),
 }
@@ -211,6 +213,23 @@ class RefScene:
         self.lib.mtref_occluded(self.h, len(o), _p(o), _p(d), tmin, tmax, _p(occ))
         return occ
 
+    def queries(self, kind, o, d, tmin, tmax, threads=None):
+        """Per-query bounds, threaded. kind "nearest": scene_intersect ->
+        (prim, t); kind "shadow": pt_occluded_segment -> (blocked, None)."""
+        o = np.ascontiguousarray(o, np.float64)
+        d = np.ascontiguousarray(d, np.float64)
+        n = len(o)
+        lo = np.ascontiguousarray(np.broadcast_to(np.asarray(tmin, np.float64), (n,)))
+        hi = np.ascontiguousarray(np.broadcast_to(np.asarray(tmax, np.float64), (n,)))
+        res = np.zeros(n, np.int32)
+        t = np.zeros(n) if kind == "nearest" else None
+        k = {"nearest": 0, "shadow": 1}[kind]
+        nt = threads or os.cpu_count() or 1
+        rc = self.lib.mtref_queries(self.h, k, n, _p(o), _p(d), _p(lo), _p(hi), _p(res), _p(t), nt)
+        if rc != 0:
+            raise RuntimeError(f"mtref_queries returned {rc}")
+        return res, t
+
     # -- renderers ----------------------------------------------------
     def pathtrace_render(self, w, h, spp, depth):
         out = np.zeros((h, w, 3), np.uint8)
@@ -296,6 +315,43 @@ class RefScene:
         np_, pt, lv = C.c_longlong(), C.c_longlong(), C.c_longlong()
         self.lib.mtref_bvh_count(self.h, len(o), _p(o), _p(d), tmin, tmax, C.byref(np_), C.byref(pt), C.byref(lv))
         return np_.value, pt.value, lv.value
+
+    def bvh_work(self, kind, o, d, tmin, tmax, threads=None):
+        """Canonical traversal work of the reference's tree over queries with
+        per-query bounds: (inner nodes with both child boxes tested, triangle
+        tests, other primitive tests). kind "nearest" (bvh_intersect) or
+        "any" (bvh_occluded without its last-occluder shortcut)."""
+        o = np.ascontiguousarray(o, np.float64)
+        d = np.ascontiguousarray(d, np.float64)
+        n = len(o)
+        lo = np.ascontiguousarray(np.broadcast_to(np.asarray(tmin, np.float64), (n,)))
+        hi = np.ascontiguousarray(np.broadcast_to(np.asarray(tmax, np.float64), (n,)))
+        out = np.zeros(3, np.int64)
+        nt = threads or os.cpu_count() or 1
+        rc = self.lib.mtref_bvh_count_batch(self.h, 1 if kind == "any" else 0, n, _p(o), _p(d), _p(lo), _p(hi),
+                                            _p(out), nt)
+        if rc != 0:
+            raise RuntimeError(f"mtref_bvh_count_batch returned {rc}")
+        return int(out[0]), int(out[1]), int(out[2])
+
+
+def camera_create(eye, target, up, vfov_deg: float, aspect: float):
+    """The reference's camera_create (src/camera.c:24-66), evaluated by the
+    oracle library (so that CPU-only callers never load libmtgpu)."""
+    from marmel_trace_b200 import _capi as capi
+    from marmel_trace_b200.api import Camera
+
+    lib = load()
+    out = capi.MtCamera()
+    e, t, u = (np.ascontiguousarray(v, dtype=np.float64) for v in (eye, target, up))
+    lib.mtref_camera_create(_p(e), _p(t), _p(u), float(vfov_deg), float(aspect), C.byref(out))
+    return Camera(out)
+
+
+def scene_camera(desc, width: int, height: int):
+    """The camera a scene descriptor's make_camera builds, from the oracle."""
+    c = desc.camera or dict(eye=(-18.0, 6.0, 22.0), target=(0.0, 5.0, -20.0), up=(0.0, 1.0, 0.0), vfov=40.0)
+    return camera_create(c["eye"], c["target"], c["up"], c["vfov"], width / height)
 
 
 def pt_hash3(a, b, c) -> int:

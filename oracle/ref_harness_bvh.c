@@ -143,3 +143,160 @@ int mtref_bvh_count(void *hp, int n, const double *o, const double *d, double tm
     if (leaf_visits) *leaf_visits = lv;
     return 0;
 }
+
+/*
+ * Canonical traversal work on the reference's tree for a batch of queries
+ * with per-query bounds, on `threads` threads: the nearest-hit walk of
+ * bvh_intersect (src/bvh.c:557-712) or the any-hit walk of bvh_occluded
+ * (src/bvh.c:714-813, without its last-occluder shortcut), both restated
+ * with counters. out[0] = inner nodes whose two child boxes were tested,
+ * out[1] = triangle tests, out[2] = other primitive tests (planes included).
+ * Used only for the algorithmic-bytes accounting of the roofline.
+ */
+#include <pthread.h>
+
+typedef struct {
+    const Scene *s;
+    int any, n;
+    const double *o, *d, *tmin, *tmax;
+    long long out[3];
+    int next;
+    pthread_mutex_t lock;
+} CountJob;
+
+static void count_prim(const Primitive *p, long long *c)
+{
+    if (p->kind == PRIM_TRIANGLE)
+        ++c[1];
+    else
+        ++c[2];
+}
+
+static void count_one(const Scene *s, int any, Ray r, double tmin, double tmax, long long *c)
+{
+    const Bvh *b = s->bvh;
+    const Geometry *g = &s->geo;
+    double len_sq = vec3_length_sq(r.dir);
+    if (len_sq > 0.0 && fabs(len_sq - 1.0) > 1e-12) r.dir = vec3_normalize(r.dir);
+    Vec3 inv = vec3(1.0 / r.dir.x, 1.0 / r.dir.y, 1.0 / r.dir.z);
+    int found = 0;
+    double closest = tmax;
+    Hit best;
+    best.t = 0.0;
+    best.prim_index = -1;
+    for (int i = 0; i < b->plane_count; ++i) {
+        int pi = b->planes[i];
+        count_prim(&g->prims[pi], c);
+        if (any) {
+            if (primitive_occluded(&g->prims[pi], r, tmin, tmax)) return;
+        } else {
+            Hit h;
+            h.prim_index = pi;
+            if (primitive_intersect(&g->prims[pi], r, tmin, closest, &h) &&
+                (!found || h.t < best.t || (h.t == best.t && h.prim_index < best.prim_index))) {
+                best = h;
+                closest = h.t;
+                found = 1;
+            }
+        }
+    }
+    if (b->node_count <= 0) return;
+    struct { int idx; double t; } stack[512];
+    int sp = 0;
+    BvhRaySimd rs;
+    bvh_ray_simd_init(&rs, r.origin, inv);
+    double t_root;
+    if (bvh_slab(b->nodes[0].bounds_min, b->nodes[0].bounds_max, r.origin, inv, tmin, closest, &t_root)) {
+        stack[sp].idx = 0;
+        stack[sp].t = t_root;
+        ++sp;
+    }
+    while (sp > 0) {
+        --sp;
+        if (!any && found && stack[sp].t > closest) continue;
+        const BvhNode *node = &b->nodes[stack[sp].idx];
+        if (node->count > 0) {
+            for (int i = 0; i < node->count; ++i) {
+                int pi = b->order[node->first + i];
+                count_prim(&g->prims[pi], c);
+                if (any) {
+                    if (primitive_occluded_norm(&g->prims[pi], r, tmin, tmax)) return;
+                } else {
+                    Hit h;
+                    h.prim_index = pi;
+                    if (primitive_intersect_norm(&g->prims[pi], r, tmin, closest, &h) &&
+                        (!found || h.t < best.t || (h.t == best.t && h.prim_index < best.prim_index))) {
+                        best = h;
+                        closest = h.t;
+                        found = 1;
+                    }
+                }
+            }
+        } else {
+            double tl = 0.0, tr = 0.0;
+            int hl = 0, hr = 0;
+            ++c[0];
+            bvh_slab_2way(&b->nodes[node->left], &b->nodes[node->right], &rs, tmin, closest, &tl, &tr, &hl,
+                          &hr);
+            if (sp + 2 > 512) return;
+            if (hl && hr) {
+                int first = tl <= tr ? node->right : node->left, second = tl <= tr ? node->left : node->right;
+                double tf = tl <= tr ? tr : tl, ts = tl <= tr ? tl : tr;
+                stack[sp].idx = first; stack[sp].t = tf; ++sp;
+                stack[sp].idx = second; stack[sp].t = ts; ++sp;
+            } else if (hl) {
+                stack[sp].idx = node->left; stack[sp].t = tl; ++sp;
+            } else if (hr) {
+                stack[sp].idx = node->right; stack[sp].t = tr; ++sp;
+            }
+        }
+    }
+}
+
+static void *count_worker(void *arg)
+{
+    CountJob *J = (CountJob *)arg;
+    long long c[3] = {0, 0, 0};
+    const int chunk = 1024;
+    for (;;) {
+        int i0;
+        pthread_mutex_lock(&J->lock);
+        i0 = J->next;
+        J->next += chunk;
+        pthread_mutex_unlock(&J->lock);
+        if (i0 >= J->n) break;
+        int i1 = i0 + chunk < J->n ? i0 + chunk : J->n;
+        for (int i = i0; i < i1; ++i) {
+            Ray r;
+            r.origin = vec3(J->o[3 * i], J->o[3 * i + 1], J->o[3 * i + 2]);
+            r.dir = vec3(J->d[3 * i], J->d[3 * i + 1], J->d[3 * i + 2]);
+            count_one(J->s, J->any, r, J->tmin[i], J->tmax[i], c);
+        }
+    }
+    pthread_mutex_lock(&J->lock);
+    for (int k = 0; k < 3; ++k) J->out[k] += c[k];
+    pthread_mutex_unlock(&J->lock);
+    return NULL;
+}
+
+int mtref_bvh_count_batch(void *hp, int any, int n, const double *o, const double *d, const double *tmin,
+                          const double *tmax, long long *out3, int threads)
+{
+    CountJob J;
+    pthread_t tids[256];
+    int nt = threads > 0 ? threads : 1;
+    if (nt > 256) nt = 256;
+    J.s = &((MtRefHandle *)hp)->scene;
+    if (!J.s->bvh) return 1;
+    J.any = any;
+    J.n = n;
+    J.o = o; J.d = d; J.tmin = tmin; J.tmax = tmax;
+    J.out[0] = J.out[1] = J.out[2] = 0;
+    J.next = 0;
+    pthread_mutex_init(&J.lock, NULL);
+    for (int i = 0; i < nt; ++i) pthread_create(&tids[i], NULL, count_worker, &J);
+    for (int i = 0; i < nt; ++i) pthread_join(tids[i], NULL);
+    pthread_mutex_destroy(&J.lock);
+    for (int k = 0; k < 3; ++k) out3[k] = J.out[k];
+    return 0;
+}

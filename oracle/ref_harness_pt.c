@@ -132,3 +132,77 @@ int mtref_pathtrace_linear(void *hp, int w, int h, int s0, int spp, int depth, d
     pthread_mutex_destroy(&J.lock);
     return 0;
 }
+
+/*
+ * Batched traversal queries with per-query bounds, on `threads` threads, for
+ * checking logged device queries one by one:
+ *   kind 0: scene_intersect over [tmin[i], tmax[i]] (src/scene.c:767-775):
+ *           result = prim_index (-1: miss), t_out = hit distance;
+ *   kind 1: pt_occluded_segment over [tmin[i], tmax[i]] (src/pathtrace.c:504-532),
+ *           the path tracer's shadow query: result = 1 when blocked.
+ */
+typedef struct {
+    MtRefHandle *H;
+    int kind, n;
+    const double *o, *d, *tmin, *tmax;
+    int *result;
+    double *t_out;
+    int next;
+    pthread_mutex_t lock;
+} QueryJob;
+
+static void *mtref_query_worker(void *arg)
+{
+    QueryJob *J = (QueryJob *)arg;
+    const int chunk = 1024;
+    for (;;) {
+        int i0;
+        pthread_mutex_lock(&J->lock);
+        i0 = J->next;
+        J->next += chunk;
+        pthread_mutex_unlock(&J->lock);
+        if (i0 >= J->n) break;
+        int i1 = i0 + chunk < J->n ? i0 + chunk : J->n;
+        for (int i = i0; i < i1; ++i) {
+            Ray r;
+            r.origin = vec3(J->o[3 * i], J->o[3 * i + 1], J->o[3 * i + 2]);
+            r.dir = vec3(J->d[3 * i], J->d[3 * i + 1], J->d[3 * i + 2]);
+            if (J->kind == 0) {
+                Hit h;
+                if (scene_intersect(&J->H->scene, r, J->tmin[i], J->tmax[i], &h)) {
+                    J->result[i] = h.prim_index;
+                    if (J->t_out) J->t_out[i] = h.t;
+                } else {
+                    J->result[i] = -1;
+                    if (J->t_out) J->t_out[i] = 0.0;
+                }
+            } else {
+                Vec3 att;
+                J->result[i] = pt_occluded_segment(&J->H->scene, r, J->tmin[i], J->tmax[i], &att);
+            }
+        }
+    }
+    return NULL;
+}
+
+int mtref_queries(void *hp, int kind, int n, const double *o, const double *d, const double *tmin,
+                  const double *tmax, int *result, double *t_out, int threads)
+{
+    QueryJob J;
+    pthread_t tids[256];
+    int nt = threads > 0 ? threads : 1;
+    if (nt > 256) nt = 256;
+    if (kind != 0 && kind != 1) return 1;
+    J.H = (MtRefHandle *)hp;
+    J.kind = kind;
+    J.n = n;
+    J.o = o; J.d = d; J.tmin = tmin; J.tmax = tmax;
+    J.result = result;
+    J.t_out = t_out;
+    J.next = 0;
+    pthread_mutex_init(&J.lock, NULL);
+    for (int i = 0; i < nt; ++i) pthread_create(&tids[i], NULL, mtref_query_worker, &J);
+    for (int i = 0; i < nt; ++i) pthread_join(tids[i], NULL);
+    pthread_mutex_destroy(&J.lock);
+    return 0;
+}

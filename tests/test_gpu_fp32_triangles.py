@@ -1,0 +1,290 @@
+"""Parity of the production FP32 path on the benchmarked triangle scene.
+
+The torus field (4096 instances of a 256-triangle torus, 1,048,576
+triangles, 8 emissive spheres, a plane; seed 2) is the scene the benchmark
+times. Its FP32 path uses the watertight triangle test, FP32 slab tests and,
+in the wavefront, the occluder cache, none of which the FP64 instantiation
+shares, so each is compared here with the oracle (the reference renderer):
+
+* nearest hits of primary rays (mt_intersect): prim ids equal outside the
+  FP32 ambiguity band (tests/_band.py) on >= 99.95 % of rays, the excluded
+  count reported; t within 1e-5 relative where the prims agree;
+* every traversal query the FP32 wavefront answers while rendering
+  (extension rays and shadow connections, logged by mt_trace_log_*), with
+  the occluder cache cold and warm, against scene_intersect and
+  pt_occluded_segment (src/scene.c:767-775, src/pathtrace.c:504-532);
+* mt_occluded on segments between surface points and toward the lights;
+* the FP32 wavefront image within 3 standard errors per pixel of a
+  converged image that is itself checked against the oracle;
+* the FP32 Whitted image within 1/255 on >= 99.9 % of channels;
+* the drop-in CLI in its default configuration (FP32 wavefront) against
+  the reference CLI.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+import torch
+
+import marmel_trace_b200 as mt
+from marmel_trace_b200 import _capi, scenes
+
+from _band import classify_nearest, classify_shadow
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def field():
+    return scenes.torus_field_scene()
+
+
+@pytest.fixture(scope="module")
+def field_ref(oracle, field):
+    rs = oracle.RefScene.from_desc(field, field.make_camera(192, 108))
+    yield rs
+    rs.free()
+
+
+def _report(name, differ, in_band):
+    n = len(differ)
+    out = int((differ & ~in_band).sum())
+    print(f"{name}: {n} queries, {int(differ.sum())} differ, {int(in_band.sum())} of them in the FP32 band, "
+          f"{out} outside it")
+    return out
+
+
+def test_primary_hits_fp32_triangles(field, field_ref, mtlib):
+    w, h, spp = 192, 108, 2
+    rays = field_ref.primary_rays(w, h, spp)
+    o, d = rays[:, :3], rays[:, 3:]
+    rp, rt, *_ = field_ref.intersect(o, d, 1e-4, 1e30)
+    with mt.GpuScene(field, precision="fp32") as g:
+        gp, gt, *_ = g.intersect(o, d, 1e-4, 1e30)
+    differ, band = classify_nearest(field_ref, field, o, d, 1e-4, 1e30, gp, rp, rt)
+    out = _report("primary hits", differ, band)
+    assert (rp >= 0).mean() > 0.5
+    assert out <= 5e-4 * (~band).sum(), f"{out} prim ids differ outside the FP32 band"
+    same = (gp == rp) & (rp >= 0)
+    rel = np.abs(gt[same] - rt[same]) / np.abs(rt[same])
+    print(f"primary hits: t max rel err {rel.max():.3g}, 99.99th pct {np.quantile(rel, 0.9999):.3g}")
+    assert rel.max() < 1e-5
+
+
+def _log_render(g, cam, w, h, s0, s1, depth, cap):
+    g.trace_log_enable(cap)
+    acc = torch.zeros((h, w, 3), dtype=torch.float32, device="cuda")
+    _capi.check(g.lib.mt_render_accumulate_device(g.h, cam.ref, w, h, s0, s1, depth, 0, acc.data_ptr(), 0, None),
+                "mt_render_accumulate_device")
+    torch.cuda.synchronize()
+    rec, seen = g.trace_log_read(cap)
+    assert seen <= cap, f"log overflow: {seen} queries for {cap} records"
+    return rec, acc.cpu().numpy()
+
+
+def _check_log(rs, desc, rec, tag, rng, max_queries=1_500_000):
+    o = rec["o"].astype(np.float64)
+    d = rec["d"].astype(np.float64)
+    ext = rec["kind"] == 0
+    shd = rec["kind"] == 1
+    # extension rays
+    ie = np.flatnonzero(ext)
+    if len(ie) > max_queries:
+        ie = np.sort(rng.choice(ie, max_queries, replace=False))
+    want, wt = rs.queries("nearest", o[ie], d[ie], 1e-4, 1e30)
+    got = rec["result"][ie]
+    differ, band = classify_nearest(rs, desc, o[ie], d[ie], 1e-4, 1e30, got, want, wt)
+    out_e = _report(f"{tag} extension rays", differ, band)
+    same = (got == want) & (want >= 0)
+    rel = np.abs(rec["t"][ie][same] - wt[same]) / np.abs(wt[same])
+    print(f"{tag} extension rays: t rel err 99.99th pct {np.quantile(rel, 0.9999):.3g}, max {rel.max():.3g}")
+    # shadow connections
+    js = np.flatnonzero(shd)
+    if len(js) > max_queries:
+        js = np.sort(rng.choice(js, max_queries, replace=False))
+    tmax = rec["t"][js].astype(np.float64)
+    want_s, _ = rs.queries("shadow", o[js], d[js], 1e-3, tmax)
+    got_s = rec["result"][js]
+    differ_s, band_s = classify_shadow(rs, o[js], d[js], 1e-3, tmax, got_s, want_s)
+    out_s = _report(f"{tag} shadow connections", differ_s, band_s)
+    for b in range(0, 9):
+        sel = rec["bounce"][js] == b
+        if sel.any():
+            print(f"  bounce {b}: {int(sel.sum())} connections, {want_s[sel].mean():.3f} blocked, "
+                  f"{int(differ_s[sel].sum())} differ ({int((differ_s & ~band_s)[sel].sum())} outside the band)")
+    return (len(ie), out_e, (~band).sum(), rel), (len(js), out_s, (~band_s).sum())
+
+
+@pytest.mark.parametrize("sort", [0, 1], ids=["unsorted", "sorted"])
+def test_wavefront_queries_fp32_match_oracle(field, field_ref, mtlib, sort):
+    """Every extension ray and shadow connection of a FP32 wavefront render,
+    first with a cold occluder cache, then the same samples again with the
+    cache warm, answered as the oracle answers them."""
+    w, h, spp, depth = 128, 72, 4, 8
+    cam = field.make_camera(w, h)
+    rng = np.random.default_rng(5)
+    cap = 6_000_000
+    with mt.GpuScene(field, precision="fp32", integrator="wavefront", sort_threshold=sort) as g:
+        cold, img_cold = _log_render(g, cam, w, h, 0, spp, depth, cap)
+        warm, img_warm = _log_render(g, cam, w, h, 0, spp, depth, cap)
+        g.trace_log_enable(0)
+    assert np.array_equal(img_cold, img_warm)
+    for tag, rec in (("cold cache", cold), ("warm cache", warm)):
+        (ne, oe, nbe, rel), (ns, os_, nbs) = _check_log(field_ref, field, rec, tag, rng)
+        assert ne > 10_000 and ns > 10_000
+        assert oe <= 5e-4 * nbe, f"{tag}: {oe} extension hits differ outside the FP32 band"
+        assert os_ <= 5e-4 * nbs, f"{tag}: {os_} shadow answers differ outside the FP32 band"
+        assert np.quantile(rel, 0.9999) < 1e-5
+
+
+def test_occluded_fp32_triangles(field, field_ref, mtlib):
+    """mt_occluded against scene_occluded on segments between surface points
+    of the field and from surface points toward the eight lights."""
+    w, h = 96, 54
+    rays = field_ref.primary_rays(w, h, 1)
+    rp, rt, rn, *_ = field_ref.intersect(rays[:, :3], rays[:, 3:], 1e-4, 1e30)
+    hit = rp >= 0
+    pts = rays[hit, :3] + rays[hit, 3:] * rt[hit, None] + 1e-4 * rn[hit]
+    rng = np.random.default_rng(11)
+    a = pts[rng.integers(0, len(pts), 20000)]
+    b = pts[rng.integers(0, len(pts), 20000)]
+    seg = b - a
+    dist = np.linalg.norm(seg, axis=1)
+    keep = dist > 1e-2
+    a, seg, dist = a[keep], seg[keep], dist[keep]
+    dirs = seg / dist[:, None]
+    lights = field.prims[field.prims["kind"] == _capi.PRIM_SPHERE]["v"][:, :3]
+    la = pts[rng.integers(0, len(pts), 8000)]
+    lc = lights[rng.integers(0, len(lights), 8000)]
+    ld = lc - la
+    ldist = np.linalg.norm(ld, axis=1)
+    o = np.concatenate([a, la])
+    d = np.concatenate([dirs, ld / ldist[:, None]])
+    tmax = np.concatenate([dist - 1e-3, ldist - 0.5 - 1e-3])
+    want = np.zeros(len(o), np.int32)
+    got = np.zeros(len(o), np.int32)
+    # mt_occluded and the oracle take one tmax per call: group by rounding
+    # is not exact, so query one tmax at a time in vectorised chunks
+    order = np.argsort(tmax)
+    with mt.GpuScene(field, precision="fp32") as g:
+        for chunk in np.array_split(order, 64):
+            tm = float(tmax[chunk].min())
+            got[chunk] = g.occluded(o[chunk], d[chunk], 1e-3, tm)
+            want[chunk] = field_ref.occluded(o[chunk], d[chunk], 1e-3, tm)
+            tmax[chunk] = tm
+    differ, band = classify_shadow(field_ref, o, d, 1e-3, tmax, got, want)
+    out = _report("mt_occluded", differ, band)
+    assert 0.05 < want.mean() < 0.95
+    assert out <= 5e-4 * (~band).sum()
+
+
+W3, H3, DEPTH3 = 48, 27, 8
+
+
+@pytest.fixture(scope="module")
+def converged_field(mtlib, field):
+    """16,384-spp FP64 wavefront image of the torus field at 48x27."""
+    cam = field.make_camera(W3, H3)
+    with mt.GpuScene(field, precision="fp64", integrator="wavefront") as g:
+        img = g.linear(cam, W3, H3, 16384, DEPTH3).astype(np.float64)
+    return cam, img
+
+
+def _within_3se(est, se, truth, floor=1e-6):
+    z = np.abs(est - truth) / np.maximum(se, floor)
+    return (z <= 3.0).mean(), float(np.median(z))
+
+
+def test_converged_field_agrees_with_oracle(field, field_ref, converged_field):
+    cam, conv = converged_field
+    field_ref.set_camera(cam)
+    wins = np.stack([field_ref.pathtrace_linear(W3, H3, 64, DEPTH3, s0=40000 + 64 * k) for k in range(16)])
+    mean = wins.mean(0)
+    se = wins.std(0, ddof=1) / np.sqrt(len(wins))
+    frac, med = _within_3se(mean, se, conv)
+    print(f"oracle 1024 spp vs converged FP64: {frac:.4f} of channels within 3 SE (median z {med:.3f})")
+    assert frac >= 0.98, f"only {frac:.4f} of channels within 3 SE (median z {med:.3f})"
+
+
+def test_fp32_wavefront_field_within_3se(field, converged_field):
+    cam, conv = converged_field
+    acc = torch.zeros((H3, W3, 3), dtype=torch.float32, device="cuda")
+    wins = []
+    with mt.GpuScene(field, precision="fp32", integrator="wavefront") as g:
+        for k in range(16):
+            s0 = 100000 + 64 * k
+            _capi.check(g.lib.mt_render_accumulate_device(g.h, cam.ref, W3, H3, s0, s0 + 64, DEPTH3, 0,
+                                                          acc.data_ptr(), 0, None), "mt_render_accumulate_device")
+            torch.cuda.synchronize()
+            wins.append(acc.cpu().numpy().astype(np.float64) / 64)
+    wins = np.stack(wins)
+    mean = wins.mean(0)
+    se = wins.std(0, ddof=1) / np.sqrt(len(wins))
+    frac, med = _within_3se(mean, se, conv)
+    rmse64 = float(np.sqrt(np.mean((wins[0] - conv) ** 2)))
+    rmse1k = float(np.sqrt(np.mean((mean - conv) ** 2)))
+    print(f"FP32 wavefront 1024 spp vs converged: {frac:.4f} within 3 SE (median z {med:.3f}); "
+          f"RMSE 64 spp {rmse64:.5f}, 1024 spp {rmse1k:.5f}")
+    assert frac >= 0.98, f"only {frac:.4f} of channels within 3 SE (median z {med:.3f})"
+    assert 2.0 < rmse64 / rmse1k < 8.0  # ideal sqrt(16) = 4
+
+
+def test_whitted_fp32_triangles_within_one_level(field, field_ref, mtlib):
+    w, h, spp, depth = 160, 90, 4, 4
+    cam = field.make_camera(w, h)
+    field_ref.set_camera(cam)
+    want = field_ref.whitted_render(w, h, spp, depth)
+    with mt.GpuScene(field, precision="fp32") as g:
+        got = g.whitted(cam, w, h, spp, depth)
+    diff = np.abs(got.astype(int) - want.astype(int))
+    frac = (diff <= 1).mean()
+    print(f"Whitted FP32 torus field: {frac:.5f} of channels within 1/255, max diff {diff.max()}")
+    assert frac >= 0.999, f"only {frac:.5f} of channels within 1/255"
+
+
+def _cli(oracle, binary, tmp_path, args, env_extra, name):
+    exe = oracle.HERE / "_ref" / binary
+    if not exe.exists():
+        pytest.skip(f"{exe} not built")
+    out = tmp_path / name
+    env = dict(os.environ, RAYTRACER_NO_PROGRESS="1", **env_extra)
+    subprocess.run([str(exe), *args, "--out", str(out)], check=True, env=env, stdout=subprocess.DEVNULL)
+    return out
+
+
+def _bmp_rgb(path):
+    data = path.read_bytes()
+    off = int.from_bytes(data[10:14], "little")
+    w = int.from_bytes(data[18:22], "little", signed=True)
+    h = int.from_bytes(data[22:26], "little", signed=True)
+    row = (w * 3 + 3) & ~3
+    px = np.frombuffer(data, np.uint8, count=row * abs(h), offset=off).reshape(abs(h), row)[:, : w * 3]
+    img = px.reshape(abs(h), w, 3)[:, :, ::-1]
+    return img[::-1] if h > 0 else img
+
+
+@pytest.mark.parametrize("scene", ["default", "torus"])
+def test_dropin_cli_default_fp32_matches_reference(oracle, mtlib, tmp_path, scene):
+    """The relinked CLI with no environment override (FP32 wavefront path
+    tracer) against the reference CLI on the same frame. Both draw the same
+    random streams, so most samples take identical paths; FP32 rounding moves
+    a few paths onto others. Criteria: the mean of the decoded linear images
+    agrees within 1 %, and >= 99 % of channels are within 2/255."""
+    args = ["--width", "160", "--height", "90", "--samples", "16", "--depth", "6"]
+    if scene == "torus":
+        d = scenes.torus_field_scene(n_instances=512, area=40.0)
+        sf = tmp_path / "torus.scene"
+        sf.write_text(scenes.to_scene_text(d))
+        args += ["--scene", str(sf)]
+    gpu = _bmp_rgb(_cli(oracle, "raytracer_gpu", tmp_path, args, {}, "gpu.bmp")).astype(np.float64)
+    cpu = _bmp_rgb(_cli(oracle, "raytracer", tmp_path, args, {}, "cpu.bmp")).astype(np.float64)
+    assert gpu.shape == cpu.shape == (90, 160, 3)
+    lin_g = (gpu / 255.0) ** 2.2
+    lin_c = (cpu / 255.0) ** 2.2
+    rel = abs(lin_g.mean() - lin_c.mean()) / lin_c.mean()
+    within = (np.abs(gpu - cpu) <= 2).mean()
+    print(f"CLI {scene}: mean linear {lin_g.mean():.5f} vs {lin_c.mean():.5f} (rel {rel:.4f}), "
+          f"{within:.4f} of channels within 2/255, {(gpu == cpu).mean():.4f} equal")
+    assert rel < 0.01
+    assert within >= 0.99
