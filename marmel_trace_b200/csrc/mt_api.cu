@@ -408,6 +408,15 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     S->has_extras = d->fog_density > 0.0 || d->fog_shadow_steps > 0 || d->sky.cloud_thickness > 1e-4;
     for (int i = 0; i < d->material_count; ++i)
         if (d->materials[i].texture_kind != MT_TEXTURE_NONE) S->has_extras = 1;
+    // a scene of PBR surfaces only: no path enters a medium or takes the
+    // legacy BSDF (the wavefront's specialised shade kernel)
+    S->pbr_only = !S->has_extras && !S->has_passthrough && d->water_material < 0;
+    for (int i = 0; i < d->material_count; ++i) {
+        const mt_material &m = d->materials[i];
+        if (!m.pbr || m.is_water || m.beer_lambert || m.atmosphere_glow[0] != 0.0 || m.atmosphere_glow[1] != 0.0 ||
+            m.atmosphere_glow[2] != 0.0)
+            S->pbr_only = 0;
+    }
     S->water_level = (R)d->water_level;
     S->ocean.enabled = d->ocean.enabled;
     S->ocean.seed = d->ocean.seed;

@@ -166,6 +166,7 @@ template <typename R> struct DevScene {
     int water_material;
     int has_passthrough;   // some material lets shadow rays through (water, transparency > 0.8)
     int has_extras;        // fog, marched media, volumetric clouds or a textured material
+    int pbr_only;          // every material PBR, no water / media / atmosphere glow, no extras
     int stack_depth;       // traversal stack entries per thread (dynamic shared memory)
     int bvh_width;         // 2, or 4 / 8 when `wnodes` is present
     int wide_stack_depth;  // stack entries per thread for the wide tree

@@ -283,7 +283,13 @@ MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> 
 // The FP32 forward kernel is held to 7 blocks of 128 per SM (72 registers):
 // left alone the compiler takes 79 and the SM runs 6 blocks, which measured
 // 22.2 vs 27.0 ms of shading per 16-spp torus-field frame.
-template <typename R, bool ADJ, bool EXTRAS>
+//
+// PBR: every material of the scene is a PBR surface without water, media or
+// atmosphere glow (DevScene::pbr_only). Such a path never enters a medium and
+// never takes the legacy BSDF, so those branches compile out and the kernel's
+// code (and its instruction-cache footprint) shrinks; the arithmetic of the
+// remaining branches is unchanged.
+template <typename R, bool ADJ, bool EXTRAS, bool PBR = false>
 __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRAS) ? 7 : 0) k_wf_shade(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
                                                   WfCounters *C, int which, int b, int max_depth, WfPath<R> *paths,
                                                   R *nee, WfRay<R> *rays_out, WfShadow<R> *sq, WfAdj<R> A,
@@ -342,7 +348,7 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
             if (hh.prim < 0) {
                 // escaped: medium fallback depth then the sky, through the fog
                 // (src/pathtrace.c:837-857)
-                if (st.medium >= 0) {
+                if (!PBR && st.medium >= 0) {
                     const V3<R> beta_in = throughput;
                     if constexpr (EXTRAS)
                         pt_water_segment(S, st.medium, ro, d, R(5.0), st.seed_key, b, &throughput, &radiance);
@@ -371,7 +377,7 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
                 th.code = hh.code;
                 SurfaceHit<R> h;
                 finish_hit(S, ro, unit_dir(d), th, &h);
-                if (st.medium >= 0) {
+                if (!PBR && st.medium >= 0) {
                     const V3<R> beta_in = throughput;
                     if constexpr (EXTRAS)
                         pt_water_segment(S, st.medium, ro, d, h.t, st.seed_key, b, &throughput, &radiance);
@@ -403,7 +409,7 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
                     }
                     P = h.point;
                     N = h.normal;
-                    if (m.is_water) {
+                    if (!PBR && m.is_water) {
                         if (mfabs(h.normal.y) > R(0.999) && mfabs(h.normal.x) < R(1e-4) && mfabs(h.normal.z) < R(1e-4))
                             N = water_normal(P.x, P.z, R(0));
                     }
@@ -421,7 +427,7 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
                                     gadd(ctx, kParamsPerMaterial * mat + 5 + ch,
                                          (float)(comp3(adj, ch) * comp3(throughput, ch)));
                         }
-                        if (b == 0 && length_sq(mat3(m.atmosphere_glow)) > R(1e-6))
+                        if (!PBR && b == 0 && length_sq(mat3(m.atmosphere_glow)) > R(1e-6))
                             radiance = add(radiance, mul(throughput, atmosphere_term(m, N, V, mat3(S.sky.sun_dir))));
                         do_sun = (b == 0 || (b == 1 && st.medium >= 0 && st.last_specular));
                         vflags = (h.front_face ? kVertFront : 0) | (do_sun ? kVertSun : 0);
@@ -434,7 +440,7 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
                         V3<R> wi, w;
                         int refracted = 0, sampled_specular = 0;
                         bool ok;
-                        if (m.pbr)
+                        if (PBR || m.pbr)
                             ok = pt_sample_pbr(*msh, N, d, V, u1, u2, u_lobe, &wi, &w, &sampled_specular);
                         else
                             ok = pt_sample_legacy(*msh, N, d, V, h.front_face, u1, u2, u_lobe, u_glass, &wi, &w,
@@ -443,7 +449,7 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
                             st.last_specular = sampled_specular;
                             throughput = mul(throughput, w);
                             if (finite3(throughput) && pt_max_component(throughput) > R(0)) {
-                                if (refracted && (m.is_water || m.beer_lambert))
+                                if (!PBR && refracted && (m.is_water || m.beer_lambert))
                                     st.medium = h.front_face ? h.material : -1;
                                 bool alive = true;
                                 if (b >= 2) {  // PT_RR_START_BOUNCE (src/pathtrace.c:69)
@@ -493,7 +499,8 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
                                 so = add(P, scale(N, R(1e-3)));
                                 R lt_t;
                                 if (light_sphere_t(S, lt.prim, so, wi, R(1e-3), R(1e30), &lt_t)) {
-                                    V3<R> lit = shade(*msh, N, wi, V, mat3(lt.emissive));
+                                    V3<R> lit = PBR ? shade_pbr(*msh, N, wi, V, mat3(lt.emissive))
+                                                    : shade(*msh, N, wi, V, mat3(lt.emissive));
                                     contrib = mul(beta, scale(lit, Omega));
                                     tmax = lt_t - R(1e-3);
                                     want = true;
@@ -517,7 +524,8 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
                     so = add(P, scale(N, R(1e-3)));
                     R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
                     R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
-                    V3<R> lit = shade(*msh, N, L, V, mat3(S.sky.sun_color));
+                    V3<R> lit = PBR ? shade_pbr(*msh, N, L, V, mat3(S.sky.sun_color))
+                                    : shade(*msh, N, L, V, mat3(S.sky.sun_color));
                     contrib = mul(beta, scale(lit, Omega));
                     want = true;
                 }

@@ -337,6 +337,10 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
                     k_wf_shade<R, false, true><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth,
                                                                             paths, nee, rays[which ^ 1], sq, none,
                                                                             srays, (const WfHit<R> *)st->sorted_hits);
+                else if (sizeof(R) == 4 && S.pbr_only)
+                    k_wf_shade<R, false, false, sizeof(R) == 4><<<g, block, smem_shade, s>>>(
+                        S, rays[which], hits, C, which, b, depth, paths, nee, rays[which ^ 1], sq, none, srays,
+                        (const WfHit<R> *)st->sorted_hits);
                 else
                     k_wf_shade<R, false, false><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth,
                                                                              paths, nee, rays[which ^ 1], sq, none,

@@ -17,7 +17,6 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_ref" / "libmtref.so"
 CLI = HERE / "_ref" / "raytracer"
-REF_DIR = Path(os.environ.get("MT_REF_DIR", "/root/reference"))
 
 P, I, D, U = C.c_void_p, C.c_int, C.c_double, C.c_uint
 
@@ -62,15 +61,21 @@ _SIG = {
 _lib = None
 
 
+def sources_present() -> bool:
+    """Whether oracle/Makefile finds the reference sources (its REF_DIR, or
+    the MT_REF_DIR environment variable)."""
+    return subprocess.run(["make", "-s", "-C", str(HERE), "have-ref"], capture_output=True).returncode == 0
+
+
 def available() -> bool:
-    return LIB.exists() or (REF_DIR / "src").is_dir()
+    return LIB.exists() or sources_present()
 
 
 def build() -> None:
     """Compile the oracle (needs the reference sources; never run on the GPU box)."""
-    if not (REF_DIR / "src").is_dir():
-        raise RuntimeError(f"reference sources not found at {REF_DIR}")
-    subprocess.run(["make", "-s", "-C", str(HERE), f"REF_DIR={REF_DIR}", "cpu", "-j8"], check=True)
+    if not sources_present():
+        raise RuntimeError("reference sources not found (set MT_REF_DIR to the reference checkout)")
+    subprocess.run(["make", "-s", "-C", str(HERE), "cpu", "-j8"], check=True)
 
 
 def load() -> C.CDLL:

@@ -83,7 +83,7 @@ def _log_render(g, cam, w, h, s0, s1, depth, cap):
     return rec, acc.cpu().numpy()
 
 
-def _check_log(rs, desc, rec, tag, rng, max_queries=1_500_000):
+def _check_log(rs, desc, rec, tag, rng, cam_pos, max_queries=1_500_000):
     o = rec["o"].astype(np.float64)
     d = rec["d"].astype(np.float64)
     ext = rec["kind"] == 0
@@ -97,8 +97,17 @@ def _check_log(rs, desc, rec, tag, rng, max_queries=1_500_000):
     differ, band = classify_nearest(rs, desc, o[ie], d[ie], 1e-4, 1e30, got, want, wt)
     out_e = _report(f"{tag} extension rays", differ, band)
     same = (got == want) & (want >= 0)
-    rel = np.abs(rec["t"][ie][same] - wt[same]) / np.abs(wt[same])
-    print(f"{tag} extension rays: t rel err 99.99th pct {np.quantile(rel, 0.9999):.3g}, max {rel.max():.3g}")
+    tg, tw = rec["t"][ie][same].astype(np.float64), wt[same]
+    # primary rays (from the pinhole): t within 1e-5 relative. Later rays
+    # start on a surface, where a hit can lie within 1e-3 of the origin: there
+    # the FP32 error of t is set by the coordinates (origin and vertices, up
+    # to ~60 here), not by t, so it is bounded relative to |o| + t.
+    primary = np.all(o[ie][same] == cam_pos, axis=1)
+    rel = np.abs(tg - tw) / np.abs(tw)
+    rel_coord = np.abs(tg - tw) / (np.abs(o[ie][same]).max(axis=1) + np.abs(tw))
+    print(f"{tag} extension rays: primary t rel err max {rel[primary].max():.3g} ({int(primary.sum())} rays); "
+          f"all rays |dt| / (|o| + t) max {rel_coord.max():.3g}, t rel err 99.99th pct {np.quantile(rel, 0.9999):.3g}")
+    rel = (rel[primary], rel_coord)
     # shadow connections
     js = np.flatnonzero(shd)
     if len(js) > max_queries:
@@ -130,12 +139,14 @@ def test_wavefront_queries_fp32_match_oracle(field, field_ref, mtlib, sort):
         warm, img_warm = _log_render(g, cam, w, h, 0, spp, depth, cap)
         g.trace_log_enable(0)
     assert np.array_equal(img_cold, img_warm)
+    cam_pos = np.array(cam.c.position, np.float32).astype(np.float64)
     for tag, rec in (("cold cache", cold), ("warm cache", warm)):
-        (ne, oe, nbe, rel), (ns, os_, nbs) = _check_log(field_ref, field, rec, tag, rng)
-        assert ne > 10_000 and ns > 10_000
+        (ne, oe, nbe, (rel_p, rel_c)), (ns, os_, nbs) = _check_log(field_ref, field, rec, tag, rng, cam_pos)
+        assert ne > 10_000 and ns > 10_000 and len(rel_p) > 5_000
         assert oe <= 5e-4 * nbe, f"{tag}: {oe} extension hits differ outside the FP32 band"
         assert os_ <= 5e-4 * nbs, f"{tag}: {os_} shadow answers differ outside the FP32 band"
-        assert np.quantile(rel, 0.9999) < 1e-5
+        assert rel_p.max() < 1e-5
+        assert rel_c.max() < 1e-5
 
 
 def test_occluded_fp32_triangles(field, field_ref, mtlib):
