@@ -245,7 +245,7 @@ class Frames:
 
 def tuned_options(tune) -> dict:
     ch = tune["chosen"]
-    return {"queue_capacity": ch["queue_capacity"], "traversal": 2 if ch["traversal"] == "dynamic" else 1,
+    return {"queue_capacity": ch["queue_capacity"], "traversal": {"dynamic": 2, "packet": 3}.get(ch["traversal"], 1),
             "block_size": ch["block"], "bvh_width": ch["bvh_width"], "sort_threshold": ch["sort_threshold"]}
 
 
@@ -724,7 +724,7 @@ def large_bench(torch, device: int, spp: int = 2, adj_spp: int = 1):
     st = g.stats()
     g.release()
     ch = tune["chosen"]
-    opts = {"traversal": 2 if ch["traversal"] == "dynamic" else 1, "block_size": ch["block"],
+    opts = {"traversal": {"dynamic": 2, "packet": 3}.get(ch["traversal"], 1), "block_size": ch["block"],
             "bvh_width": ch["bvh_width"], "sort_threshold": 0, "queue_capacity": ch["queue_capacity"]}
     r = DiffRenderer(d, LW, LH, adj_spp, LD, precision="fp32", integrator="wavefront", bvh_builder=1, device=device,
                      **opts)

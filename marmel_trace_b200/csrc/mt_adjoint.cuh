@@ -52,11 +52,12 @@ MT_D void gadd(const AdjCtx &c, int i, float v)
 
 template <typename R> MT_D R comp3(V3<R> v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
 
-// d d_ggx(ndh, a) / d a
-template <typename R> MT_D R d_ggx_dalpha(R ndh, R a)
+// d d_ggx_cs(ndh, sin2, a) / d a (the denominator in the precision's form,
+// see d_ggx_cs)
+template <typename R> MT_D R d_ggx_dalpha(R ndh, R sin2, R a)
 {
     R a2 = a * a;
-    R d = ndh * ndh * (a2 - R(1)) + R(1);
+    R d = sizeof(R) == 4 ? a2 * ndh * ndh + sin2 : ndh * ndh * (a2 - R(1)) + R(1);
     R dD_da2 = (d - R(2) * a2 * ndh * ndh) / (Const<R>::pi * d * d * d);
     return dD_da2 * R(2) * a;
 }
@@ -101,20 +102,22 @@ MT_D void shade_grad(const DevMaterial<R> &m, int mi, V3<R> N, V3<R> L, V3<R> V,
     bool dmet = m.metallic > R(0) && m.metallic < R(1);
     R alpha = roughness_to_alpha(m.roughness);
     V3<R> h = add(L, V);
-    R ndh = R(0);
+    R ndh = R(0), sin2 = R(1);
     if (length_sq(h) > R(1e-12)) {
-        ndh = dot(N, normalize(h));
+        const V3<R> hn = normalize(h);
+        ndh = dot(N, hn);
         if (ndh < R(0)) ndh = R(0);
+        else sin2 = sin2_between(N, hn);
     }
     R cv = mat_clamp01(ndv);
     R mm = R(1) - cv;
     R m2 = mm * mm;
     R k5 = m2 * m2 * mm;
-    R D = d_ggx(ndh, alpha);
+    R D = d_ggx_cs(ndh, sin2, alpha);
     R G = g_smith_schlick(ndl, ndv, mat_clamp01(m.roughness));
     R denom = R(4) * ndl * ndv;
     R specs = denom > R(0) ? D * G / denom : R(0);
-    R dspecs = denom > R(0) ? (d_ggx_dalpha(ndh, alpha) * dalpha_drough(m.roughness) * G +
+    R dspecs = denom > R(0) ? (d_ggx_dalpha(ndh, sin2, alpha) * dalpha_drough(m.roughness) * G +
                                D * dG_drough(ndl, ndv, m.roughness)) / denom
                             : R(0);
     R d_rough = R(0), d_met = R(0);
@@ -194,7 +197,8 @@ MT_D bool sample_with_info(const DevMaterial<R> &m, V3<R> N, V3<R> d, V3<R> V, i
             if (*specular) {
                 // the same half vector pt_sample_pbr drew
                 info->H = ggx_half_vector(N, roughness_to_alpha(roughness), u1, u2);
-                info->pdf = ggx_pdf(dot(N, info->H), dot(V, info->H), roughness_to_alpha(roughness));
+                info->pdf = ggx_pdf(dot(N, info->H), sin2_between(N, info->H), dot(V, info->H),
+                                    roughness_to_alpha(roughness));
                 info->p = p_spec;
                 info->kind = 1;
             } else {
@@ -244,10 +248,12 @@ MT_D void weight_grad(const DevMaterial<R> &m, int mi, const LobeInfo<R> &info, 
         R mm = R(1) - cv;
         R m2 = mm * mm;
         R k5 = m2 * m2 * mm;
-        R D = d_ggx(ndh, alpha);
+        const R sin2 = sin2_between(N, H);
+        R D = d_ggx_cs(ndh, sin2, alpha);
         R G = g_smith_schlick(ndl, ndv, roughness);
         R S = D * G / (R(4) * ndv * info.pdf * info.p);
-        R dS = (d_ggx_dalpha(ndh, alpha) * dalpha_drough(m.roughness) * G + D * dG_drough(ndl, ndv, m.roughness)) /
+        R dS = (d_ggx_dalpha(ndh, sin2, alpha) * dalpha_drough(m.roughness) * G +
+                D * dG_drough(ndl, ndv, m.roughness)) /
                (R(4) * ndv * info.pdf * info.p);
         R d_rough = R(0), d_met = R(0);
         for (int ch = 0; ch < 3; ++ch) {
@@ -380,11 +386,12 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
         R dc2 = length_sq(to_c);
         R dc = msqrt(dc2);
         R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
-        R Omega = R(2) * R(3.14159265358979323846) * (R(1) - cos_mx);
+        const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
+        R Omega = R(2) * R(3.14159265358979323846) * omc;
         V3<R> w = scale(to_c, R(1) / dc);
         R u1 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
         R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
-        V3<R> wi = light_sphere_sample_dir(w, cos_mx, u1, u2);
+        V3<R> wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
         V3<R> coeff = scale(nee_w, Omega);
         shade_grad(mm, mi, N, wi, V, mul(mat3(lt.emissive), a), coeff, ctx);
         V3<R> s1 = shade(mm, N, wi, V, one);
@@ -508,12 +515,13 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
                 R dc = msqrt(dc2);
                 if (dc <= lt.radius) continue;
                 R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
-                R Omega = R(2) * R(3.14159265358979323846) * (R(1) - cos_mx);
+                const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
+                R Omega = R(2) * R(3.14159265358979323846) * omc;
                 if (!(Omega > R(0))) continue;
                 V3<R> w = scale(to_c, R(1) / dc);
                 R u1 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
                 R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
-                V3<R> wi = light_sphere_sample_dir(w, cos_mx, u1, u2);
+                V3<R> wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
                 if (!finite3(wi) || dot(N, wi) <= R(0)) continue;
                 V3<R> so = add(P, scale(N, R(1e-3)));
                 R lt_t;

@@ -1019,6 +1019,106 @@ MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R 
     return tv.found;
 }
 
+// Warp-cooperative any hit on the binary tree (a packet walk, for coherent
+// rays): the 32 lanes of a warp share one walk and one stack (`wstk`, one
+// int per level, in shared memory). A child is entered when the box test of
+// at least one live lane passes (a live lane holds a query that has found no
+// hit yet), the nearer child first by the vote of the lanes that hit both; at
+// a leaf every live lane tests every primitive against its own [tmin, tmax].
+// A lane may so test primitives its own walk would have culled, but it never
+// skips one its own walk would test (every child its own box test passes is
+// entered), so each lane's answer is its any-hit answer. Connections from one
+// pixel toward one light visit nearly the same nodes, so the lanes stay busy
+// where independent walks diverge. All 32 lanes call it together (lanes
+// without a query pass live = false). Returns this lane's answer; *leaf_out
+// is the blocking leaf (leaf_code), -1 for a plane or no hit.
+template <typename R>
+MT_D bool warp_any2(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, bool live, int *wstk, int *leaf_out,
+                    TravCount &c)
+{
+    bool found = false;
+    *leaf_out = -1;
+    if (live) {
+        for (int i = 0; i < S.plane_count; ++i) {
+            R t;
+            ++c.ntest;
+            if (plane_t(S.planes + 6 * (size_t)i, rp.o, rp.d, tmin, tmax, &t)) {
+                found = true;
+                break;
+            }
+        }
+    }
+    live = live && !found;
+    if (S.node_count <= 0 || !__any_sync(0xffffffffu, live)) return found;
+    const int cap = S.stack_depth;
+    const bool leader = (threadIdx.x & 31) == 0;
+    int sp = 0, node = 0;  // warp-uniform
+    for (;;) {
+        while (node >= 0) {
+            const float4 *Nd = S.nodes + 4 * (size_t)node;
+            const float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
+            const int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
+            bool hl = false, hr = false;
+            R tl = R(0), tr = R(0);
+            if (live) {
+                ++c.nvis;
+                node_test(q0, q1, q2, rp, tmin, tmax, &hl, &hr, &tl, &tr);
+            }
+            const unsigned bl = __ballot_sync(0xffffffffu, hl), br = __ballot_sync(0xffffffffu, hr);
+            if (bl && br) {
+                const unsigned both = bl & br;
+                const unsigned left_first = __ballot_sync(0xffffffffu, hl && hr && tl <= tr);
+                const bool lnear = 2 * __popc(left_first) >= __popc(both);
+                if (sp >= cap) {
+                    if (leader) atomicOr(S.err, ERR_STACK);
+                    return found;
+                }
+                if (leader) wstk[sp] = lnear ? q3.y : q3.x;
+                ++sp;
+                node = lnear ? q3.x : q3.y;
+            } else if (bl) {
+                node = q3.x;
+            } else if (br) {
+                node = q3.y;
+            } else {
+                __syncwarp();
+                node = sp > 0 ? wstk[--sp] : kEmpty;
+            }
+        }
+        if (node == kEmpty) break;
+        if (live) {
+            const int leaf = ~node, first = leaf >> 4, count = leaf & 7;
+            if ((leaf >> 3) & 1) {
+                for (int i = 0; i < count; ++i) {
+                    ++c.ntest;
+                    ++c.ntri;
+                    if (tri_occ(S, first + i, rp, tmin, tmax)) {
+                        found = true;
+                        break;
+                    }
+                }
+            } else {
+                for (int i = 0; i < count; ++i) {
+                    const int2 ref = __ldg(S.refs + first + i);
+                    ++c.ntest;
+                    c.ntri += (ref.y >> 28) == KIND_TRIANGLE;
+                    if (prim_occluded(S, ref.y, rp, tmin, tmax)) {
+                        found = true;
+                        break;
+                    }
+                }
+            }
+            if (found) *leaf_out = node;
+        }
+        live = live && !found;
+        if (!__any_sync(0xffffffffu, live)) break;
+        __syncwarp();
+        node = sp > 0 ? wstk[--sp] : kEmpty;
+        if (node == kEmpty) break;
+    }
+    return found;
+}
+
 // scene_intersect / scene_occluded entry semantics: a direction that is not
 // unit length (|d|^2 off by more than 1e-12) is normalised first
 // (src/bvh.c:563-566, :720-723).

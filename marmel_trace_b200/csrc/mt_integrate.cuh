@@ -393,12 +393,13 @@ MT_D V3<R> pt_nee_emissive(const DevScene<R> &S, const DevMaterial<R> &mm, V3<R>
         R dc = msqrt(dc2);
         if (dc <= lt.radius) continue;
         R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
-        R Omega = R(2) * R(3.14159265358979323846) * (R(1) - cos_mx);
+        const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
+        R Omega = R(2) * R(3.14159265358979323846) * omc;
         if (!(Omega > R(0))) continue;
         V3<R> w = scale(to_c, R(1) / dc);
         R u1 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)bounce, PT_CH_NEE_EMIT_A);
         R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)bounce, PT_CH_NEE_EMIT_B);
-        V3<R> wi = light_sphere_sample_dir(w, cos_mx, u1, u2);
+        V3<R> wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
         if (!finite3(wi) || dot(N, wi) <= R(0)) continue;
         V3<R> so = add(P, scale(N, R(1e-3)));
         R lt_t;
@@ -434,10 +435,11 @@ MT_D bool pt_sample_pbr(const DevMaterial<R> &m, V3<R> N, V3<R> d, V3<R> V, R u1
         R ndh = dot(N, H);
         R vdh = dot(V, H);
         if (!(ndl > R(0)) || !(ndh > R(0)) || !(vdh > R(0))) return false;
-        R D = d_ggx(ndh, alpha);
+        const R sin2 = sin2_between(N, H);
+        R D = d_ggx_cs(ndh, sin2, alpha);
         R G = g_smith_schlick(ndl, ndv, roughness);
         V3<R> F = sampling_fresnel_schlick_rgb(vdh, f0);
-        R pdf = ggx_pdf(ndh, vdh, alpha);
+        R pdf = ggx_pdf(ndh, sin2, vdh, alpha);
         if (!(pdf > R(0)) || !(p_spec > R(0))) return false;
         R sc = D * G / (R(4) * ndv * pdf * p_spec);
         *wi_out = wi;
@@ -747,14 +749,15 @@ MT_D V3<R> emissive_direct(const DevScene<R> &S, const DevMaterial<R> &mm, V3<R>
         R dc = msqrt(dc2);
         if (dc <= lt.radius) continue;
         R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
-        R solid = R(2) * R(3.14159265358979323846) * (R(1) - cos_mx);
+        const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
+        R solid = R(2) * R(3.14159265358979323846) * omc;
         if (!(solid > R(0))) continue;
         V3<R> w = scale(to_c, R(1) / dc);
         for (int si = 0; si < 16; ++si) {  // EMISSIVE_LIGHT_SAMPLES (src/render.c:448)
             uint32_t k = hash3(seed_key ^ 0xE311u, (uint32_t)li, (uint32_t)si);
             R u1 = rand01<R>(k, (uint32_t)si, 0x4c11u);
             R u2 = rand01<R>(k, (uint32_t)si, 0x9d27u);
-            V3<R> w_i = light_sphere_sample_dir(w, cos_mx, u1, u2);
+            V3<R> w_i = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
             if (dot(N, w_i) <= R(0)) continue;
             R lt_t;
             bool visible;

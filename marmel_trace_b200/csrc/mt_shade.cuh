@@ -613,7 +613,8 @@ template <typename R> MT_D V3<R> sun_disk_dir(V3<R> sun_dir, R radius_deg, R r1,
 }
 
 // light_sphere_sample_dir (src/material.c:1113-1146)
-template <typename R> MT_D V3<R> light_sphere_sample_dir(V3<R> w, R cos_alpha_max, R u1, R u2)
+// omc_max: 1 - cos_alpha_max from cone_one_minus_cos (used by FP32)
+template <typename R> MT_D V3<R> light_sphere_sample_dir(V3<R> w, R cos_alpha_max, R omc_max, R u1, R u2)
 {
     const R rmax = sizeof(R) == 8 ? R(0.9999999999999999) : R(0.99999994f);
     w = normalize(w);
@@ -624,8 +625,18 @@ template <typename R> MT_D V3<R> light_sphere_sample_dir(V3<R> w, R cos_alpha_ma
     else if (u1 > rmax) u1 = rmax;
     if (!(u2 > R(0))) u2 = R(0);
     else if (u2 > rmax) u2 = rmax;
-    R cos_alpha = R(1) - u1 * (R(1) - cos_alpha_max);
-    R sin_alpha = msqrt(R(1) - cos_alpha * cos_alpha);
+    R cos_alpha, sin_alpha;
+    if constexpr (sizeof(R) == 4) {
+        // y = 1 - cos(alpha) within the cone: sin^2 = y (2 - y), no cancellation
+        if (!(omc_max >= R(0))) omc_max = R(0);
+        else if (omc_max > R(1)) omc_max = R(1);
+        const R y = u1 * omc_max;
+        cos_alpha = R(1) - y;
+        sin_alpha = msqrt(y * (R(2) - y));
+    } else {
+        cos_alpha = R(1) - u1 * (R(1) - cos_alpha_max);
+        sin_alpha = msqrt(R(1) - cos_alpha * cos_alpha);
+    }
     R phi = R(2) * Const<R>::pi * u2;
     V3<R> t, b;
     basis(w, &t, &b);
@@ -766,6 +777,41 @@ template <typename R> MT_D R d_ggx(R ndh, R a)
     return a2 / (Const<R>::pi * d * d);
 }
 
+// GGX D of a half vector at angle theta from the normal, given cos(theta) =
+// ndh and sin^2(theta). The denominator ndh^2 (a^2 - 1) + 1 equals
+// a^2 ndh^2 + sin^2(theta). FP64 keeps the reference's form (its bits match
+// the reference's); FP32 uses the second form, whose terms are all positive.
+// Near the normal the first form subtracts two numbers within an ulp of 1:
+// for roughness 0.02 (a^2 = 1.6e-7, about FP32's epsilon) it is off by up to
+// a factor of two, so D is off by up to four, which biased FP32 images of
+// near-mirror metals bright.
+template <typename R> MT_D R d_ggx_cs(R ndh, R sin2, R a)
+{
+    if constexpr (sizeof(R) == 4) {
+        const R a2 = a * a;
+        const R d = a2 * ndh * ndh + sin2;
+        return a2 / (Const<R>::pi * d * d);
+    } else {
+        return d_ggx(ndh, a);
+    }
+}
+
+// sin^2 of the angle between unit vectors n and h, |n x h|^2 (Lagrange's
+// identity): accurate where 1 - (n.h)^2 cancels.
+template <typename R> MT_D R sin2_between(V3<R> n, V3<R> h) { return length_sq(cross(n, h)); }
+
+// 1 - cos(alpha_max) of the cone a sphere of radius^2 / distance^2 = x
+// subtends, given cos(alpha_max) = sqrt(1 - x). FP64: the reference's
+// 1 - cos; FP32: x / (1 + cos), the same value without the cancellation that
+// costs distant lights (x ~ 1e-4) three decimal digits of their solid angle.
+template <typename R> MT_D R cone_one_minus_cos(R x, R cos_max)
+{
+    if constexpr (sizeof(R) == 4)
+        return x / (R(1) + cos_max);
+    else
+        return R(1) - cos_max;
+}
+
 // g_smith_schlick (src/material.c:207-218, same as pt_g_smith_schlick :192-200
 // up to the NaN behaviour of the clamp)
 template <typename R> MT_D R g_smith_schlick(R ndl, R ndv, R roughness)
@@ -800,15 +846,17 @@ MT_D V3<R> shade_pbr(const DevMaterial<R> &m, V3<R> N, V3<R> L, V3<R> V, V3<R> l
     R metallic = mat_clamp01(m.metallic);
     R alpha = roughness_to_alpha(m.roughness);
     V3<R> h = add(L, V);
-    R ndh = R(0);
+    R ndh = R(0), sin2 = R(1);
     if (length_sq(h) > R(1e-12)) {
-        ndh = dot(N, normalize(h));
+        const V3<R> hn = normalize(h);
+        ndh = dot(N, hn);
         if (ndh < R(0)) ndh = R(0);
+        else sin2 = sin2_between(N, hn);
     }
     V3<R> albedo = mat3(m.albedo);
     V3<R> f0 = lerp(v3(R(0.04), R(0.04), R(0.04)), albedo, metallic);
     V3<R> F = fresnel_schlick_rgb(ndv, f0);
-    R D = d_ggx(ndh, alpha);
+    R D = d_ggx_cs(ndh, sin2, alpha);
     R G = g_smith_schlick(ndl, ndv, mat_clamp01(m.roughness));
     R denom = R(4) * ndl * ndv;
     R spec_scale = (denom > R(0)) ? (D * G / denom) : R(0);
@@ -857,8 +905,18 @@ MT_D V3<R> sample_glossy_dir(const DevMaterial<R> &m, V3<R> N, V3<R> incident, R
     else if (r1 > rmax) r1 = rmax;
     if (!(r2 > R(0))) r2 = R(0);
     else if (r2 > rmax) r2 = rmax;
-    R cos_theta = msqrt((R(1) - r1) / (R(1) + (a2 - R(1)) * r1));
-    R sin_theta = msqrt(R(1) - cos_theta * cos_theta);
+    R cos_theta, sin_theta;
+    if constexpr (sizeof(R) == 4) {
+        // cos^2 and sin^2 of the GGX angle as (1 - r1) / den and a2 r1 / den,
+        // den = 1 - r1 + a2 r1 (1 - r1 is exact: r1 is a multiple of 2^-24):
+        // no cancellation for small alpha (see d_ggx_cs)
+        const R omr = R(1) - r1, den = omr + a2 * r1;
+        cos_theta = msqrt(omr / den);
+        sin_theta = msqrt(a2 * r1 / den);
+    } else {
+        cos_theta = msqrt((R(1) - r1) / (R(1) + (a2 - R(1)) * r1));
+        sin_theta = msqrt(R(1) - cos_theta * cos_theta);
+    }
     R phi = R(2) * Const<R>::pi * r2;
     V3<R> t, b;
     basis(N, &t, &b);
@@ -988,8 +1046,17 @@ template <typename R> MT_D V3<R> ggx_half_vector(V3<R> n, R alpha, R u1, R u2)
     R a2 = a * a;
     R r1 = clamp_uniform(u1);
     R r2 = clamp_uniform(u2);
-    R cos_theta = msqrt((R(1) - r1) / (R(1) + (a2 - R(1)) * r1));
-    R sin_theta = msqrt(mfmax(R(0), R(1) - cos_theta * cos_theta));
+    R cos_theta, sin_theta;
+    if constexpr (sizeof(R) == 4) {
+        // the same angle from (1 - r1) / den and a2 r1 / den (see
+        // sample_glossy_dir): no cancellation for small alpha
+        const R omr = R(1) - r1, den = omr + a2 * r1;
+        cos_theta = msqrt(omr / den);
+        sin_theta = msqrt(a2 * r1 / den);
+    } else {
+        cos_theta = msqrt((R(1) - r1) / (R(1) + (a2 - R(1)) * r1));
+        sin_theta = msqrt(mfmax(R(0), R(1) - cos_theta * cos_theta));
+    }
     R phi = R(2) * Const<R>::pi * r2;
     V3<R> t, b;
     sampling_basis(nn, &t, &b);
@@ -1000,12 +1067,14 @@ template <typename R> MT_D V3<R> ggx_half_vector(V3<R> n, R alpha, R u1, R u2)
 }
 
 // sampling_ggx_pdf (src/sampling.c:270-281)
-template <typename R> MT_D R ggx_pdf(R n_dot_h, R h_dot_v, R alpha)
+// (sin2: sin^2 of the angle between n and h, for the FP32 form of D)
+template <typename R> MT_D R ggx_pdf(R n_dot_h, R sin2, R h_dot_v, R alpha)
 {
     if (!(h_dot_v > R(0)) || !(n_dot_h > R(0))) return R(0);
     R a = alpha > R(1e-4) ? alpha : R(1e-4);
     R ndh = n_dot_h > R(1) ? R(1) : n_dot_h;
-    R D = d_ggx(ndh, a);
+    if (n_dot_h > R(1)) sin2 = R(0);
+    R D = d_ggx_cs(ndh, sin2, a);
     return D * ndh / (R(4) * h_dot_v);
 }
 

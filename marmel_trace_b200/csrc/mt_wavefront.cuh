@@ -489,12 +489,13 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
                     R dc = msqrt(dc2);
                     if (dc > lt.radius) {
                         R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
-                        R Omega = R(2) * R(3.14159265358979323846) * (R(1) - cos_mx);
+                        const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
+                        R Omega = R(2) * R(3.14159265358979323846) * omc;
                         if (Omega > R(0)) {
                             V3<R> w = scale(to_c, R(1) / dc);
                             R u1 = rand01<R>(st.seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
                             R u2 = rand01<R>(st.seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
-                            wi = light_sphere_sample_dir(w, cos_mx, u1, u2);
+                            wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
                             if (finite3(wi) && dot(N, wi) > R(0)) {
                                 so = add(P, scale(N, R(1e-3)));
                                 R lt_t;
@@ -879,6 +880,56 @@ __global__ void __launch_bounds__(kWfMaxBlock, 8) k_wf_shadow_cache(const __grid
         const int at = warp_append(&C->walk_count, miss);
         if (miss) walk[at] = q;
     }
+}
+
+// Second pass with the packet walk (MT_TRAVERSAL_PACKET): the connections the
+// cached leaves did not resolve (`walk`), 32 consecutive ones per warp walked
+// together (warp_any2). Consecutive connections leave nearby points of one
+// pixel block toward one light, so they share most nodes. A blocking leaf
+// goes to the front of the connection's cache entry, as in scene_any_cached.
+// Each warp's stack takes stack_depth ints of the dynamic shared memory.
+template <typename R, bool ADJ>
+__global__ void __launch_bounds__(kWfMaxBlock, 7) k_wf_shadow_packet(const __grid_constant__ DevScene<R> S,
+                                                                  const WfShadow<R> *sq, const WfCounters *C, R *nee,
+                                                                  R *att, int *occ_cache, int wh, int b,
+                                                                  const int *walk)
+{
+    const int n = C->walk_count;
+    const int stride = gridDim.x * blockDim.x;
+    const int n_round = (n + stride - 1) / stride * stride;
+    int *wstk = mt_stack_smem + (threadIdx.x >> 5) * (S.stack_depth > 0 ? S.stack_depth : 1);
+    TravCount cnt;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
+        const bool live = q < n;
+        WfShadow<R> s;
+        RayPre<R> rp;
+        int *entry = nullptr;
+        int c0 = -1;
+        s.tmax = R(0);
+        if (live) {
+            s = sq[walk[q]];
+            rp = ray_pre(v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2])));
+            entry = occ_entry(S, occ_cache, wh, b, s);
+            c0 = entry[0];
+        }
+        int leaf = -1;
+        const bool occ = warp_any2(S, rp, R(1e-3), s.tmax, live, wstk, &leaf, cnt);
+        if (live) {
+            if (occ && leaf != -1 && leaf != c0) {
+                const int4 e = *reinterpret_cast<const int4 *>(entry);
+                *reinterpret_cast<int4 *>(entry) = make_int4(leaf, e.x, e.y, e.z);
+            }
+            V3<R> atten = v3(R(1), R(1), R(1));
+            if (!occ && s.li == kMaxLights)
+                atten = scale(atten, cloud_transmittance(S.sky, v3(s.o[0], s.o[1], s.o[2]), v3(s.d[0], s.d[1], s.d[2])));
+            AbsorbPath<R> ab;
+            ab.mat[0] = ab.mat[1] = -1;
+            ab.dist[0] = ab.dist[1] = R(0);
+            shadow_result<R, ADJ>(s, occ, atten, ab, nee, att);
+            if (S.trace_rec) trace_put(S, rp.o, rp.d, s.tmax, occ ? 1 : 0, 1, b, s.li);
+        }
+    }
+    trav_count_flush<R, true>(S, cnt);
 }
 
 // ------------------------------------------------------------------
