@@ -1119,6 +1119,71 @@ MT_D bool warp_any2(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, b
     return found;
 }
 
+// Warp-cooperative nearest hit on the binary tree (packet walk, for coherent
+// rays such as the primary rays of neighbouring pixels): as warp_any2, one
+// walk and one stack per warp, a child entered when at least one live lane's
+// box test against its own [tmin, closest] passes, and every live lane testing
+// every primitive of each leaf the warp visits with the reference's rules
+// (trav_leaf: [tmin, closest], equal t to the lowest prim index). Each lane's
+// result is its own walk's: every box around its nearest hit has entry <= t
+// <= its closest at any moment, so it is entered. Lanes stay live to the end
+// (a nearest hit has no early exit); all 32 lanes call it together.
+template <typename R>
+MT_D bool warp_nearest2(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, bool live, int *wstk,
+                        Hit<R> *best, TravCount &c)
+{
+    Trav<R> tv;
+    if (live) {
+        trav_init<R, false>(S, tv, rp, tmin, tmax, best, c);
+    } else {
+        tv.found = false;
+        tv.closest = tmax;
+    }
+    if (S.node_count <= 0 || !__any_sync(0xffffffffu, live)) return tv.found;
+    const int cap = S.stack_depth;
+    const bool leader = (threadIdx.x & 31) == 0;
+    int sp = 0, node = 0;  // warp-uniform
+    for (;;) {
+        while (node >= 0) {
+            const float4 *Nd = S.nodes + 4 * (size_t)node;
+            const float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
+            const int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
+            bool hl = false, hr = false;
+            R tl = R(0), tr = R(0);
+            if (live) {
+                ++c.nvis;
+                node_test(q0, q1, q2, rp, tmin, tv.closest, &hl, &hr, &tl, &tr);
+            }
+            const unsigned bl = __ballot_sync(0xffffffffu, hl), br = __ballot_sync(0xffffffffu, hr);
+            if (bl && br) {
+                const unsigned both = bl & br;
+                const unsigned left_first = __ballot_sync(0xffffffffu, hl && hr && tl <= tr);
+                const bool lnear = 2 * __popc(left_first) >= __popc(both);
+                if (sp >= cap) {
+                    if (leader) atomicOr(S.err, ERR_STACK);
+                    return tv.found;
+                }
+                if (leader) wstk[sp] = lnear ? q3.y : q3.x;
+                ++sp;
+                node = lnear ? q3.x : q3.y;
+            } else if (bl) {
+                node = q3.x;
+            } else if (br) {
+                node = q3.y;
+            } else {
+                __syncwarp();
+                node = sp > 0 ? wstk[--sp] : kEmpty;
+            }
+        }
+        if (node == kEmpty) break;
+        if (live) trav_leaf<R, false>(S, tv, node, best, c);
+        __syncwarp();
+        node = sp > 0 ? wstk[--sp] : kEmpty;
+        if (node == kEmpty) break;
+    }
+    return tv.found;
+}
+
 // scene_intersect / scene_occluded entry semantics: a direction that is not
 // unit length (|d|^2 off by more than 1e-12) is normalised first
 // (src/bvh.c:563-566, :720-723).

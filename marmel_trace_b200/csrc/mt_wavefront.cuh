@@ -237,6 +237,54 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend(const __grid_constant
     if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->extension_rays, (unsigned long long)n);
 }
 
+// extend with the packet walk (MT_TRAVERSAL_PACKET, primary rays): 32
+// consecutive rays per warp -- neighbouring pixels of one sample -- walked
+// together (warp_nearest2). Same results as k_wf_extend. Each warp's stack
+// takes stack_depth ints of the dynamic shared memory.
+template <typename R>
+__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend_packet(const __grid_constant__ DevScene<R> S,
+                                                                  const WfRay<R> *rays, const WfCounters *C, int which,
+                                                                  WfHit<R> *hits)
+{
+    const int n = C->ray_count[which];
+    const int stride = gridDim.x * blockDim.x;
+    const int n_round = (n + stride - 1) / stride * stride;
+    int *wstk = mt_stack_smem + (threadIdx.x >> 5) * (S.stack_depth > 0 ? S.stack_depth : 1);
+    TravCount cnt;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
+        const bool live = q < n;
+        V3<R> o = v3(R(0), R(0), R(0)), d = v3(R(0), R(0), R(1));
+        if (live) {
+            const WfRay<R> r = rays[q];
+            o = v3(r.o[0], r.o[1], r.o[2]);
+            d = unit_dir(v3(r.d[0], r.d[1], r.d[2]));
+        }
+        const RayPre<R> rp = ray_pre(o, d);
+        Hit<R> h;
+        const bool found = warp_nearest2(S, rp, R(1e-4), R(1e30), live, wstk, &h, cnt);
+        if (live) {
+            WfHit<R> out;
+            if (found) {
+                out.t = h.t;
+                out.u = h.u;
+                out.v = h.v;
+                out.prim = h.prim;
+                out.code = h.code;
+            } else {
+                out.t = R(0);
+                out.u = R(0);
+                out.v = R(0);
+                out.prim = -1;
+                out.code = 0;
+            }
+            hits[q] = out;
+            if (S.trace_rec) trace_put(S, o, d, out.t, out.prim, 0, 0, 0);
+        }
+    }
+    trav_count_flush<R, false>(S, cnt);
+    if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->extension_rays, (unsigned long long)n);
+}
+
 template <typename R> MT_D void gather_nee(const DevScene<R> &S, R *nee_slot, V3<R> *radiance)
 {
     V3<R> sum = v3(R(0), R(0), R(0));

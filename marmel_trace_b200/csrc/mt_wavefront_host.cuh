@@ -311,7 +311,10 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         int which = 0;
         for (int b = 0; b <= depth; ++b) {
             tic();
-            launch_extend_w<R>(W, dyn, g, block, smem_w, s, S, rays[which], C, which, hits);
+            if (sizeof(R) == 4 && packet && b == 0 && W == 2)
+                k_wf_extend_packet<R><<<g, block, smem, s>>>(S, rays[which], C, which, hits);
+            else
+                launch_extend_w<R>(W, dyn, g, block, smem_w, s, S, rays[which], C, which, hits);
             toc(0);
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
             // shadow_count, shadow_fetch, ray_fetch (the next extend's), sorted
