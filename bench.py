@@ -245,7 +245,7 @@ class Frames:
 
 def tuned_options(tune) -> dict:
     ch = tune["chosen"]
-    return {"queue_capacity": ch["queue_capacity"], "traversal": {"dynamic": 2, "packet": 3}.get(ch["traversal"], 1),
+    return {"queue_capacity": ch["queue_capacity"], "traversal": 2 if ch["traversal"] == "dynamic" else 1,
             "block_size": ch["block"], "bvh_width": ch["bvh_width"], "sort_threshold": ch["sort_threshold"]}
 
 
@@ -391,7 +391,10 @@ def run_ours(args):
         h0, h1 = res["history"][0], res["history"][-1]
         inverse = {"steps": res["steps"], "steps_per_s": round(res["steps_per_s"], 2), "params": res["params"],
                    "loss_first": round(h0["loss"], 6), "loss_last": round(h1["loss"], 6),
-                   "param_rmse_start": round(res["start_param_rmse"], 4), "param_rmse_last": round(h1["param_rmse"], 4)}
+                   "param_rmse_start": round(res["start_param_rmse"], 4), "param_rmse_last": round(h1["param_rmse"], 4),
+                   "group_rmse_start": {k: round(v, 4) for k, v in res["start_groups"].items()},
+                   "group_rmse_last": {k: round(v, 4) for k, v in h1["groups"].items()},
+                   "materials_seen": res["materials_seen"]}
     batch = None
     if single and not args.no_batch:
         batch, detail["batch"] = batch_bench(torch, local)
@@ -724,7 +727,7 @@ def large_bench(torch, device: int, spp: int = 2, adj_spp: int = 1):
     st = g.stats()
     g.release()
     ch = tune["chosen"]
-    opts = {"traversal": {"dynamic": 2, "packet": 3}.get(ch["traversal"], 1), "block_size": ch["block"],
+    opts = {"traversal": 2 if ch["traversal"] == "dynamic" else 1, "block_size": ch["block"],
             "bvh_width": ch["bvh_width"], "sort_threshold": 0, "queue_capacity": ch["queue_capacity"]}
     r = DiffRenderer(d, LW, LH, adj_spp, LD, precision="fp32", integrator="wavefront", bvh_builder=1, device=device,
                      **opts)

@@ -251,9 +251,6 @@ typedef struct {
 #define MT_TRAVERSAL_STATIC  1   /* grid-stride loop: one ray per lane per pass      */
 #define MT_TRAVERSAL_DYNAMIC 2   /* persistent lanes that refill from the queue as   */
                                  /* their rays finish                                 */
-#define MT_TRAVERSAL_PACKET  3   /* grid-stride, and the bounce-0 shadow connections */
-                                 /* the occluder cache leaves are walked 32 at a     */
-                                 /* time, one walk per warp                           */
 
 /* Fill `o` with the library defaults (FP32, megakernel, BVH2, device 0). */
 void mt_options_default(mt_options *o);

@@ -285,7 +285,7 @@ class GpuScene:
         check(self.lib.mt_autotune(self.h, cam.ref, w, h, probe_spp, depth, C.byref(rep)), "mt_autotune")
 
         def opts(o):
-            return {"traversal": {0: "static", 1: "static", 2: "dynamic", 3: "packet"}[o.traversal], "block": o.block_size,
+            return {"traversal": {0: "static", 1: "static", 2: "dynamic"}[o.traversal], "block": o.block_size,
                     "bvh_width": o.bvh_width, "sort_threshold": o.sort_threshold,
                     "queue_capacity": o.queue_capacity or 1 << 25}
 

@@ -29,6 +29,9 @@ template <typename R> struct Hit {
 template <typename R> struct RayPre {
     V3<R> o, d, inv;
     V3<R> oi;  // o * inv: an FP32 slab distance is one fma, box * inv - oi
+    // FP32: absolute error bound of a slab distance from the rounding of oi
+    // (2^-23 max |oi_k| over the axes with a finite inverse); see node_test
+    float slab_eps;
     // watertight-triangle shear (FP32 path)
     int kx, ky, kz;
     float sx, sy, sz;
@@ -50,6 +53,14 @@ template <typename R> MT_D RayPre<R> ray_pre(V3<R> o, V3<R> d)
         p.inv.z = fabsf(d.z) < 1e-30f ? copysignf(1e30f, d.z) : p.inv.z;
     }
     p.oi = v3<R>(o.x * p.inv.x, o.y * p.inv.y, o.z * p.inv.z);
+    p.slab_eps = 0.0f;
+    if constexpr (sizeof(R) == 4) {
+        float m = 0.0f;
+        if (fabsf(d.x) >= 1e-30f) m = fmaxf(m, fabsf(p.oi.x));
+        if (fabsf(d.y) >= 1e-30f) m = fmaxf(m, fabsf(p.oi.y));
+        if (fabsf(d.z) >= 1e-30f) m = fmaxf(m, fabsf(p.oi.z));
+        p.slab_eps = 0x1p-23f * m;
+    }
     float ax = fabsf((float)d.x), ay = fabsf((float)d.y), az = fabsf((float)d.z);
     int kz = (ax > ay) ? ((ax > az) ? 0 : 2) : ((ay > az) ? 1 : 2);
     int kx = kz + 1 == 3 ? 0 : kz + 1;
@@ -521,6 +532,18 @@ MT_D void node_test<float>(const float4 q0, const float4 q1, const float4 q2, co
     float lexit = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fmaxf(lz0, lz1));
     float renter = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fminf(rz0, rz1));
     float rexit = fminf(fminf(fmaxf(rx0, rx1), fmaxf(ry0, ry1)), fmaxf(rz0, rz1));
+    // Conservative bounds: a slab distance fma(box, inv, -oi) differs from
+    // (box - o) / d by at most 2^-23 |t| + 2^-24 |oi| (the roundings of inv,
+    // oi and the fma), so each interval is widened by 3 * 2^-24 |t| +
+    // slab_eps on both ends. A box that a ray meets in exact arithmetic is
+    // then never culled, whatever the FP32 rounding (cf. Ize, "Robust BVH Ray
+    // Traversal", JCGT 2013, which scales the exit distance for the same
+    // reason).
+    const float k = 3.0f * 0x1p-24f;
+    lenter -= fmaf(k, fabsf(lenter), rp.slab_eps);
+    lexit += fmaf(k, fabsf(lexit), rp.slab_eps);
+    renter -= fmaf(k, fabsf(renter), rp.slab_eps);
+    rexit += fmaf(k, fabsf(rexit), rp.slab_eps);
     *hl = (lexit >= lenter && lexit >= tmin && lenter <= tmax);
     *hr = (rexit >= renter && rexit >= tmin && renter <= tmax);
     *tl = lenter < tmin ? tmin : lenter;
@@ -769,6 +792,9 @@ MT_D bool box_hit(float lx, float hx, float ly, float hy, float lz, float hz, co
     R z0 = fmaf(lz, rp.inv.z, -rp.oi.z), z1 = fmaf(hz, rp.inv.z, -rp.oi.z);
     R en = mfmax(mfmax(mfmin(x0, x1), mfmin(y0, y1)), mfmin(z0, z1));
     R ex = mfmin(mfmin(mfmax(x0, x1), mfmax(y0, y1)), mfmax(z0, z1));
+    // widened as in node_test<float>
+    en -= fmaf(3.0f * 0x1p-24f, fabsf(en), rp.slab_eps);
+    ex += fmaf(3.0f * 0x1p-24f, fabsf(ex), rp.slab_eps);
     *enter = en < tmin ? tmin : en;
     return ex >= en && ex >= tmin && en <= tmax;
 }
@@ -1015,171 +1041,6 @@ MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R 
             for (int k = WAYS - 1; k > 0; --k) cache[k] = cache[k - 1];
             cache[0] = tv.any_leaf;
         }
-    }
-    return tv.found;
-}
-
-// Warp-cooperative any hit on the binary tree (a packet walk, for coherent
-// rays): the 32 lanes of a warp share one walk and one stack (`wstk`, one
-// int per level, in shared memory). A child is entered when the box test of
-// at least one live lane passes (a live lane holds a query that has found no
-// hit yet), the nearer child first by the vote of the lanes that hit both; at
-// a leaf every live lane tests every primitive against its own [tmin, tmax].
-// A lane may so test primitives its own walk would have culled, but it never
-// skips one its own walk would test (every child its own box test passes is
-// entered), so each lane's answer is its any-hit answer. Connections from one
-// pixel toward one light visit nearly the same nodes, so the lanes stay busy
-// where independent walks diverge. All 32 lanes call it together (lanes
-// without a query pass live = false). Returns this lane's answer; *leaf_out
-// is the blocking leaf (leaf_code), -1 for a plane or no hit.
-template <typename R>
-MT_D bool warp_any2(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, bool live, int *wstk, int *leaf_out,
-                    TravCount &c)
-{
-    bool found = false;
-    *leaf_out = -1;
-    if (live) {
-        for (int i = 0; i < S.plane_count; ++i) {
-            R t;
-            ++c.ntest;
-            if (plane_t(S.planes + 6 * (size_t)i, rp.o, rp.d, tmin, tmax, &t)) {
-                found = true;
-                break;
-            }
-        }
-    }
-    live = live && !found;
-    if (S.node_count <= 0 || !__any_sync(0xffffffffu, live)) return found;
-    const int cap = S.stack_depth;
-    const bool leader = (threadIdx.x & 31) == 0;
-    int sp = 0, node = 0;  // warp-uniform
-    for (;;) {
-        while (node >= 0) {
-            const float4 *Nd = S.nodes + 4 * (size_t)node;
-            const float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
-            const int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
-            bool hl = false, hr = false;
-            R tl = R(0), tr = R(0);
-            if (live) {
-                ++c.nvis;
-                node_test(q0, q1, q2, rp, tmin, tmax, &hl, &hr, &tl, &tr);
-            }
-            const unsigned bl = __ballot_sync(0xffffffffu, hl), br = __ballot_sync(0xffffffffu, hr);
-            if (bl && br) {
-                const unsigned both = bl & br;
-                const unsigned left_first = __ballot_sync(0xffffffffu, hl && hr && tl <= tr);
-                const bool lnear = 2 * __popc(left_first) >= __popc(both);
-                if (sp >= cap) {
-                    if (leader) atomicOr(S.err, ERR_STACK);
-                    return found;
-                }
-                if (leader) wstk[sp] = lnear ? q3.y : q3.x;
-                ++sp;
-                node = lnear ? q3.x : q3.y;
-            } else if (bl) {
-                node = q3.x;
-            } else if (br) {
-                node = q3.y;
-            } else {
-                __syncwarp();
-                node = sp > 0 ? wstk[--sp] : kEmpty;
-            }
-        }
-        if (node == kEmpty) break;
-        if (live) {
-            const int leaf = ~node, first = leaf >> 4, count = leaf & 7;
-            if ((leaf >> 3) & 1) {
-                for (int i = 0; i < count; ++i) {
-                    ++c.ntest;
-                    ++c.ntri;
-                    if (tri_occ(S, first + i, rp, tmin, tmax)) {
-                        found = true;
-                        break;
-                    }
-                }
-            } else {
-                for (int i = 0; i < count; ++i) {
-                    const int2 ref = __ldg(S.refs + first + i);
-                    ++c.ntest;
-                    c.ntri += (ref.y >> 28) == KIND_TRIANGLE;
-                    if (prim_occluded(S, ref.y, rp, tmin, tmax)) {
-                        found = true;
-                        break;
-                    }
-                }
-            }
-            if (found) *leaf_out = node;
-        }
-        live = live && !found;
-        if (!__any_sync(0xffffffffu, live)) break;
-        __syncwarp();
-        node = sp > 0 ? wstk[--sp] : kEmpty;
-        if (node == kEmpty) break;
-    }
-    return found;
-}
-
-// Warp-cooperative nearest hit on the binary tree (packet walk, for coherent
-// rays such as the primary rays of neighbouring pixels): as warp_any2, one
-// walk and one stack per warp, a child entered when at least one live lane's
-// box test against its own [tmin, closest] passes, and every live lane testing
-// every primitive of each leaf the warp visits with the reference's rules
-// (trav_leaf: [tmin, closest], equal t to the lowest prim index). Each lane's
-// result is its own walk's: every box around its nearest hit has entry <= t
-// <= its closest at any moment, so it is entered. Lanes stay live to the end
-// (a nearest hit has no early exit); all 32 lanes call it together.
-template <typename R>
-MT_D bool warp_nearest2(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, bool live, int *wstk,
-                        Hit<R> *best, TravCount &c)
-{
-    Trav<R> tv;
-    if (live) {
-        trav_init<R, false>(S, tv, rp, tmin, tmax, best, c);
-    } else {
-        tv.found = false;
-        tv.closest = tmax;
-    }
-    if (S.node_count <= 0 || !__any_sync(0xffffffffu, live)) return tv.found;
-    const int cap = S.stack_depth;
-    const bool leader = (threadIdx.x & 31) == 0;
-    int sp = 0, node = 0;  // warp-uniform
-    for (;;) {
-        while (node >= 0) {
-            const float4 *Nd = S.nodes + 4 * (size_t)node;
-            const float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
-            const int4 q3 = __ldg(reinterpret_cast<const int4 *>(Nd + 3));
-            bool hl = false, hr = false;
-            R tl = R(0), tr = R(0);
-            if (live) {
-                ++c.nvis;
-                node_test(q0, q1, q2, rp, tmin, tv.closest, &hl, &hr, &tl, &tr);
-            }
-            const unsigned bl = __ballot_sync(0xffffffffu, hl), br = __ballot_sync(0xffffffffu, hr);
-            if (bl && br) {
-                const unsigned both = bl & br;
-                const unsigned left_first = __ballot_sync(0xffffffffu, hl && hr && tl <= tr);
-                const bool lnear = 2 * __popc(left_first) >= __popc(both);
-                if (sp >= cap) {
-                    if (leader) atomicOr(S.err, ERR_STACK);
-                    return tv.found;
-                }
-                if (leader) wstk[sp] = lnear ? q3.y : q3.x;
-                ++sp;
-                node = lnear ? q3.x : q3.y;
-            } else if (bl) {
-                node = q3.x;
-            } else if (br) {
-                node = q3.y;
-            } else {
-                __syncwarp();
-                node = sp > 0 ? wstk[--sp] : kEmpty;
-            }
-        }
-        if (node == kEmpty) break;
-        if (live) trav_leaf<R, false>(S, tv, node, best, c);
-        __syncwarp();
-        node = sp > 0 ? wstk[--sp] : kEmpty;
-        if (node == kEmpty) break;
     }
     return tv.found;
 }

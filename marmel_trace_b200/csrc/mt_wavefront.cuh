@@ -237,54 +237,6 @@ __global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend(const __grid_constant
     if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->extension_rays, (unsigned long long)n);
 }
 
-// extend with the packet walk (MT_TRAVERSAL_PACKET, primary rays): 32
-// consecutive rays per warp -- neighbouring pixels of one sample -- walked
-// together (warp_nearest2). Same results as k_wf_extend. Each warp's stack
-// takes stack_depth ints of the dynamic shared memory.
-template <typename R>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend_packet(const __grid_constant__ DevScene<R> S,
-                                                                  const WfRay<R> *rays, const WfCounters *C, int which,
-                                                                  WfHit<R> *hits)
-{
-    const int n = C->ray_count[which];
-    const int stride = gridDim.x * blockDim.x;
-    const int n_round = (n + stride - 1) / stride * stride;
-    int *wstk = mt_stack_smem + (threadIdx.x >> 5) * (S.stack_depth > 0 ? S.stack_depth : 1);
-    TravCount cnt;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
-        const bool live = q < n;
-        V3<R> o = v3(R(0), R(0), R(0)), d = v3(R(0), R(0), R(1));
-        if (live) {
-            const WfRay<R> r = rays[q];
-            o = v3(r.o[0], r.o[1], r.o[2]);
-            d = unit_dir(v3(r.d[0], r.d[1], r.d[2]));
-        }
-        const RayPre<R> rp = ray_pre(o, d);
-        Hit<R> h;
-        const bool found = warp_nearest2(S, rp, R(1e-4), R(1e30), live, wstk, &h, cnt);
-        if (live) {
-            WfHit<R> out;
-            if (found) {
-                out.t = h.t;
-                out.u = h.u;
-                out.v = h.v;
-                out.prim = h.prim;
-                out.code = h.code;
-            } else {
-                out.t = R(0);
-                out.u = R(0);
-                out.v = R(0);
-                out.prim = -1;
-                out.code = 0;
-            }
-            hits[q] = out;
-            if (S.trace_rec) trace_put(S, o, d, out.t, out.prim, 0, 0, 0);
-        }
-    }
-    trav_count_flush<R, false>(S, cnt);
-    if (S.counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S.counters->extension_rays, (unsigned long long)n);
-}
-
 template <typename R> MT_D void gather_nee(const DevScene<R> &S, R *nee_slot, V3<R> *radiance)
 {
     V3<R> sum = v3(R(0), R(0), R(0));
@@ -928,56 +880,6 @@ __global__ void __launch_bounds__(kWfMaxBlock, 8) k_wf_shadow_cache(const __grid
         const int at = warp_append(&C->walk_count, miss);
         if (miss) walk[at] = q;
     }
-}
-
-// Second pass with the packet walk (MT_TRAVERSAL_PACKET): the connections the
-// cached leaves did not resolve (`walk`), 32 consecutive ones per warp walked
-// together (warp_any2). Consecutive connections leave nearby points of one
-// pixel block toward one light, so they share most nodes. A blocking leaf
-// goes to the front of the connection's cache entry, as in scene_any_cached.
-// Each warp's stack takes stack_depth ints of the dynamic shared memory.
-template <typename R, bool ADJ>
-__global__ void __launch_bounds__(kWfMaxBlock, 7) k_wf_shadow_packet(const __grid_constant__ DevScene<R> S,
-                                                                  const WfShadow<R> *sq, const WfCounters *C, R *nee,
-                                                                  R *att, int *occ_cache, int wh, int b,
-                                                                  const int *walk)
-{
-    const int n = C->walk_count;
-    const int stride = gridDim.x * blockDim.x;
-    const int n_round = (n + stride - 1) / stride * stride;
-    int *wstk = mt_stack_smem + (threadIdx.x >> 5) * (S.stack_depth > 0 ? S.stack_depth : 1);
-    TravCount cnt;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
-        const bool live = q < n;
-        WfShadow<R> s;
-        RayPre<R> rp;
-        int *entry = nullptr;
-        int c0 = -1;
-        s.tmax = R(0);
-        if (live) {
-            s = sq[walk[q]];
-            rp = ray_pre(v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2])));
-            entry = occ_entry(S, occ_cache, wh, b, s);
-            c0 = entry[0];
-        }
-        int leaf = -1;
-        const bool occ = warp_any2(S, rp, R(1e-3), s.tmax, live, wstk, &leaf, cnt);
-        if (live) {
-            if (occ && leaf != -1 && leaf != c0) {
-                const int4 e = *reinterpret_cast<const int4 *>(entry);
-                *reinterpret_cast<int4 *>(entry) = make_int4(leaf, e.x, e.y, e.z);
-            }
-            V3<R> atten = v3(R(1), R(1), R(1));
-            if (!occ && s.li == kMaxLights)
-                atten = scale(atten, cloud_transmittance(S.sky, v3(s.o[0], s.o[1], s.o[2]), v3(s.d[0], s.d[1], s.d[2])));
-            AbsorbPath<R> ab;
-            ab.mat[0] = ab.mat[1] = -1;
-            ab.dist[0] = ab.dist[1] = R(0);
-            shadow_result<R, ADJ>(s, occ, atten, ab, nee, att);
-            if (S.trace_rec) trace_put(S, rp.o, rp.d, s.tmax, occ ? 1 : 0, 1, b, s.li);
-        }
-    }
-    trav_count_flush<R, true>(S, cnt);
 }
 
 // ------------------------------------------------------------------

@@ -186,8 +186,7 @@ void launch_extend(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
 
 template <typename R, bool ADJ, int W>
 void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
-                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk,
-                   bool packet = false)
+                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk)
 {
     if (S.has_passthrough) {
         k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
@@ -196,10 +195,7 @@ void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
     } else if (occ && walk) {
         // cached occluders first, then the tree walk for the misses
         k_wf_shadow_cache<R, ADJ><<<g, block, 0, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
-        if (sizeof(R) == 4 && W == 2 && packet && b == 0)
-            k_wf_shadow_packet<R, ADJ><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
-        else
-            k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
+        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
     } else {
         k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
     }
@@ -207,14 +203,13 @@ void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
 
 template <typename R, bool ADJ>
 void launch_shadow_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
-                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk,
-                     bool packet = false)
+                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk)
 {
     if constexpr (sizeof(R) == 4) {
         if (W == 4) return launch_shadow<R, ADJ, 4>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
         if (W == 8) return launch_shadow<R, ADJ, 8>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
     }
-    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk, packet);
+    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
 }
 
 template <typename R>
@@ -259,7 +254,7 @@ template <typename R> int wf_reserve_sort(WavefrontState *st, int buckets)
 template <typename R>
 int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch_spp, int n_batches, int depth,
                cudaStream_t s, bool prof, int block, bool adjoint = false, bool dyn = false,
-               const void *params = nullptr, int sort_threshold = 0, bool packet = false)
+               const void *params = nullptr, int sort_threshold = 0)
 {
     const int wh = w * h;
     const int n_paths = wh * batch_spp;
@@ -311,10 +306,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         int which = 0;
         for (int b = 0; b <= depth; ++b) {
             tic();
-            if (sizeof(R) == 4 && packet && b == 0 && W == 2)
-                k_wf_extend_packet<R><<<g, block, smem, s>>>(S, rays[which], C, which, hits);
-            else
-                launch_extend_w<R>(W, dyn, g, block, smem_w, s, S, rays[which], C, which, hits);
+            launch_extend_w<R>(W, dyn, g, block, smem_w, s, S, rays[which], C, which, hits);
             toc(0);
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
             // shadow_count, shadow_fetch, ray_fetch (the next extend's), sorted
@@ -361,7 +353,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
                                          (int *)st->walk);
             else
                 launch_shadow_w<R, false>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, nullptr, occ, wh, b,
-                                          (int *)st->walk, packet);
+                                          (int *)st->walk);
             toc(2);
             which ^= 1;
         }
@@ -456,8 +448,6 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     // rays, NEE rays grouped by light) the grid-stride kernels are faster, so
     // they are the default and dynamic fetch is a tuning candidate
     const bool dyn = opts && opts->traversal == MT_TRAVERSAL_DYNAMIC;
-    // packet walk of the bounce-0 shadow connections the occluder cache left
-    const bool packet = opts && opts->traversal == MT_TRAVERSAL_PACKET;
     std::string &exec_key = adjoint ? st->adj_key : st->key;
     if (use_graph) {
         char key[256];
@@ -465,14 +455,14 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         // its identity, counters and parameter version are part of the key
         snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d:%d:%d:%d:%p:%d", (int)sizeof(R), w, h, batch_spp,
                  n_batches, depth, (const void *)S.nodes, (const void *)S.counters, S.version, (int)dyn, block,
-                 sort_threshold, S.bvh_width, (const void *)S.trace_rec, (int)st->occ_cache_on + 2 * (int)packet);
+                 sort_threshold, S.bvh_width, (const void *)S.trace_rec, (int)st->occ_cache_on);
         if (!exec || exec_key != key) {
             if (exec) cudaGraphExecDestroy(exec);
             exec = nullptr;
             if (!st->cap_stream) WF_CK(cudaStreamCreateWithFlags(&st->cap_stream, cudaStreamNonBlocking), "stream");
             WF_CK(cudaStreamBeginCapture(st->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
             int erc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, st->cap_stream, false, block, adjoint,
-                                    dyn, nullptr, sort_threshold, packet);
+                                    dyn, nullptr, sort_threshold);
             cudaGraph_t graph = nullptr;
             cudaError_t ce = cudaStreamEndCapture(st->cap_stream, &graph);
             if (erc) {
@@ -488,7 +478,7 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         WF_CK(cudaGraphLaunch(exec, stream), "graph launch");
     } else {
         rc = wf_enqueue<R>(st, S, w, h, batch_spp, n_batches, depth, stream, prof, block, adjoint, dyn, nullptr,
-                           sort_threshold, packet);
+                           sort_threshold);
         if (rc) return rc;
     }
     if (ev1) WF_CK(cudaEventRecord(ev1, stream), "cudaEventRecord");
