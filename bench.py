@@ -503,7 +503,7 @@ def run_ours(args):
 
 
 def rmse_bench(torch, mt, desc, device: int, opts: dict, w: int = 480, h: int = 270, n_conv: int = 16384,
-               n_max: int = 1024, chunk: int = 64):
+               n_max: int = 1024, chunk: int = 64, target: float | None = None):
     """Time to RMSE on 480x270 frames of the benchmark scene and view.
 
     A converged image of `n_conv` samples per pixel (FP32 wavefront, 16
@@ -512,7 +512,9 @@ def rmse_bench(torch, mt, desc, device: int, opts: dict, w: int = 480, h: int = 
     every pixel in windows of `chunk` samples, accumulating, with device time
     per window; at 64, 128, ..., n_max samples the RMSE (linear RGB) against
     the converged image is taken. The measured RMSE includes the converged
-    image's own noise, sigma^2 / n_conv; `rmse_vs_exact` subtracts it."""
+    image's own noise, sigma^2 / n_conv; `rmse_vs_exact` subtracts it.
+    `target`: each integrator stops at the first checkpoint where
+    rmse_vs_exact <= target, and the summary gives the time to it."""
     from marmel_trace_b200 import _capi
 
     cam = desc.make_camera(w, h)
@@ -526,11 +528,17 @@ def rmse_bench(torch, mt, desc, device: int, opts: dict, w: int = 480, h: int = 
     gw = mt.GpuScene(desc, precision="fp32", integrator="wavefront", device=device, **opts)
     k_win = 16
     per = n_conv // k_win
+    # the converged image in windows of at most 1024 samples, summed per part
+    part = torch.zeros((h, w, 3), dtype=torch.float64, device="cuda")
     wins = []
     t0 = time.perf_counter()
+    step = min(per, 1024)
     for k in range(k_win):
-        window(gw, 5_000_000 + k * per, 5_000_000 + (k + 1) * per, 0)
-        wins.append((acc.double() / per).cpu().numpy())
+        part.zero_()
+        for s0 in range(5_000_000 + k * per, 5_000_000 + (k + 1) * per, step):
+            window(gw, s0, s0 + step, 0)
+            part += acc.double()
+        wins.append((part / per).cpu().numpy())
     conv_s = time.perf_counter() - t0
     wins = np.stack(wins)
     conv = wins.mean(0)
@@ -561,15 +569,19 @@ def rmse_bench(torch, mt, desc, device: int, opts: dict, w: int = 480, h: int = 
                 exact = float(np.sqrt(max(rmse ** 2 - conv_noise ** 2, 0.0)))
                 rows.append({"spp": n, "seconds": round(t_cum, 4), "rmse": round(rmse, 6),
                              "rmse_vs_exact": round(exact, 6)})
+                if target is not None and exact <= target:
+                    break
         curves[name] = rows
     gw.release()
     gm.release()
     last_w, last_p = curves["wavefront"][-1], curves["plain_gpu"][-1]
-    target = max(last_w["rmse"], last_p["rmse"])
+    key = "rmse" if target is None else "rmse_vs_exact"
+    if target is None:
+        target = max(last_w["rmse"], last_p["rmse"])
 
     def time_to(rows, tau):
         for r in rows:
-            if r["rmse"] <= tau:
+            if r[key] <= tau:
                 return r["seconds"], r["spp"]
         return None, None
 
@@ -580,7 +592,8 @@ def rmse_bench(torch, mt, desc, device: int, opts: dict, w: int = 480, h: int = 
     rate_p = last_p["spp"] * w * h / last_p["seconds"]
     summary = {"frame": f"{w}x{h}, depth {DEPTH}, same scene and view", "converged_spp": n_conv,
                "converged_noise_rmse": round(conv_noise, 6), "sigma2_per_sample": round(sigma2, 5),
-               "target_rmse": round(target, 6), "wavefront_s": tw, "plain_gpu_s": tp, "spp_at_target": [nw, np_],
+               "target_rmse": round(target, 6), "target_against": key,
+               "wavefront_s": tw, "plain_gpu_s": tp, "spp_at_target": [nw, np_],
                "ratio": round(tp / tw, 3) if tw and tp else None,
                "rmse_1e-3": {"spp_needed": round(n_star), "wavefront_s_est": round(n_star * w * h / rate_w, 1),
                              "plain_gpu_s_est": round(n_star * w * h / rate_p, 1)},
@@ -917,6 +930,9 @@ def main():
         ap.add_argument(f"--no-{leg}", action="store_true")
     ap.add_argument("--queue-capacity", type=int, default=0,
                     help="path slots per wavefront batch (0: the library default, 32M)")
+    ap.add_argument("--rmse-target", type=float, default=0.0,
+                    help="only measure the time of both integrators to this RMSE against the exact image "
+                         "(480x270, 262,144-spp converged reference, 1024-spp windows); prints its own JSON line")
     ap.add_argument("--profile-case", action="store_true",
                     help="only render the small profiling case (480x270, 16 spp, depth 8, plain launches) twice, "
                          "for ncu captures of the stage kernels; prints nothing")
@@ -924,6 +940,19 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
         profile_case()
+        return
+    if args.rmse_target > 0:
+        import torch
+
+        import marmel_trace_b200 as mt
+
+        torch.cuda.set_device(0)
+        desc = build_scene()
+        with ClockSampler(0, "_rmse") as clk:
+            summary, detail = rmse_bench(torch, mt, desc, 0, {}, n_conv=262144, n_max=131072, chunk=1024,
+                                         target=args.rmse_target)
+        summary["clocks"] = clk.summary()
+        print(json.dumps({"time_to_rmse": summary, "curves": detail["curves"]}), flush=True)
         return
     if args.impl == "reference":
         run_reference(args)
