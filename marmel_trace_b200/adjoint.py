@@ -63,13 +63,20 @@ class DiffRenderer:
 
 
 class RenderFunction(torch.autograd.Function):
-    """image = RenderFunction.apply(params, renderer, s0)."""
+    """image = RenderFunction.apply(params, renderer, s0, s0_replay).
+
+    The forward renders the sample window starting at s0; the backward
+    replays the window starting at s0_replay (default: s0). For a loss that is
+    not linear in the image (an L2 loss) the two should differ: with the same
+    samples the image and its derivative are correlated, and the product in
+    dL/dparams = dL/dimage . dimage/dparams is then a biased estimate of the
+    gradient of the expected loss."""
 
     @staticmethod
-    def forward(ctx, params: torch.Tensor, renderer: DiffRenderer, s0: int = 0):
+    def forward(ctx, params: torch.Tensor, renderer: DiffRenderer, s0: int = 0, s0_replay: int | None = None):
         renderer.set_params(params.detach().cpu().numpy())
         ctx.renderer = renderer
-        ctx.s0 = s0
+        ctx.s0 = s0 if s0_replay is None else s0_replay
         ctx.dtype = params.dtype
         ctx.device = params.device
         return renderer.render(s0)
@@ -77,4 +84,4 @@ class RenderFunction(torch.autograd.Function):
     @staticmethod
     def backward(ctx, grad_image: torch.Tensor):
         g = ctx.renderer.backward(grad_image, ctx.s0)
-        return g.to(device=ctx.device, dtype=ctx.dtype), None, None
+        return g.to(device=ctx.device, dtype=ctx.dtype), None, None, None

@@ -8,10 +8,14 @@ perturbs them by N(0, 0.15) and clips to the valid ranges (albedo and
 metallic in [0, 1], roughness in [0.01, 1], emissive and sun >= 0). Each step
 renders a fresh sample window (so the noise decorrelates between steps),
 takes the L2 image loss and its gradient through RenderFunction, and applies
-an Adam update. The learning rate follows a cosine from `lr` down to lr / 20:
-once the loss reaches its Monte-Carlo noise floor the gradients of weakly
-observed parameters (roughness, metallic) are mostly noise, and Adam's
-normalised steps would otherwise walk them at the full rate.
+an Adam update. The adjoint replays a different sample window than the one
+the loss sees: with the same samples the image and its derivative are
+correlated, which biases the gradient of an L2 loss (toward parameters that
+lower the image's variance rather than its error). The learning rate follows
+a cosine from `lr` down to lr / 20: once the loss reaches its Monte-Carlo
+noise floor the gradients of weakly observed parameters (roughness,
+metallic) are mostly noise, and Adam's normalised steps would otherwise walk
+them at the full rate.
 
 The parameter error is reported per group (albedo, roughness, metallic,
 emissive, sun; the absorption parameters do not act on this scene, which has
@@ -88,7 +92,9 @@ def run(steps: int = 200, width: int = 512, height: int = 512, spp: int = 32, de
         for grp in opt.param_groups:
             grp["lr"] = lr * (0.05 + 0.95 * 0.5 * (1.0 + math.cos(math.pi * k / max(steps - 1, 1))))
         opt.zero_grad()
-        img = RenderFunction.apply(params, r, spp * k)
+        # the loss sees window 2k, the adjoint replays window 2k + 1: an
+        # unbiased estimate of the gradient of the expected L2 loss
+        img = RenderFunction.apply(params, r, spp * 2 * k, spp * (2 * k + 1))
         loss = ((img - target) ** 2).mean()
         loss.backward()
         opt.step()
