@@ -105,6 +105,15 @@ template <typename R> MT_D V3<R> adj_of_path(const WfParams<R> *P, int slot)
 // allocation is tuned for the 128-thread bound.
 static constexpr int kWfMaxBlock = 128;
 
+// Blocks of 128 per SM the binary-tree walks are compiled for (the register
+// budget, 65536 / (128 * blocks)): extend and the any-hit shadow walk.
+#ifndef MT_EXTEND_MIN_BLOCKS
+#define MT_EXTEND_MIN_BLOCKS 0
+#endif
+#ifndef MT_SHADOW_MIN_BLOCKS
+#define MT_SHADOW_MIN_BLOCKS 7
+#endif
+
 struct WfCounters {
     int ray_count[2];
     int shadow_count;
@@ -207,7 +216,7 @@ __global__ void k_wf_generate(const __grid_constant__ DevScene<R> S, const WfPar
 // extend: nearest hit (scene_intersect, src/scene.c:767 -> src/bvh.c:557)
 // ------------------------------------------------------------------
 template <typename R, int W>
-__global__ void __launch_bounds__(kWfMaxBlock) k_wf_extend(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? MT_EXTEND_MIN_BLOCKS : 0) k_wf_extend(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays, const WfCounters *C,
                                                    int which, WfHit<R> *hits)
 {
     const int n = C->ray_count[which];
@@ -809,7 +818,7 @@ MT_D void shadow_result(const WfShadow<R> &s, bool occ, V3<R> atten, const Absor
 template <typename R, bool ADJ, int W, bool PASS>
 // (binary tree: at most 72 registers, so 7 blocks of 128 fit an SM; the
 // pass-through instantiation would otherwise take 80 and run 6)
-__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? 7 : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? MT_SHADOW_MIN_BLOCKS : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
                                                    R *nee, R *att, int *occ_cache, int wh, int b, const int *walk)
 {
     const int n = walk ? C->walk_count : C->shadow_count;
