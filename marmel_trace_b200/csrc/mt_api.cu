@@ -390,11 +390,6 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
 
     S->node_count = fb.node_count;
     S->stack_depth = fb.depth + 1;  // pushes happen only on the way down
-    // the largest |coordinate| of the root node's two child boxes (every
-    // primitive of the tree lies inside them): bounds the FP32 slab slack
-    S->coord_bound = 0.0f;
-    if (fb.node_count > 0)
-        for (int k = 0; k < 12; ++k) S->coord_bound = fmaxf(S->coord_bound, fabsf(fb.nodes[k]));
     S->bvh_width = 2;
     S->wide_stack_depth = 0;
     if (sizeof(R) == 4) {

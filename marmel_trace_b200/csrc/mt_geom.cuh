@@ -29,9 +29,6 @@ template <typename R> struct Hit {
 template <typename R> struct RayPre {
     V3<R> o, d, inv;
     V3<R> oi;  // o * inv: an FP32 slab distance is one fma, box * inv - oi
-    // FP32: the per-ray part of the slab slack (node_test):
-    // 10 * 2^-24 max |o_k| + 3 * 2^-24 max |oi_k| (axes with a finite inverse)
-    float slack_ray;
     // watertight-triangle shear (FP32 path)
     int kx, ky, kz;
     float sx, sy, sz;
@@ -53,15 +50,6 @@ template <typename R> MT_D RayPre<R> ray_pre(V3<R> o, V3<R> d)
         p.inv.z = fabsf(d.z) < 1e-30f ? copysignf(1e30f, d.z) : p.inv.z;
     }
     p.oi = v3<R>(o.x * p.inv.x, o.y * p.inv.y, o.z * p.inv.z);
-    p.slack_ray = 0.0f;
-    if constexpr (sizeof(R) == 4) {
-        float m = 0.0f;
-        if (fabsf(d.x) >= 1e-30f) m = fmaxf(m, fabsf(p.oi.x));
-        if (fabsf(d.y) >= 1e-30f) m = fmaxf(m, fabsf(p.oi.y));
-        if (fabsf(d.z) >= 1e-30f) m = fmaxf(m, fabsf(p.oi.z));
-        const float om = fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fabsf(o.z));
-        p.slack_ray = fmaf(10.0f * 0x1p-24f, om, 3.0f * 0x1p-24f * m);
-    }
     float ax = fabsf((float)d.x), ay = fabsf((float)d.y), az = fabsf((float)d.z);
     int kz = (ax > ay) ? ((ax > az) ? 0 : 2) : ((ay > az) ? 1 : 2);
     int kx = kz + 1 == 3 ? 0 : kz + 1;
@@ -516,23 +504,12 @@ MT_D bool prim_occluded(const DevScene<R> &S, int code, const RayPre<R> &rp, R t
 //
 // FP32: one fma per slab plane (box * inv - o * inv). FP64: the reference's
 // (box - o) * inv.
-//
-// FP32 boxes are tested conservatively: a slab distance fma(box, inv, -oi)
-// differs from (box - o) / d by at most 2^-23 |t| + 2^-24 |oi| (the roundings
-// of inv, oi and the fma). A distance matters only while |t| is below a bound
-// of the scene (every hit point has |p_k| <= coord_bound, so t <= 2
-// (coord_bound + max |o_k|)); beyond it no primitive of the box can be hit.
-// So each interval's exit is moved out by `slack` = 10 * 2^-24 (coord_bound +
-// max |o_k|) + 3 * 2^-24 max |oi_k|, which covers the error of both ends, and
-// a box the ray meets in exact arithmetic is never culled (cf. Ize, "Robust
-// BVH Ray Traversal", JCGT 2013, which scales the exit distance for the same
-// reason). One add per child box.
 template <typename R>
 MT_D void node_test(const float4 q0, const float4 q1, const float4 q2, const RayPre<R> &rp, R tmin, R tmax,
-                    R slack, bool *hl, bool *hr, R *tl, R *tr);
+                    bool *hl, bool *hr, R *tl, R *tr);
 template <>
 MT_D void node_test<float>(const float4 q0, const float4 q1, const float4 q2, const RayPre<float> &rp, float tmin,
-                           float tmax, float slack, bool *hl, bool *hr, float *tl, float *tr)
+                           float tmax, bool *hl, bool *hr, float *tl, float *tr)
 {
     float lx0 = fmaf(q0.x, rp.inv.x, -rp.oi.x), lx1 = fmaf(q0.y, rp.inv.x, -rp.oi.x);
     float ly0 = fmaf(q0.z, rp.inv.y, -rp.oi.y), ly1 = fmaf(q0.w, rp.inv.y, -rp.oi.y);
@@ -544,9 +521,6 @@ MT_D void node_test<float>(const float4 q0, const float4 q1, const float4 q2, co
     float lexit = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fmaxf(lz0, lz1));
     float renter = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fminf(rz0, rz1));
     float rexit = fminf(fminf(fmaxf(rx0, rx1), fmaxf(ry0, ry1)), fmaxf(rz0, rz1));
-    lexit += slack;
-    rexit += slack;
-    tmax += slack;
     *hl = (lexit >= lenter && lexit >= tmin && lenter <= tmax);
     *hr = (rexit >= renter && rexit >= tmin && renter <= tmax);
     *tl = lenter < tmin ? tmin : lenter;
@@ -554,7 +528,7 @@ MT_D void node_test<float>(const float4 q0, const float4 q1, const float4 q2, co
 }
 template <>
 MT_D void node_test<double>(const float4 q0, const float4 q1, const float4 q2, const RayPre<double> &rp, double tmin,
-                            double tmax, double, bool *hl, bool *hr, double *tl, double *tr)
+                            double tmax, bool *hl, bool *hr, double *tl, double *tr)
 {
     using R = double;
     R lx0 = (R(q0.x) - rp.o.x) * rp.inv.x, lx1 = (R(q0.y) - rp.o.x) * rp.inv.x;
@@ -754,7 +728,6 @@ template <typename R>
 MT_D int descend2(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp, int *stk, int stride, TravCount &c)
 {
     const int cap = S.stack_depth;
-    const R slack = sizeof(R) == 4 ? R(fmaf(10.0f * 0x1p-24f, S.coord_bound, (float)tv.rp.slack_ray)) : R(0);
     while (node >= 0) {
         const float4 *Nd = S.nodes + 4 * (size_t)node;
         float4 q0 = __ldg(Nd), q1 = __ldg(Nd + 1), q2 = __ldg(Nd + 2);
@@ -762,7 +735,7 @@ MT_D int descend2(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp, in
         bool hl, hr;
         R tl, tr;
         ++c.nvis;
-        node_test(q0, q1, q2, tv.rp, tv.tmin, tv.closest, slack, &hl, &hr, &tl, &tr);
+        node_test(q0, q1, q2, tv.rp, tv.tmin, tv.closest, &hl, &hr, &tl, &tr);
         if (hl && hr) {
             bool lnear = tl <= tr;
             int nearc = lnear ? q3.x : q3.y;
@@ -788,7 +761,7 @@ MT_D int descend2(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp, in
 // Slab test of one child box (the arithmetic of node_test).
 template <typename R>
 MT_D bool box_hit(float lx, float hx, float ly, float hy, float lz, float hz, const RayPre<R> &rp, R tmin, R tmax,
-                  R slack, R *enter)
+                  R *enter)
 {
     static_assert(sizeof(R) == 4, "wide trees are an FP32 path");
     R x0 = fmaf(lx, rp.inv.x, -rp.oi.x), x1 = fmaf(hx, rp.inv.x, -rp.oi.x);
@@ -796,10 +769,8 @@ MT_D bool box_hit(float lx, float hx, float ly, float hy, float lz, float hz, co
     R z0 = fmaf(lz, rp.inv.z, -rp.oi.z), z1 = fmaf(hz, rp.inv.z, -rp.oi.z);
     R en = mfmax(mfmax(mfmin(x0, x1), mfmin(y0, y1)), mfmin(z0, z1));
     R ex = mfmin(mfmin(mfmax(x0, x1), mfmax(y0, y1)), mfmax(z0, z1));
-    // conservative as in node_test<float>
-    ex += slack;
     *enter = en < tmin ? tmin : en;
-    return ex >= en && ex >= tmin && en <= tmax + slack;
+    return ex >= en && ex >= tmin && en <= tmax;
 }
 
 // Descend the wide tree (W = 4 or 8 children per node): test every child box,
@@ -811,7 +782,6 @@ MT_D int descend_wide(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp
 {
     constexpr int G = W / 4;  // float4 words per coordinate row
     const int cap = S.wide_stack_depth;
-    const R slack = R(fmaf(10.0f * 0x1p-24f, S.coord_bound, (float)tv.rp.slack_ray));
     while (node >= 0) {
         const float4 *Nd = S.wnodes + (size_t)(8 * G) * node;
         ++c.nvis;
@@ -829,13 +799,13 @@ MT_D int descend_wide(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp
             ch[b + 1] = cc.y;
             ch[b + 2] = cc.z;
             ch[b + 3] = cc.w;
-            if (cc.x != kEmpty && box_hit(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, tv.rp, tv.tmin, tv.closest, slack, &d[b]))
+            if (cc.x != kEmpty && box_hit(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, tv.rp, tv.tmin, tv.closest, &d[b]))
                 mask |= 1u << b;
-            if (cc.y != kEmpty && box_hit(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, tv.rp, tv.tmin, tv.closest, slack, &d[b + 1]))
+            if (cc.y != kEmpty && box_hit(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, tv.rp, tv.tmin, tv.closest, &d[b + 1]))
                 mask |= 2u << b;
-            if (cc.z != kEmpty && box_hit(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, tv.rp, tv.tmin, tv.closest, slack, &d[b + 2]))
+            if (cc.z != kEmpty && box_hit(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, tv.rp, tv.tmin, tv.closest, &d[b + 2]))
                 mask |= 4u << b;
-            if (cc.w != kEmpty && box_hit(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, tv.rp, tv.tmin, tv.closest, slack, &d[b + 3]))
+            if (cc.w != kEmpty && box_hit(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, tv.rp, tv.tmin, tv.closest, &d[b + 3]))
                 mask |= 8u << b;
         }
         if (!mask) {

@@ -171,7 +171,6 @@ template <typename R> struct DevScene {
     int bvh_width;         // 2, or 4 / 8 when `wnodes` is present
     int wide_stack_depth;  // stack entries per thread for the wide tree
     int version;           // bumped whenever material / sun parameters change
-    float coord_bound;     // largest |coordinate| of the FP32 root box (bounds the slab slack)
     R water_level;
     DevOcean<R> ocean;
     DevSky<R> sky;
