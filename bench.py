@@ -179,12 +179,14 @@ def build_scene():
     return scenes.torus_field_scene()
 
 
-# DRAM and L2 bytes per path sample of the stage kernels, from the committed
-# ncu capture of the current kernels (profiles/). None until a capture of the
-# current code exists; the roofline then carries traffic = null.
-TRAFFIC = {"shadow": {"dram_bytes_per_sample": None, "l2_bytes_per_sample": None},
-           "extend": {"dram_bytes_per_sample": None, "l2_bytes_per_sample": None},
-           "source": None}
+# DRAM and L2 bytes per path sample of the stage kernels, from the ncu capture
+# of the stage kernels on the 480x270, 16-spp profiling case (bounces 0-4
+# measured, scaled to all bounces by the launch-list time; summarised in
+# profiles/wavefront_stages_torus480x270.md). The stage traffic is the queue
+# records plus the tree, so it follows the samples.
+TRAFFIC = {"shadow": {"dram_bytes_per_sample": 482.0 + 331.0, "l2_bytes_per_sample": 1777.0 + 2865.0},
+           "extend": {"dram_bytes_per_sample": 122.0, "l2_bytes_per_sample": 1727.0},
+           "source": "ncu capture of the stage kernels, 480x270 x 16 spp (profiles/wavefront_stages_torus480x270.md)"}
 
 
 def traversal_bytes(st, kind: str, width: int = 2) -> float:
