@@ -1019,74 +1019,6 @@ MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R 
     return tv.found;
 }
 
-// Nearest hit seeded from a cache entry of WAYS triangle codes (kind << 28 |
-// slot, newest first, -1 empty): each cached triangle is tested against
-// [tmin, tmax] first, and the nearest of those hits (ties to the lower prim
-// index) starts the walk as its current best, so the walk culls everything
-// beyond it. A cached triangle's hit is a hit of this query, so the result is
-// the query's nearest hit under the reference's rules, as without the seed.
-// The triangle of the final hit goes to the front of the entry (triangles
-// only: the prim index of a cached code must be recoverable for the tie rule).
-template <typename R, int WAYS>
-MT_D bool scene_nearest_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best, int *cache)
-{
-    Hit<R> seed;
-    bool seeded = false;
-    int c[WAYS];
-    if constexpr (WAYS == 4) {
-        const int4 e = *reinterpret_cast<const int4 *>(cache);
-        c[0] = e.x;
-        c[1] = e.y;
-        c[2] = e.z;
-        c[3] = e.w;
-    } else {
-#pragma unroll
-        for (int k = 0; k < WAYS; ++k) c[k] = cache[k];
-    }
-    TravCount cnt;
-#pragma unroll
-    for (int k = 0; k < WAYS; ++k) {
-        if (c[k] < 0) break;
-        R t, u, v;
-        ++cnt.ntest;
-        ++cnt.ntri;
-        if (tri_t(S, c[k] & 0x0FFFFFFF, rp, tmin, tmax, &t, &u, &v)) {
-            const int pi = tri_prim_index(S, c[k] & 0x0FFFFFFF);
-            if (!seeded || t < seed.t || (t == seed.t && pi < seed.prim)) {
-                seed.t = t;
-                seed.u = u;
-                seed.v = v;
-                seed.prim = pi;
-                seed.code = c[k];
-                seeded = true;
-            }
-        }
-    }
-    Trav<R> tv;
-    trav_init<R, false>(S, tv, rp, tmin, seeded ? seed.t : tmax, best, cnt);
-    if (seeded) {
-        if (!tv.found || seed.t < best->t || (seed.t == best->t && seed.prim < best->prim)) *best = seed;
-        tv.found = true;
-        tv.closest = best->t;
-    }
-    if (tv.node != kEmpty) {
-        int *stk = mt_stack_smem + threadIdx.x;
-        while (trav_step<R, false, 2>(S, tv, stk, blockDim.x, best, cnt)) {
-        }
-    }
-    trav_count_flush<R, false>(S, cnt);
-    if (tv.found && (best->code >> 28) == KIND_TRIANGLE && best->code != c[0]) {
-        if constexpr (WAYS == 4) {
-            *reinterpret_cast<int4 *>(cache) = make_int4(best->code, c[0], c[1], c[2]);
-        } else {
-#pragma unroll
-            for (int k = WAYS - 1; k > 0; --k) cache[k] = c[k - 1];
-            cache[0] = best->code;
-        }
-    }
-    return tv.found;
-}
-
 // scene_intersect / scene_occluded entry semantics: a direction that is not
 // unit length (|d|^2 off by more than 1e-12) is normalised first
 // (src/bvh.c:563-566, :720-723).

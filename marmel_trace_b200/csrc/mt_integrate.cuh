@@ -309,50 +309,6 @@ template <typename R> struct AbsorbPath {
     R dist[2];
 };
 
-// pt_occluded_segment with the first link's nearest hit seeded from the
-// occluder cache entry `entry` (scene_nearest_cached: triangles that blocked
-// or were first met from this pixel / place toward this light). The seed only
-// lets the walk cull beyond a hit it already knows, so every link -- and the
-// answer and attenuation -- is pt_occluded_segment's. entry == NULL: no seed.
-template <typename R>
-MT_D bool pt_occluded_segment_cached(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax, V3<R> *attenuation,
-                                     int *entry)
-{
-    if (!entry || !S.has_passthrough) return pt_occluded_segment(S, o, d, tmin, tmax, attenuation);
-    *attenuation = v3(R(1), R(1), R(1));
-    V3<R> cur_o = o;
-    R remaining = tmax;
-    if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
-    for (int step = 0; step < 6; ++step) {
-        SurfaceHit<R> h;
-        if (step == 0) {
-            const V3<R> du = unit_dir(d);
-            Hit<R> hh;
-            if (S.counters) atomicAdd(&S.counters->extension_rays, 1ull);
-            if (!scene_nearest_cached<R, 4>(S, ray_pre(cur_o, du), tmin, remaining, &hh, entry)) return false;
-            finish_hit(S, cur_o, du, hh, &h);
-        } else if (!scene_intersect(S, cur_o, d, tmin, remaining, &h)) {
-            return false;
-        }
-        if (h.material < 0 || h.material >= S.material_count) return true;
-        const DevMaterial<R> &m = S.materials[h.material];
-        if (m.is_water || m.transparency > R(0.8)) {
-            if (m.beer_lambert || m.is_water) {
-                V3<R> seg = v3(mexp(-m.absorption[0] * h.t), mexp(-m.absorption[1] * h.t),
-                               mexp(-m.absorption[2] * h.t));
-                *attenuation = mul(*attenuation, seg);
-            }
-            cur_o = add(h.point, scale(d, R(1e-3)));
-            remaining -= h.t;
-            if (remaining <= R(1e-3)) return false;
-            tmin = R(1e-3);
-            continue;
-        }
-        return true;
-    }
-    return true;
-}
-
 // pt_occluded_segment with the same result and attenuation, also reporting
 // the absorbing materials passed and the distance factor of each one: the
 // attenuation is prod exp(-absorption * t) over the passed hits, so

@@ -113,10 +113,6 @@ static constexpr int kWfMaxBlock = 128;
 #ifndef MT_SHADOW_MIN_BLOCKS
 #define MT_SHADOW_MIN_BLOCKS 7
 #endif
-// the chained pass-through walk (scenes with water or glass)
-#ifndef MT_PASS_MIN_BLOCKS
-#define MT_PASS_MIN_BLOCKS 7
-#endif
 
 struct WfCounters {
     int ray_count[2];
@@ -822,7 +818,7 @@ MT_D void shadow_result(const WfShadow<R> &s, bool occ, V3<R> atten, const Absor
 template <typename R, bool ADJ, int W, bool PASS>
 // (binary tree: at most 72 registers, so 7 blocks of 128 fit an SM; the
 // pass-through instantiation would otherwise take 80 and run 6)
-__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOCKS : MT_SHADOW_MIN_BLOCKS) : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? MT_SHADOW_MIN_BLOCKS : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
                                                    R *nee, R *att, int *occ_cache, int wh, int b, const int *walk)
 {
     const int n = walk ? C->walk_count : C->shadow_count;
@@ -836,11 +832,8 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOC
         ab.dist[0] = ab.dist[1] = R(0);
         bool occ;
         if constexpr (PASS) {
-            // the first link's nearest hit is seeded from the occluder cache
-            // (scene_nearest_cached); the adjoint keeps the plain chain
             occ = ADJ ? pt_occluded_segment_abs(S, o, d, R(1e-3), s.tmax, &atten, &ab)
-                      : pt_occluded_segment_cached(S, o, d, R(1e-3), s.tmax, &atten,
-                                                   occ_cache ? occ_entry(S, occ_cache, wh, b, s) : nullptr);
+                      : pt_occluded_segment(S, o, d, R(1e-3), s.tmax, &atten);
         } else {
             // No material lets a shadow ray through: the chained nearest-hit
             // walk stops at its first hit, so it equals an any-hit query.
