@@ -517,14 +517,19 @@ MT_D void node_test<float>(const float4 q0, const float4 q1, const float4 q2, co
     float rx0 = fmaf(q1.x, rp.inv.x, -rp.oi.x), rx1 = fmaf(q1.y, rp.inv.x, -rp.oi.x);
     float ry0 = fmaf(q1.z, rp.inv.y, -rp.oi.y), ry1 = fmaf(q1.w, rp.inv.y, -rp.oi.y);
     float rz0 = fmaf(q2.z, rp.inv.z, -rp.oi.z), rz1 = fmaf(q2.w, rp.inv.z, -rp.oi.z);
-    float lenter = fmaxf(fmaxf(fminf(lx0, lx1), fminf(ly0, ly1)), fminf(lz0, lz1));
-    float lexit = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fmaxf(lz0, lz1));
-    float renter = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fminf(rz0, rz1));
-    float rexit = fminf(fminf(fmaxf(rx0, rx1), fmaxf(ry0, ry1)), fmaxf(rz0, rz1));
-    *hl = (lexit >= lenter && lexit >= tmin && lenter <= tmax);
-    *hr = (rexit >= renter && rexit >= tmin && renter <= tmax);
-    *tl = lenter < tmin ? tmin : lenter;
-    *tr = renter < tmin ? tmin : renter;
+    // Entry clamped to tmin, exit to tmax: a child is hit when its clamped
+    // entry is not past its clamped exit. For every ray whose entry and exit
+    // are not NaN (a nonzero direction leaves at least one axis NaN-free) this
+    // is the test lexit >= lenter && lexit >= tmin && lenter <= tmax, with the
+    // entry distance max(lenter, tmin), in fewer instructions.
+    const float lenter = fmax3f(fminf(lx0, lx1), fminf(ly0, ly1), fmaxf(fminf(lz0, lz1), tmin));
+    const float lexit = fmin3f(fmaxf(lx0, lx1), fmaxf(ly0, ly1), fminf(fmaxf(lz0, lz1), tmax));
+    const float renter = fmax3f(fminf(rx0, rx1), fminf(ry0, ry1), fmaxf(fminf(rz0, rz1), tmin));
+    const float rexit = fmin3f(fmaxf(rx0, rx1), fmaxf(ry0, ry1), fminf(fmaxf(rz0, rz1), tmax));
+    *hl = lenter <= lexit;
+    *hr = renter <= rexit;
+    *tl = lenter;
+    *tr = renter;
 }
 template <>
 MT_D void node_test<double>(const float4 q0, const float4 q1, const float4 q2, const RayPre<double> &rp, double tmin,
