@@ -37,7 +37,9 @@ adjoint      : forward + path-replay backward of the inverse-rendering
                configuration (512x512, 32 spp, depth 6, 355 parameters).
 inverse      : 200 Adam steps of inverse rendering on that configuration.
 batch        : the batched uneven workload (64 scenes) in one graph launch.
-large        : the 10M-triangle water / tree scene at 3840x2160, depth 12.
+large        : the 10M-triangle water / tree scene at 3840x2160, depth 12
+               (cpu_reference_msamples_s: the reference on the same scene and
+               view at 960x540, where the host has the ~36 GB it needs).
 cpu_baseline : the reference's own multithreaded CPU renderer (oracle/_ref)
                on bounded samples of the same workloads.
 
@@ -494,6 +496,8 @@ def run_ours(args):
         if cpu:
             out["cpu_baseline"] = cpu["baseline"]
             out["cpu_more"] = cpu["more"]
+        if large and cpu:
+            large["cpu_reference_msamples_s"] = cpu["more"].get("c5_msamples_s")
         out["large"] = large
         out["batch"] = batch
         out["c1"] = c1
@@ -785,7 +789,8 @@ def cpu_baseline(desc, spp: int, queries=None):
       CPU Mrays/s on those queries;
     * config 1 (path tracer and Whitted), the adjoint configuration's central
       finite-difference gradient cost, and config 3's scenes one after
-      another (a sample of 8 of the 64)."""
+      another (a sample of 8 of the 64), and config 5 at a quarter of its
+      resolution where the host has the memory for it."""
     from marmel_trace_b200 import scenes
     from oracle import ref
 
@@ -861,7 +866,40 @@ def cpu_baseline(desc, spp: int, queries=None):
         n3 += it["width"] * it["height"]
         r3.free()
     more["c3_sequential_msamples_s"] = round(n3 / t3 / 1e6, 3)
+    # config 5: the large scene and view at 960x540, 1 spp, depth 12. The
+    # reference keeps two 1632-byte copies of every primitive (about 36 GB
+    # here), so this runs only with room for it on the host.
+    avail = _host_available_bytes()
+    if avail >= C5_HOST_BYTES:
+        d5 = scenes.large_scene()
+        t0 = time.perf_counter()
+        r5 = ref.RefScene.from_desc(d5, ref.scene_camera(d5, 960, 540))
+        build_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        r5.pathtrace_render(960, 540, 1, 12)
+        t5 = time.perf_counter() - t0
+        r5.free()
+        del d5
+        more["c5_msamples_s"] = round(960 * 540 / t5 / 1e6, 4)
+        more["c5_note"] = (f"pathtrace_render of the large scene and view at 960x540, 1 spp, depth 12: {t5:.1f} s "
+                           f"(scene and tree build {build_s:.0f} s)")
+    else:
+        more["c5_msamples_s"] = None
+        more["c5_note"] = f"skipped: {avail / 1e9:.0f} GB of host memory available, {C5_HOST_BYTES / 1e9:.0f} GB wanted"
     return {"baseline": baseline, "more": more, "canonical": canonical}
+
+
+# host memory the reference's copy of the large scene wants, with headroom
+C5_HOST_BYTES = 80e9
+
+
+def _host_available_bytes() -> float:
+    try:
+        import psutil
+
+        return float(psutil.virtual_memory().available)
+    except Exception:
+        return 0.0
 
 
 def run_reference(args):
