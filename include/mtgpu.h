@@ -236,8 +236,11 @@ typedef struct {
     int32_t device;          /* CUDA device ordinal                             */
     int32_t traversal;       /* wavefront traversal kernels: MT_TRAVERSAL_*     */
     int32_t bvh_builder;     /* MT_BVH_BUILDER_*                                */
-    int32_t occluder_cache;  /* wavefront shadow stage: 0 = library default (on),
-                                -1 = off (every connection walks the tree)      */
+    int32_t occluder_cache;  /* wavefront shadow stage: 0 = library default (on
+                                for scenes whose materials stop every shadow ray,
+                                off for scenes with water or transparency > 0.8),
+                                1 = on for every scene, -1 = off (every
+                                connection walks the tree)                      */
 } mt_options;
 
 /* Where the scene's BVH is built. Both run the reference's binned-SAH

@@ -287,7 +287,7 @@ class GpuScene:
         def opts(o):
             return {"traversal": {0: "static", 1: "static", 2: "dynamic"}[o.traversal], "block": o.block_size,
                     "bvh_width": o.bvh_width, "sort_threshold": o.sort_threshold,
-                    "queue_capacity": o.queue_capacity or 1 << 25}
+                    "queue_capacity": o.queue_capacity or 1 << 25, "occluder_cache": o.occluder_cache}
 
         return {"chosen": opts(rep.chosen), "chosen_ms": rep.chosen_ms, "default_ms": rep.default_ms,
                 "candidates": [dict(opts(rep.entries[i].options), ms=round(rep.entries[i].ms, 3))

@@ -11,6 +11,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
+#include <cmath>
 #include <limits>
 #include <string>
 #include <vector>
@@ -128,6 +130,12 @@ struct mt_scene {
         return 0;
     }
 };
+
+// Outward growth of the FP32 node boxes, in units of 2^-24 times the
+// largest coordinate magnitude of the scene (see upload_scene).
+#ifndef MT_BOX_PAD
+#define MT_BOX_PAD 16
+#endif
 
 namespace {
 
@@ -370,6 +378,94 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
         }
     }
 
+    // FP32 slab tests (box * inv - o * inv, one fma per plane) round by up to
+    // a few units of 2^-24 of the largest coordinate magnitude M of the scene
+    // (in world units, whatever the direction), so a hit on or next to a box
+    // face could be culled. Every FP32 box is grown outward by MT_BOX_PAD
+    // units of 2^-24 * M (and rounded outward): the walks stay conservative,
+    // at the cost of a few more node visits. (FP64 keeps the tree as built.)
+    double pad = 0.0;
+    if (!nodes.empty()) {
+        double m = 0.0;
+        for (size_t i = 0; i < nodes.size() / 4; ++i) {
+            const float *q = reinterpret_cast<const float *>(&nodes[4 * i]);
+            for (int k = 0; k < 12; ++k)
+                if (std::isfinite(q[k])) m = std::max(m, (double)fabsf(q[k]));
+        }
+        pad = MT_BOX_PAD * std::ldexp(m, -24);
+    }
+    auto pad_boxes = [&](size_t first, size_t count) {
+        for (size_t i = first; i < first + count; ++i) {
+            float *q = reinterpret_cast<float *>(&nodes[4 * i]);
+            // lo / hi pairs: x (0, 1), y (2, 3) left; x (4, 5), y (6, 7) right;
+            // z (8, 9) left, (10, 11) right
+            for (int k = 0; k < 12; k += 2) {
+                float lo = (float)((double)q[k] - pad), hi = (float)((double)q[k + 1] + pad);
+                if ((double)lo > (double)q[k] - pad) lo = nextafterf(lo, -INFINITY);
+                if ((double)hi < (double)q[k + 1] + pad) hi = nextafterf(hi, INFINITY);
+                q[k] = lo;
+                q[k + 1] = hi;
+            }
+        }
+    };
+    if (sizeof(R) == 4) pad_boxes(0, nodes.size() / 4);
+    if (sizeof(R) == 4) {
+        sc->nodes2.resize(nodes.size() * 4);
+        if (!nodes.empty()) memcpy(sc->nodes2.data(), nodes.data(), sc->nodes2.size() * sizeof(float));
+    }
+
+    // Pass tree (DevScene::pass_root): the main tree pruned to the tree
+    // primitives whose material lets a shadow ray through, appended after the
+    // main tree's nodes and references.
+    int pass_depth = 0;
+    S->pass_root = kNoPassTree;
+    {
+        std::vector<char> mat_pass(d->material_count > 0 ? d->material_count : 1, 0);
+        bool any_pass = false;
+        for (int i = 0; i < d->material_count; ++i) {
+            mat_pass[i] = d->materials[i].is_water || d->materials[i].transparency > 0.8;
+            any_pass = any_pass || mat_pass[i];
+        }
+        auto passes = [&](int pi) {
+            const int m = d->prims[pi].material;
+            return m >= 0 && m < d->material_count && mat_pass[m];
+        };
+        bool plane_pass = false;
+        for (int pi : sc->bvh.planes) plane_pass = plane_pass || passes(pi);
+        if (any_pass && !plane_pass) {
+            std::vector<char> keep(n > 0 ? n : 1, 0);
+            for (int pi : sc->bvh.order) keep[pi] = passes(pi);
+            HostBvh pb;
+            FlatBvh pf;
+            prune_bvh(sc->bvh, d->prims, keep, &pb);
+            flatten_bvh(pb, &pf);
+            if (pf.node_count == 0) {
+                S->pass_root = kEmptyPassTree;
+            } else {
+                const int node_off = (int)(nodes.size() / 4), ref_off = (int)refs.size();
+                for (int pi : pf.ref_prim) refs.push_back(make_int2(pi, prim_info[pi].x));
+                const size_t base = nodes.size();
+                nodes.resize(base + pf.nodes.size() / 4);
+                memcpy(&nodes[base], pf.nodes.data(), pf.nodes.size() * sizeof(float));
+                for (int i = 0; i < pf.node_count; ++i) {
+                    int *q3 = reinterpret_cast<int *>(&nodes[base + 4 * (size_t)i + 3]);
+                    for (int side = 0; side < 2; ++side) {
+                        const int c = q3[side];
+                        if (c >= 0) {
+                            q3[side] = c + node_off;
+                        } else {
+                            const int leaf = ~c, count = leaf & 7;
+                            if (count) q3[side] = ~((((leaf >> 4) + ref_off) << 4) | count);
+                        }
+                    }
+                }
+                pad_boxes(base / 4, (size_t)pf.node_count);
+                S->pass_root = node_off;
+                pass_depth = pf.depth;
+            }
+        }
+    }
+
     int rc = 0;
     if ((rc = sc->upload(nodes, &S->nodes))) return rc;
     if ((rc = sc->upload(refs, &S->refs))) return rc;
@@ -389,13 +485,10 @@ template <typename R> int upload_scene(mt_scene *sc, const mt_scene_desc *d, Dev
     if ((rc = sc->upload(mats, &S->materials))) return rc;
 
     S->node_count = fb.node_count;
-    S->stack_depth = fb.depth + 1;  // pushes happen only on the way down
+    // pushes happen only on the way down, in either tree
+    S->stack_depth = (fb.depth > pass_depth ? fb.depth : pass_depth) + 1;
     S->bvh_width = 2;
     S->wide_stack_depth = 0;
-    if (sizeof(R) == 4) {
-        sc->nodes2.resize(nodes.size() * 4);
-        if (!nodes.empty()) memcpy(sc->nodes2.data(), nodes.data(), sc->nodes2.size() * sizeof(float));
-    }
     S->plane_count = (int)plane_prims.size();
     S->prim_count = n;
     S->material_count = d->material_count;
@@ -1079,6 +1172,7 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
     cur.sort_threshold = 1 << 18;
     cur.queue_capacity = 0;
     cur.use_graph = 1;
+    cur.occluder_cache = 0;
     float cur_ms = 0.f;
     rc = probe(cur, &cur_ms);
     rep->default_ms = cur_ms;
@@ -1091,7 +1185,10 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
         return 1;
     };
     // coordinate descent over the knobs, defaults first in each stage
-    for (int stage = 0; stage < 5 && !rc; ++stage) {
+    // (stage 5, scenes with pass-through materials: the occluder cache with
+    // the pass tree, off by default there)
+    const bool pass_scene = sc->sf.has_passthrough && sc->sf.pass_root != kNoPassTree;
+    for (int stage = 0; stage < 6 && !rc; ++stage) {
         int vals[4];
         int nv = 0;
         switch (stage) {
@@ -1099,7 +1196,10 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
         case 1: vals[nv++] = 64; break;
         case 2: vals[nv++] = 4; vals[nv++] = 8; break;
         case 3: vals[nv++] = 0; vals[nv++] = 1; break;
-        default: vals[nv++] = 8 << 20; vals[nv++] = 2 << 20; break;
+        case 4: vals[nv++] = 8 << 20; vals[nv++] = 2 << 20; break;
+        default:
+            if (pass_scene) vals[nv++] = 1;
+            break;
         }
         for (int i = 0; i < nv && !rc; ++i) {
             mt_options o = cur;
@@ -1107,7 +1207,8 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
             else if (stage == 1) o.block_size = vals[i];
             else if (stage == 2) o.bvh_width = vals[i];
             else if (stage == 3) o.sort_threshold = vals[i];
-            else o.queue_capacity = vals[i];
+            else if (stage == 4) o.queue_capacity = vals[i];
+            else o.occluder_cache = vals[i];
             // a capacity that splits the probe window into the same batches as
             // the current one cannot be told apart by the probe: skip it
             if (stage == 4 && probe_batch(o.queue_capacity) == probe_batch(cur.queue_capacity)) continue;

@@ -211,6 +211,7 @@ int mt_batch_render(mt_batch *b, int32_t n, const mt_batch_item *items, void *st
     for (int l = 0; l < b->lanes; ++l) {
         b->st[l]->grid = b->grid;
         b->st[l]->occ_cache_on = true;  // reset before each item: a lane renders several scenes
+        b->st[l]->pass_cache_on = false;
     }
     // ---- parameter blocks ----
     if (n > b->params_cap) {

@@ -359,6 +359,103 @@ void prim_bounds(const mt_prim &p, double mn[3], double mx[3])
     }
 }
 
+namespace {
+
+struct Pruner {
+    const HostBvh &b;
+    const mt_prim *prims;
+    const std::vector<char> &keep;
+    std::vector<HostNode> post;  // kept nodes, children before parents
+    std::vector<int> order;
+
+    static void pad(HostNode &n)
+    {
+        for (int k = 0; k < 3; ++k) {
+            const double m = fabs(n.mn[k]) > fabs(n.mx[k]) ? fabs(n.mn[k]) : fabs(n.mx[k]);
+            const double e = 4e-6 * (m + (n.mx[k] - n.mn[k])) + 1e-12;
+            n.mn[k] -= e;
+            n.mx[k] += e;
+        }
+    }
+
+    // index in `post` of the pruned subtree of b.nodes[i], -1 when empty
+    int run(int i)
+    {
+        const HostNode &n = b.nodes[i];
+        HostNode o;
+        for (int k = 0; k < 3; ++k) {
+            o.mn[k] = 1e300;
+            o.mx[k] = -1e300;
+        }
+        o.left = o.right = -1;
+        o.first = o.count = 0;
+        if (n.count > 0) {
+            o.first = (int)order.size();
+            for (int j = 0; j < n.count; ++j) {
+                const int pi = b.order[n.first + j];
+                if (!keep[pi]) continue;
+                order.push_back(pi);
+                double mn[3], mx[3];
+                prim_bounds(prims[pi], mn, mx);
+                for (int k = 0; k < 3; ++k) {
+                    o.mn[k] = vmin(o.mn[k], mn[k]);
+                    o.mx[k] = vmax(o.mx[k], mx[k]);
+                }
+            }
+            o.count = (int)order.size() - o.first;
+            if (!o.count) return -1;
+            pad(o);
+            post.push_back(o);
+            return (int)post.size() - 1;
+        }
+        const int l = run(n.left), r = run(n.right);
+        if (l < 0) return r;
+        if (r < 0) return l;
+        for (int k = 0; k < 3; ++k) {
+            o.mn[k] = vmin(post[l].mn[k], post[r].mn[k]);
+            o.mx[k] = vmax(post[l].mx[k], post[r].mx[k]);
+        }
+        o.left = l;
+        o.right = r;
+        post.push_back(o);
+        return (int)post.size() - 1;
+    }
+
+    // copy the kept subtree at post[p] into out->nodes in preorder
+    int emit(int p, int depth, HostBvh *out)
+    {
+        const int idx = (int)out->nodes.size();
+        out->nodes.push_back(post[p]);
+        if (post[p].count > 0) {
+            if (depth > out->depth) out->depth = depth;
+            return idx;
+        }
+        const int l = emit(post[p].left, depth + 1, out);
+        const int r = emit(post[p].right, depth + 1, out);
+        out->nodes[idx].left = l;
+        out->nodes[idx].right = r;
+        return idx;
+    }
+};
+
+}  // namespace
+
+int prune_bvh(const HostBvh &b, const mt_prim *prims, const std::vector<char> &keep, HostBvh *out)
+{
+    out->nodes.clear();
+    out->order.clear();
+    out->planes.clear();
+    out->depth = 0;
+    if (b.nodes.empty()) return 0;
+    Pruner pr{b, prims, keep, {}, {}};
+    const int root = pr.run(0);
+    if (root < 0) return 0;
+    out->order = std::move(pr.order);
+    out->nodes.reserve(pr.post.size());
+    pr.emit(root, 1, out);
+    return 0;
+}
+
 int build_bvh(const mt_prim *prims, int n, HostBvh *out)
 {
     out->nodes.clear();

@@ -36,6 +36,15 @@ int build_bvh(const mt_prim *prims, int n, HostBvh *out);
 // Returns 0 or an MT_ERR_* code (message in *err); *ms: device build time.
 int build_bvh_device(const mt_prim *prims, int n, HostBvh *out, std::string *err, float *ms);
 
+// The tree `b` restricted to the primitives with keep[prim] != 0: each leaf
+// keeps only those primitives, subtrees left empty are dropped, an inner node
+// left with one child is replaced by that child, and every box is refit to
+// the primitives left (prim_bounds, padded outward by a few parts per
+// million so that no FP32 slab test can cull a kept primitive's hit). Planes
+// are not carried over. `out->nodes` is empty when nothing is kept. Linear
+// in the size of `b` (no new SAH build).
+int prune_bvh(const HostBvh &b, const mt_prim *prims, const std::vector<char> &keep, HostBvh *out);
+
 // Device-ready flattened tree (see mt_layout.h for the node record).
 struct FlatBvh {
     std::vector<float> nodes;      // 16 floats per node (q0..q3; q3 holds ints)

@@ -663,8 +663,9 @@ MT_D void trav_init(const DevScene<R> &S, Trav<R> &tv, const RayPre<R> &rp, R tm
     tv.node = (S.node_count > 0 && !(ANY && tv.found)) ? 0 : kEmpty;
 }
 
-// Primitive tests of one leaf (code < 0, see leaf_code).
-template <typename R, bool ANY>
+// Primitive tests of one leaf (code < 0, see leaf_code). REC (nearest hit):
+// tv.any_leaf records the leaf of the current best hit.
+template <typename R, bool ANY, bool REC = false>
 MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, TravCount &c)
 {
     const RayPre<R> &rp = tv.rp;
@@ -694,6 +695,7 @@ MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, T
                     best->code = (KIND_TRIANGLE << 28) | (first + i);
                     tv.closest = t;
                     tv.found = true;
+                    if (REC) tv.any_leaf = node;
                 }
             }
         }
@@ -720,6 +722,7 @@ MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, T
                     best->code = ref.y;
                     tv.closest = t;
                     tv.found = true;
+                    if (REC) tv.any_leaf = node;
                 }
             }
         }
@@ -855,7 +858,7 @@ MT_D int descend_wide(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp
 // One while-while step: descend to a leaf, test it, pop the next node.
 // Returns false once the walk is over. `stk` is this thread's stack (entry k
 // at stk[k * stride]). W is the tree: 2 (binary `nodes`), 4 or 8 (`wnodes`).
-template <typename R, bool ANY, int W = 2>
+template <typename R, bool ANY, int W = 2, bool REC = false>
 MT_D bool trav_step(const DevScene<R> &S, Trav<R> &tv, int *stk, int stride, Hit<R> *best, TravCount &c)
 {
     int sp = tv.sp;
@@ -868,7 +871,7 @@ MT_D bool trav_step(const DevScene<R> &S, Trav<R> &tv, int *stk, int stride, Hit
         tv.node = kEmpty;
         return false;
     }
-    trav_leaf<R, ANY>(S, tv, node, best, c);
+    trav_leaf<R, ANY, REC>(S, tv, node, best, c);
     if (ANY && tv.found) {
         tv.node = kEmpty;
         return false;
@@ -1021,6 +1024,100 @@ MT_D bool scene_any_cached(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R 
             cache[0] = tv.any_leaf;
         }
     }
+    return tv.found;
+}
+
+// ------------------------------------------------------------------
+// Pass-through shadow segments with an occluder cache (scenes with water or
+// transparency > 0.8). The chain of pt_occluded_segment starts with the
+// nearest hit over every primitive; when that hit is opaque the answer is
+// "occluded". A cached opaque blocker P hit at t_P makes that certain as soon
+// as no pass-through primitive is hit in [tmin, t_P]: the nearest hit is then
+// at t <= t_P and opaque. The pass tree (DevScene::pass_root) answers that
+// question over the pass-through primitives alone.
+// ------------------------------------------------------------------
+
+// Whether primitive `pi` lets a shadow ray through (src/pathtrace.c:514-516;
+// a material index out of range stops the segment there).
+template <typename R> MT_D bool prim_passes(const DevScene<R> &S, int pi)
+{
+    const int m = __ldg(S.prim_info + pi).y;
+    if (m < 0 || m >= S.material_count) return false;
+    const DevMaterial<R> &M = S.materials[m];
+    return M.is_water || M.transparency > R(0.8);
+}
+
+// The nearest t in [tmin, tmax] among the opaque primitives of the cached
+// leaves of a four-way entry (leaf codes of the main tree, newest first, -1
+// empty); -1 when none is hit. Hits use the nearest-hit tests, so each t is
+// the one the chain's first link would see.
+template <typename R>
+MT_D R occ_opaque_nearest(const DevScene<R> &S, const int *entry, const RayPre<R> &rp, R tmin, R tmax)
+{
+    const int4 e = *reinterpret_cast<const int4 *>(entry);
+    const int c[4] = {e.x, e.y, e.z, e.w};
+    R best = R(-1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (c[k] == -1) break;
+        const int leaf = ~c[k], first = leaf >> 4, count = leaf & 7;
+        const bool tri_only = (leaf >> 3) & 1;
+        for (int i = 0; i < count; ++i) {
+            R t, u, v;
+            int pi;
+            bool hit;
+            if (tri_only) {
+                hit = tri_t(S, first + i, rp, tmin, tmax, &t, &u, &v);
+                pi = hit ? tri_prim_index(S, first + i) : 0;
+            } else {
+                const int2 ref = __ldg(S.refs + first + i);
+                hit = prim_hit_t(S, ref.y, rp, tmin, tmax, &t, &u, &v);
+                pi = ref.x;
+            }
+            if (hit && (best < R(0) || t < best) && !prim_passes(S, pi)) best = t;
+        }
+    }
+    return best;
+}
+
+// Whether some pass-through primitive is hit in [tmin, tmax] (nearest-hit
+// tests over the pass tree; the walk stops at the first hit).
+template <typename R> MT_D bool pass_hit(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax)
+{
+    if (S.pass_root < 0) return false;  // kEmptyPassTree (callers check kNoPassTree)
+    TravCount cnt;
+    Trav<R> tv;
+    Hit<R> best;
+    tv.rp = rp;
+    tv.tmin = tmin;
+    tv.closest = tmax;
+    tv.found = false;
+    tv.sp = 0;
+    tv.any_code = -1;
+    tv.any_leaf = -1;
+    tv.node = S.pass_root;
+    int *stk = mt_stack_smem + threadIdx.x;
+    while (trav_step<R, false, 2>(S, tv, stk, blockDim.x, &best, cnt))
+        if (tv.found) break;
+    trav_count_flush<R, false>(S, cnt);
+    return tv.found;
+}
+
+// scene_nearest (binary tree) that also returns the leaf of the nearest hit
+// (-1 for a plane or no hit).
+template <typename R>
+MT_D bool scene_nearest_leaf(const DevScene<R> &S, const RayPre<R> &rp, R tmin, R tmax, Hit<R> *best, int *leaf)
+{
+    TravCount cnt;
+    Trav<R> tv;
+    trav_init<R, false>(S, tv, rp, tmin, tmax, best, cnt);
+    if (tv.node != kEmpty) {
+        int *stk = mt_stack_smem + threadIdx.x;
+        while (trav_step<R, false, 2, true>(S, tv, stk, blockDim.x, best, cnt)) {
+        }
+    }
+    trav_count_flush<R, false>(S, cnt);
+    *leaf = tv.found ? tv.any_leaf : -1;
     return tv.found;
 }
 

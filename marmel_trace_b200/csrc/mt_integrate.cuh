@@ -309,6 +309,71 @@ template <typename R> struct AbsorbPath {
     R dist[2];
 };
 
+// Shadow segments of scenes whose materials can pass shadow rays, with an
+// occluder cache entry of opaque blocking leaves (four leaf codes of the main
+// tree, newest first). The chain of pt_occluded_segment starts with the
+// nearest hit over every primitive, and when that hit is opaque the answer is
+// "occluded". A cached opaque blocker hit at t_P makes that certain as soon
+// as no pass-through primitive is hit in [tmin, t_P]: the nearest hit is then
+// at t <= t_P and opaque. The pass tree (DevScene::pass_root) answers that
+// over the pass-through primitives alone; the interval is widened by 1e-5 of
+// itself, more than the FP32 rounding of the range tests, so a pass-through
+// hit at or next to t_P leaves the segment to the chain.
+template <typename R>
+MT_D bool pass_cache_occluded(const DevScene<R> &S, const int *entry, const RayPre<R> &rp, R tmin, R tmax)
+{
+    const R tp = occ_opaque_nearest(S, entry, rp, tmin, tmax);
+    return tp >= R(0) && !pass_hit(S, rp, tmin * R(1.0 - 1e-5), tp * R(1.0 + 1e-5));
+}
+
+// pt_occluded_segment (same answer and attenuation) whose first link also
+// reports the leaf of its hit: when that hit is opaque, the leaf goes to the
+// front of the cache entry `entry` (NULL: no entry).
+template <typename R>
+MT_D bool pt_occluded_segment_rec(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax, V3<R> *attenuation,
+                                  int *entry)
+{
+    if (!entry) return pt_occluded_segment(S, o, d, tmin, tmax, attenuation);
+    *attenuation = v3(R(1), R(1), R(1));
+    V3<R> cur_o = o;
+    R remaining = tmax;
+    for (int step = 0; step < 6; ++step) {
+        SurfaceHit<R> h;
+        int leaf = -1;
+        if (step == 0) {
+            // scene_intersect of the first link, with the leaf of its hit
+            const V3<R> du = unit_dir(d);
+            Hit<R> hh;
+            if (S.counters) atomicAdd(&S.counters->extension_rays, 1ull);
+            if (!scene_nearest_leaf(S, ray_pre(o, du), tmin, remaining, &hh, &leaf)) return false;
+            finish_hit(S, cur_o, du, hh, &h);
+        } else if (!scene_intersect(S, cur_o, d, tmin, remaining, &h)) {
+            return false;
+        }
+        if (h.material >= 0 && h.material < S.material_count) {
+            const DevMaterial<R> &m = S.materials[h.material];
+            if (m.is_water || m.transparency > R(0.8)) {
+                if (m.beer_lambert || m.is_water) {
+                    V3<R> seg = v3(mexp(-m.absorption[0] * h.t), mexp(-m.absorption[1] * h.t),
+                                   mexp(-m.absorption[2] * h.t));
+                    *attenuation = mul(*attenuation, seg);
+                }
+                cur_o = add(h.point, scale(d, R(1e-3)));
+                remaining -= h.t;
+                if (remaining <= R(1e-3)) return false;
+                tmin = R(1e-3);
+                continue;
+            }
+        }
+        if (leaf != -1) {
+            const int4 e = *reinterpret_cast<const int4 *>(entry);
+            if (e.x != leaf) *reinterpret_cast<int4 *>(entry) = make_int4(leaf, e.x, e.y, e.z);
+        }
+        return true;
+    }
+    return true;
+}
+
 // pt_occluded_segment with the same result and attenuation, also reporting
 // the absorbing materials passed and the distance factor of each one: the
 // attenuation is prod exp(-absorption * t) over the passed hits, so

@@ -141,6 +141,9 @@ struct DevCounters {
     unsigned long long pad;
 };
 
+static constexpr int kNoPassTree = -1;
+static constexpr int kEmptyPassTree = -2;
+
 template <typename R> struct DevScene {
     const float4 *nodes;
     const float4 *wnodes;    // wide tree (bvh_width 4 or 8; FP32 path), same leaves as `nodes`
@@ -165,6 +168,12 @@ template <typename R> struct DevScene {
     int light_count;
     int water_material;
     int has_passthrough;   // some material lets shadow rays through (water, transparency > 0.8)
+    // Pass tree: a second BVH over the tree primitives whose material lets
+    // shadow rays through, stored after the main tree in `nodes` / `refs`
+    // (mixed leaves, absolute indices). Root index; kNoPassTree when it is
+    // not built (no pass-through material, or a pass-through plane);
+    // kEmptyPassTree when no tree primitive lets shadow rays through.
+    int pass_root;
     int has_extras;        // fog, marched media, volumetric clouds or a textured material
     int pbr_only;          // every material PBR, no water / media / atmosphere glow, no extras
     int stack_depth;       // traversal stack entries per thread (dynamic shared memory)

@@ -832,8 +832,12 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? MT_SHADOW_MIN_BLOCKS : 1
         ab.dist[0] = ab.dist[1] = R(0);
         bool occ;
         if constexpr (PASS) {
+            // with `walk`, the connections whose cached blockers did not
+            // settle them (k_wf_shadow_pass_cache): the chain records the
+            // blocker it meets; the adjoint keeps the plain chain
             occ = ADJ ? pt_occluded_segment_abs(S, o, d, R(1e-3), s.tmax, &atten, &ab)
-                      : pt_occluded_segment(S, o, d, R(1e-3), s.tmax, &atten);
+                      : pt_occluded_segment_rec(S, o, d, R(1e-3), s.tmax, &atten,
+                                                walk ? occ_entry(S, occ_cache, wh, b, s) : nullptr);
         } else {
             // No material lets a shadow ray through: the chained nearest-hit
             // walk stops at its first hit, so it equals an any-hit query.
@@ -882,6 +886,41 @@ __global__ void __launch_bounds__(kWfMaxBlock, 8) k_wf_shadow_cache(const __grid
                 if (S.trace_rec)
                     trace_put(S, v3(s.o[0], s.o[1], s.o[2]), unit_dir(v3(s.d[0], s.d[1], s.d[2])), s.tmax, 1, 1, b,
                               s.li);
+            } else {
+                miss = true;
+            }
+        }
+        const int at = warp_append(&C->walk_count, miss);
+        if (miss) walk[at] = q;
+    }
+}
+
+// First pass of the shadow stage of a scene with pass-through materials
+// (pass tree built, occluder cache on): connections that a cached opaque
+// blocker settles (pass_cache_occluded) are answered here; the rest go to
+// `walk` for the chain (k_wf_shadow, PASS).
+template <typename R>
+__global__ void __launch_bounds__(kWfMaxBlock, MT_SHADOW_MIN_BLOCKS) k_wf_shadow_pass_cache(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq,
+                                                                          WfCounters *C, R *nee, int *occ_cache,
+                                                                          int wh, int b, int *walk)
+{
+    const int n = C->shadow_count;
+    const int stride = gridDim.x * blockDim.x;
+    const int n_round = (n + stride - 1) / stride * stride;
+    AbsorbPath<R> ab;
+    ab.mat[0] = ab.mat[1] = -1;
+    ab.dist[0] = ab.dist[1] = R(0);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
+        bool miss = false;
+        if (q < n) {
+            const WfShadow<R> s = sq[q];
+            if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
+            const V3<R> o = v3(s.o[0], s.o[1], s.o[2]);
+            const V3<R> du = unit_dir(v3(s.d[0], s.d[1], s.d[2]));
+            if (pass_cache_occluded(S, occ_entry(S, occ_cache, wh, b, s), ray_pre(o, du), R(1e-3), s.tmax)) {
+                if (S.counters) atomicAdd(&S.counters->any_prim_tests, 1ull);
+                shadow_result<R, false>(s, true, v3(R(1), R(1), R(1)), ab, nee, nullptr);
+                if (S.trace_rec) trace_put(S, o, du, s.tmax, 1, 1, b, s.li);
             } else {
                 miss = true;
             }

@@ -46,6 +46,9 @@ struct WavefrontState {
     // (a batch lane renders several, so it turns this off)
     void *occ_cache = nullptr;
     bool occ_cache_on = true;
+    // scenes with pass-through materials use the cache (cache pass with the
+    // pass tree) only when asked for (mt_options.occluder_cache = 1)
+    bool pass_cache_on = false;
     // the NEE slots hold zeros between windows: they are zeroed at
     // allocation, and every slot a shadow connection writes is gathered (and
     // zeroed) by the next shade or by finalize; a state whose buffers are
@@ -189,7 +192,14 @@ void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
                    const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk)
 {
     if (S.has_passthrough) {
-        k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
+        if (!ADJ && occ && walk && S.pass_root != kNoPassTree) {
+            // cached opaque blockers first (with the pass tree), then the
+            // chain for the rest
+            k_wf_shadow_pass_cache<R><<<g, block, smem, s>>>(S, sq, C, nee, occ, wh, b, walk);
+            k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
+        } else {
+            k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
+        }
     } else if (dyn) {
         k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
     } else if (occ && walk) {
@@ -292,7 +302,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         st->kernel_launches[kind] += 1;
         ev += 2;
     };
-    int *occ = st->occ_cache_on ? (int *)st->occ_cache : nullptr;
+    int *occ = st->occ_cache_on && (!S.has_passthrough || st->pass_cache_on) ? (int *)st->occ_cache : nullptr;
     const WfAdj<R> none{nullptr, nullptr, nullptr, P};
     const WfAdj<R> A{(AdjVertex<R> *)st->adj_verts, (R *)st->adj_att, sample_buf, P};
     // generate -> (extend, shade, shadow) x (depth + 1); the replay pass uses
@@ -438,11 +448,16 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     WF_CK(cudaMemcpyAsync(st->params, st->h_params, sizeof hp, cudaMemcpyHostToDevice, stream), "params copy");
     // the occluder cache can be switched off per scene (mt_options.occluder_cache)
     st->occ_cache_on = !(opts && opts->occluder_cache < 0);
+    st->pass_cache_on = opts && opts->occluder_cache > 0;
     // the bounce-0 shadow stage is two kernels when it uses the occluder cache
-    const int cache_pass = st->occ_cache_on && st->occ_cache && st->walk && !S.has_passthrough &&
-                           !(opts && opts->traversal == MT_TRAVERSAL_DYNAMIC);
-    int kernels_per_window = adjoint ? n_batches * 2 * ((3 + cache_pass) * (depth + 1) + 2)
-                                     : n_batches * ((3 + cache_pass + (sort_threshold ? 3 : 0)) * (depth + 1) + 3);
+    // (scenes with pass-through materials: with the pass tree, outside the
+    // adjoint's replay pass)
+    const bool cache_on = st->occ_cache_on && st->occ_cache && st->walk;
+    const int cache_pass = cache_on && !S.has_passthrough && !(opts && opts->traversal == MT_TRAVERSAL_DYNAMIC);
+    const int pass_cache = cache_on && S.has_passthrough && st->pass_cache_on && S.pass_root != kNoPassTree;
+    const int cp = cache_pass + pass_cache;
+    int kernels_per_window = adjoint ? n_batches * (((3 + cp) + (3 + cache_pass)) * (depth + 1) + 4)
+                                     : n_batches * ((3 + cp + (sort_threshold ? 3 : 0)) * (depth + 1) + 3);
     cudaGraphExec_t &exec = adjoint ? st->adj_exec : st->exec;
     // dynamic fetch reorders rays across lanes: on coherent queues (primary
     // rays, NEE rays grouped by light) the grid-stride kernels are faster, so
@@ -455,7 +470,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         // its identity, counters and parameter version are part of the key
         snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d:%d:%d:%d:%p:%d", (int)sizeof(R), w, h, batch_spp,
                  n_batches, depth, (const void *)S.nodes, (const void *)S.counters, S.version, (int)dyn, block,
-                 sort_threshold, S.bvh_width, (const void *)S.trace_rec, (int)st->occ_cache_on);
+                 sort_threshold, S.bvh_width, (const void *)S.trace_rec,
+                 (int)st->occ_cache_on + 2 * (int)st->pass_cache_on);
         if (!exec || exec_key != key) {
             if (exec) cudaGraphExecDestroy(exec);
             exec = nullptr;
