@@ -409,12 +409,14 @@ typedef struct {
 
 /*
  * Pick the wavefront integrator's configuration for this scene and view by
- * timing a probe window of `probe_spp` samples per pixel (same samples for
- * every candidate) on the scene's device. Coordinate descent, each stage
- * keeping the fastest so far (library defaults first):
+ * timing probe windows of `probe_spp` samples per pixel on the scene's device
+ * (each render takes the next sample window, so that no candidate retraces
+ * samples whose blockers the occluder cache already holds). Coordinate
+ * descent, each stage keeping the fastest so far (library defaults first):
  *   traversal schedule (grid-stride, dynamic fetch), block size (128, 64),
  *   BVH width (2, 4, 8; wide trees built on first use), sort-by-material
- *   threshold (256K rays, off, always), queue capacity (32M, 8M, 2M).
+ *   threshold (256K rays, off, always), queue capacity (32M, 8M, 2M), and for
+ *   scenes with water or transparency > 0.8 the occluder cache (off, on).
  * Every candidate computes the same image (the tests check this), so the
  * choice only moves time. The scene must be FP32; on return its options are
  * the chosen ones with the wavefront integrator. Allocates probe buffers;

@@ -1133,7 +1133,11 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
     const bool counting = sc->counting;
     sc->counting = false;
     const mt_options saved = sc->opts;
-    const int s0 = 1 << 20;  // one fixed probe window for every candidate
+    // Every probe render takes the next sample window, so no candidate sees
+    // samples an earlier render already traced (the occluder cache would
+    // otherwise hold the very blockers of its rays).
+    int window = 0;
+    const int s_base = 1 << 20;
     // time one configuration: a warm-up window (captures its graph), then the
     // better of two timed windows
     auto probe = [&](const mt_options &o, float *ms) -> int {
@@ -1143,6 +1147,7 @@ int mt_autotune(mt_scene *sc, const mt_camera *cam, int w, int h, int probe_spp,
         float best = 3.0e38f;
         for (int k = 0; k < 3; ++k) {
             if (k) CK(cudaEventRecord(e0, 0), "cudaEventRecord");
+            const int s0 = s_base + probe_spp * window++;
             r = render_dev<float>(sc, cam, w, h, s0 + probe_spp, s0, s0 + probe_spp, depth, RENDER_PT, OUT_SUM_F32,
                                   out.p, 0, false);
             if (r) return r;

@@ -1371,6 +1371,30 @@ MT_D bool scene_intersect(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax
     return true;
 }
 
+// What a link of a pass-through shadow chain reads of scene_intersect's hit
+// record: t, the hit point and the material, with finish_hit's values for
+// them (the normal and texture terms are not computed). `leaf` (optional):
+// the leaf of the hit, as scene_nearest_leaf.
+template <typename R> struct LinkHit {
+    R t;
+    V3<R> point;
+    int material;
+};
+template <typename R>
+MT_D bool scene_link(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax, LinkHit<R> *out, int *leaf = nullptr)
+{
+    d = unit_dir(d);
+    const RayPre<R> rp = ray_pre(o, d);
+    Hit<R> h;
+    if (S.counters) atomicAdd(&S.counters->extension_rays, 1ull);
+    const bool found = leaf ? scene_nearest_leaf(S, rp, tmin, tmax, &h, leaf) : scene_nearest(S, rp, tmin, tmax, &h);
+    if (!found) return false;
+    out->t = h.t;
+    out->point = at(o, d, h.t);
+    out->material = __ldg(S.prim_info + h.prim).y;
+    return true;
+}
+
 // scene_occluded (src/scene.c:804-811).
 template <typename R> MT_D bool scene_occluded(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax)
 {

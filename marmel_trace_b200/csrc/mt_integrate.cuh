@@ -151,8 +151,8 @@ MT_D bool pt_occluded_segment(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R 
         return scene_any(S, ray_pre(o, unit_dir(d)), tmin, tmax);
     }
     for (int step = 0; step < 6; ++step) {
-        SurfaceHit<R> h;
-        if (!scene_intersect(S, cur_o, d, tmin, remaining, &h)) return false;
+        LinkHit<R> h;
+        if (!scene_link(S, cur_o, d, tmin, remaining, &h)) return false;
         if (h.material < 0 || h.material >= S.material_count) return true;
         const DevMaterial<R> &m = S.materials[h.material];
         if (m.is_water || m.transparency > R(0.8)) {
@@ -338,18 +338,10 @@ MT_D bool pt_occluded_segment_rec(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin
     V3<R> cur_o = o;
     R remaining = tmax;
     for (int step = 0; step < 6; ++step) {
-        SurfaceHit<R> h;
+        LinkHit<R> h;
         int leaf = -1;
-        if (step == 0) {
-            // scene_intersect of the first link, with the leaf of its hit
-            const V3<R> du = unit_dir(d);
-            Hit<R> hh;
-            if (S.counters) atomicAdd(&S.counters->extension_rays, 1ull);
-            if (!scene_nearest_leaf(S, ray_pre(o, du), tmin, remaining, &hh, &leaf)) return false;
-            finish_hit(S, cur_o, du, hh, &h);
-        } else if (!scene_intersect(S, cur_o, d, tmin, remaining, &h)) {
-            return false;
-        }
+        // the first link also reports the leaf of its hit
+        if (!scene_link(S, cur_o, d, tmin, remaining, &h, step == 0 ? &leaf : nullptr)) return false;
         if (h.material >= 0 && h.material < S.material_count) {
             const DevMaterial<R> &m = S.materials[h.material];
             if (m.is_water || m.transparency > R(0.8)) {
@@ -391,8 +383,8 @@ MT_D bool pt_occluded_segment_abs(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin
     if (S.counters) atomicAdd(&S.counters->shadow_rays, 1ull);
     if (!S.has_passthrough) return scene_any(S, ray_pre(o, unit_dir(d)), tmin, tmax);
     for (int step = 0; step < 6; ++step) {
-        SurfaceHit<R> h;
-        if (!scene_intersect(S, cur_o, d, tmin, remaining, &h)) return false;
+        LinkHit<R> h;
+        if (!scene_link(S, cur_o, d, tmin, remaining, &h)) return false;
         if (h.material < 0 || h.material >= S.material_count) return true;
         const DevMaterial<R> &m = S.materials[h.material];
         if (m.is_water || m.transparency > R(0.8)) {

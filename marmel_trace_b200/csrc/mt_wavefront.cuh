@@ -113,6 +113,10 @@ static constexpr int kWfMaxBlock = 128;
 #ifndef MT_SHADOW_MIN_BLOCKS
 #define MT_SHADOW_MIN_BLOCKS 7
 #endif
+// the chained pass-through walk (scenes with water or glass)
+#ifndef MT_PASS_MIN_BLOCKS
+#define MT_PASS_MIN_BLOCKS 7
+#endif
 
 struct WfCounters {
     int ray_count[2];
@@ -818,7 +822,7 @@ MT_D void shadow_result(const WfShadow<R> &s, bool occ, V3<R> atten, const Absor
 template <typename R, bool ADJ, int W, bool PASS>
 // (binary tree: at most 72 registers, so 7 blocks of 128 fit an SM; the
 // pass-through instantiation would otherwise take 80 and run 6)
-__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? MT_SHADOW_MIN_BLOCKS : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOCKS : MT_SHADOW_MIN_BLOCKS) : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
                                                    R *nee, R *att, int *occ_cache, int wh, int b, const int *walk)
 {
     const int n = walk ? C->walk_count : C->shadow_count;
