@@ -199,6 +199,9 @@ int mt_batch_render(mt_batch *b, int32_t n, const mt_batch_item *items, void *st
             buckets = std::max(buckets, sort_buckets(mt_scene_dev_f32(items[i].scene)->material_count + 1));
         if (!rc) rc = wf_reserve_sort<float>(b->st[l], buckets);
         if (rc) return bfail(rc, std::string("mt_batch_render: ") + wavefront_last_error());
+        bool pass = false;
+        for (int i : lane_items[l]) pass = pass || mt_scene_dev_f32(items[i].scene)->has_passthrough;
+        if (pass) wf_reserve_links<float>(b->st[l]);
     }
     if (!b->grid) {
         int sms = 0, per_sm = 0;
@@ -230,7 +233,8 @@ int mt_batch_render(mt_batch *b, int32_t n, const mt_batch_item *items, void *st
     }
     // ---- graph: captured once per item-list shape ----
     std::string key = std::to_string(n) + ":" + std::to_string((uintptr_t)b->params);
-    for (int l = 0; l < b->lanes; ++l) key += ":" + std::to_string((uintptr_t)b->st[l]->paths);
+    for (int l = 0; l < b->lanes; ++l)
+        key += ":" + std::to_string((uintptr_t)b->st[l]->paths) + "/" + std::to_string((uintptr_t)b->st[l]->link[0]);
     for (int i = 0; i < n; ++i) {
         const DevScene<float> &S = *mt_scene_dev_f32(items[i].scene);
         char buf[160];

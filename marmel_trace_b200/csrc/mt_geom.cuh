@@ -1386,8 +1386,11 @@ MT_D bool scene_link(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax, Lin
     d = unit_dir(d);
     const RayPre<R> rp = ray_pre(o, d);
     Hit<R> h;
+    int lf;
     if (S.counters) atomicAdd(&S.counters->extension_rays, 1ull);
-    const bool found = leaf ? scene_nearest_leaf(S, rp, tmin, tmax, &h, leaf) : scene_nearest(S, rp, tmin, tmax, &h);
+    // one walk for every link (the leaf is recorded either way)
+    const bool found = scene_nearest_leaf(S, rp, tmin, tmax, &h, &lf);
+    if (leaf) *leaf = lf;
     if (!found) return false;
     out->t = h.t;
     out->point = at(o, d, h.t);

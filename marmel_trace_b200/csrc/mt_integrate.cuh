@@ -326,46 +326,6 @@ MT_D bool pass_cache_occluded(const DevScene<R> &S, const int *entry, const RayP
     return tp >= R(0) && !pass_hit(S, rp, tmin * R(1.0 - 1e-5), tp * R(1.0 + 1e-5));
 }
 
-// pt_occluded_segment (same answer and attenuation) whose first link also
-// reports the leaf of its hit: when that hit is opaque, the leaf goes to the
-// front of the cache entry `entry` (NULL: no entry).
-template <typename R>
-MT_D bool pt_occluded_segment_rec(const DevScene<R> &S, V3<R> o, V3<R> d, R tmin, R tmax, V3<R> *attenuation,
-                                  int *entry)
-{
-    if (!entry) return pt_occluded_segment(S, o, d, tmin, tmax, attenuation);
-    *attenuation = v3(R(1), R(1), R(1));
-    V3<R> cur_o = o;
-    R remaining = tmax;
-    for (int step = 0; step < 6; ++step) {
-        LinkHit<R> h;
-        int leaf = -1;
-        // the first link also reports the leaf of its hit
-        if (!scene_link(S, cur_o, d, tmin, remaining, &h, step == 0 ? &leaf : nullptr)) return false;
-        if (h.material >= 0 && h.material < S.material_count) {
-            const DevMaterial<R> &m = S.materials[h.material];
-            if (m.is_water || m.transparency > R(0.8)) {
-                if (m.beer_lambert || m.is_water) {
-                    V3<R> seg = v3(mexp(-m.absorption[0] * h.t), mexp(-m.absorption[1] * h.t),
-                                   mexp(-m.absorption[2] * h.t));
-                    *attenuation = mul(*attenuation, seg);
-                }
-                cur_o = add(h.point, scale(d, R(1e-3)));
-                remaining -= h.t;
-                if (remaining <= R(1e-3)) return false;
-                tmin = R(1e-3);
-                continue;
-            }
-        }
-        if (leaf != -1) {
-            const int4 e = *reinterpret_cast<const int4 *>(entry);
-            if (e.x != leaf) *reinterpret_cast<int4 *>(entry) = make_int4(leaf, e.x, e.y, e.z);
-        }
-        return true;
-    }
-    return true;
-}
-
 // pt_occluded_segment with the same result and attenuation, also reporting
 // the absorbing materials passed and the distance factor of each one: the
 // attenuation is prod exp(-absorption * t) over the passed hits, so

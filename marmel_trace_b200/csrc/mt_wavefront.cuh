@@ -126,7 +126,11 @@ struct WfCounters {
     int sorted;        // this bounce's extend results were sorted by material
     int walk_count;    // shadow rays whose cached occluder missed (k_wf_shadow_cache)
     int pad;
+    int link_count[6]; // pass-through chains continuing after link k (k_wf_shadow_link)
+    int pad2[2];
 };
+// Ints from shadow_count that are zeroed before every shade stage.
+static constexpr int kWfBounceCounters = 12;
 
 // Warp-aggregated queue append: one atomicAdd per warp, lanes get
 // consecutive slots in lane order.
@@ -817,17 +821,77 @@ MT_D void shadow_result(const WfShadow<R> &s, bool occ, V3<R> atten, const Absor
     }
 }
 
+// State of a pass-through chain between two of its links (the loop of
+// pt_occluded_segment, src/pathtrace.c:504-532): the next link's origin,
+// the length left, the attenuation so far and the connection sq[q].
+template <typename R> struct __align__(16) WfLink {
+    R o[3];
+    R remaining;
+    R att[3];
+    int q;
+};
+
+// One link (step `step`, 0..5) of pt_occluded_segment's chain. Returns 0 (not
+// occluded), 1 (occluded) or 2 (passed a transparent hit: cur_o, tmin,
+// remaining and atten hold the next link). `leaf`: see scene_link.
+template <typename R>
+MT_D int chain_link(const DevScene<R> &S, V3<R> &cur_o, V3<R> d, R &tmin, R &remaining, V3<R> &atten, int step,
+                    int *leaf = nullptr)
+{
+    LinkHit<R> h;
+    if (!scene_link(S, cur_o, d, tmin, remaining, &h, leaf)) return 0;
+    if (h.material < 0 || h.material >= S.material_count) return 1;
+    const DevMaterial<R> &m = S.materials[h.material];
+    if (!(m.is_water || m.transparency > R(0.8))) return 1;
+    if (m.beer_lambert || m.is_water) {
+        V3<R> seg = v3(mexp(-m.absorption[0] * h.t), mexp(-m.absorption[1] * h.t), mexp(-m.absorption[2] * h.t));
+        atten = mul(atten, seg);
+    }
+    cur_o = add(h.point, scale(d, R(1e-3)));
+    remaining -= h.t;
+    if (remaining <= R(1e-3)) return 0;
+    tmin = R(1e-3);
+    return step < 5 ? 2 : 1;  // six links at most, then occluded
+}
+
+// Append chain state to the link queue `out` (capacity cap); false when it
+// is full (the caller then finishes the chain itself).
+template <typename R>
+MT_D bool push_link(WfLink<R> *out, int *count, int cap, V3<R> o, R remaining, V3<R> atten, int q)
+{
+    const int at = warp_append(count, true);
+    if (at >= cap) return false;
+    WfLink<R> L;
+    L.o[0] = o.x;
+    L.o[1] = o.y;
+    L.o[2] = o.z;
+    L.remaining = remaining;
+    L.att[0] = atten.x;
+    L.att[1] = atten.y;
+    L.att[2] = atten.z;
+    L.q = q;
+    out[at] = L;
+    return true;
+}
+
 // `walk` (may be NULL): the connections to process are sq[walk[0 .. C->walk_count)]
 // and their cached occluder has already missed; otherwise sq[0 .. C->shadow_count).
 template <typename R, bool ADJ, int W, bool PASS>
 // (binary tree: at most 72 registers, so 7 blocks of 128 fit an SM; the
 // pass-through instantiation would otherwise take 80 and run 6)
-__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOCKS : MT_SHADOW_MIN_BLOCKS) : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, const WfCounters *C,
-                                                   R *nee, R *att, int *occ_cache, int wh, int b, const int *walk)
+//
+// PASS with `link` (not the adjoint): only the chain's first link runs here;
+// chains that pass a transparent hit go to the link queue (link_count[0]) and
+// k_wf_shadow_link runs their next links, one launch per link, so that the
+// lanes of a warp do not wait for the longest chain among them.
+__global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOCKS : MT_SHADOW_MIN_BLOCKS) : 1) k_wf_shadow(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq, WfCounters *C,
+                                                   R *nee, R *att, int *occ_cache, int wh, int b, const int *walk,
+                                                   WfLink<R> *link, int link_cap)
 {
     const int n = walk ? C->walk_count : C->shadow_count;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const WfShadow<R> s = sq[walk ? walk[q] : q];
+        const int qs = walk ? walk[q] : q;
+        const WfShadow<R> s = sq[qs];
         V3<R> o = v3(s.o[0], s.o[1], s.o[2]);
         V3<R> d = v3(s.d[0], s.d[1], s.d[2]);
         V3<R> atten;
@@ -839,9 +903,27 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOC
             // with `walk`, the connections whose cached blockers did not
             // settle them (k_wf_shadow_pass_cache): the chain records the
             // blocker it meets; the adjoint keeps the plain chain
-            occ = ADJ ? pt_occluded_segment_abs(S, o, d, R(1e-3), s.tmax, &atten, &ab)
-                      : pt_occluded_segment_rec(S, o, d, R(1e-3), s.tmax, &atten,
-                                                walk ? occ_entry(S, occ_cache, wh, b, s) : nullptr);
+            if constexpr (ADJ) {
+                occ = pt_occluded_segment_abs(S, o, d, R(1e-3), s.tmax, &atten, &ab);
+            } else {
+                // pt_occluded_segment's chain, link by link; the first link's
+                // opaque blocker goes to the front of the entry
+                int *entry = walk ? occ_entry(S, occ_cache, wh, b, s) : nullptr;
+                if (S.counters && !walk) atomicAdd(&S.counters->shadow_rays, 1ull);
+                atten = v3(R(1), R(1), R(1));
+                V3<R> cur_o = o;
+                R tmin = R(1e-3), remaining = s.tmax;
+                int leaf = -1;
+                int r = chain_link(S, cur_o, d, tmin, remaining, atten, 0, &leaf);
+                if (r == 1 && entry && leaf != -1) {
+                    const int4 e = *reinterpret_cast<const int4 *>(entry);
+                    if (e.x != leaf) *reinterpret_cast<int4 *>(entry) = make_int4(leaf, e.x, e.y, e.z);
+                }
+                if (r == 2 && link && push_link(link, &C->link_count[0], link_cap, cur_o, remaining, atten, qs))
+                    continue;
+                for (int step = 1; r == 2; ++step) r = chain_link(S, cur_o, d, tmin, remaining, atten, step);
+                occ = r == 1;
+            }
         } else {
             // No material lets a shadow ray through: the chained nearest-hit
             // walk stops at its first hit, so it equals an any-hit query.
@@ -856,6 +938,41 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOC
         // the sun through volumetric clouds (pt_nee_sun, src/pathtrace.c:545-546)
         if (!occ && s.li == kMaxLights) atten = scale(atten, cloud_transmittance(S.sky, o, d));
         shadow_result<R, ADJ>(s, occ, atten, ab, nee, att);
+        if (S.trace_rec) trace_put(S, o, unit_dir(d), s.tmax, occ ? 1 : 0, 1, b, s.li);
+    }
+}
+
+// Link `step` (1..5) of the pass-through chains queued by the previous link
+// (in[0 .. min(link_count[step - 1], cap))); chains that pass another
+// transparent hit go to `out` (link_count[step]), the others write their
+// connection's result.
+template <typename R>
+__global__ void __launch_bounds__(kWfMaxBlock, MT_PASS_MIN_BLOCKS) k_wf_shadow_link(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq,
+                                                                   WfCounters *C, R *nee, int b, int step,
+                                                                   const WfLink<R> *in, WfLink<R> *out, int cap)
+{
+    const int c = C->link_count[step - 1];
+    const int n = c < cap ? c : cap;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const WfLink<R> L = in[i];
+        const WfShadow<R> s = sq[L.q];
+        const V3<R> d = v3(s.d[0], s.d[1], s.d[2]);
+        V3<R> cur_o = v3(L.o[0], L.o[1], L.o[2]);
+        V3<R> atten = v3(L.att[0], L.att[1], L.att[2]);
+        R tmin = R(1e-3), remaining = L.remaining;
+        int r = chain_link(S, cur_o, d, tmin, remaining, atten, step);
+        if (r == 2) {
+            if (push_link(out, &C->link_count[step], cap, cur_o, remaining, atten, L.q)) continue;
+            for (int k = step + 1; r == 2; ++k) r = chain_link(S, cur_o, d, tmin, remaining, atten, k);
+        }
+        const bool occ = r == 1;
+        const V3<R> o = v3(s.o[0], s.o[1], s.o[2]);
+        // the sun through volumetric clouds (pt_nee_sun, src/pathtrace.c:545-546)
+        if (!occ && s.li == kMaxLights) atten = scale(atten, cloud_transmittance(S.sky, o, d));
+        AbsorbPath<R> ab;
+        ab.mat[0] = ab.mat[1] = -1;
+        ab.dist[0] = ab.dist[1] = R(0);
+        shadow_result<R, false>(s, occ, atten, ab, nee, nullptr);
         if (S.trace_rec) trace_put(S, o, unit_dir(d), s.tmax, occ ? 1 : 0, 1, b, s.li);
     }
 }

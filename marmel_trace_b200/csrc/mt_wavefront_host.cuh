@@ -10,6 +10,8 @@
 // when the frame's shape changes (size, batch split, depth).
 #pragma once
 
+#include <limits.h>
+
 #include <string.h>
 
 #include <string>
@@ -56,6 +58,10 @@ struct WavefrontState {
     // k_wf_generate zero them
     bool nee_clean = false;
     void *walk = nullptr;      // shadow rays left to walk after the occluder-cache pass
+    // link queues of pass-through chains (wf_reserve_links), `link_cap`
+    // records of WfLink<R> each; NULL: chains run whole in k_wf_shadow
+    void *link[2] = {nullptr, nullptr};
+    int link_cap = 0;
     int grid = 0;              // persistent grid (blocks) of the stage kernels
     cudaEvent_t kev[64];       // per-kernel timing events (profiling mode)
     bool kev_init = false;
@@ -88,7 +94,7 @@ inline void wf_free(WavefrontState *st)
     void **bufs[] = {&st->paths,       &st->rays[0],    &st->rays[1],     &st->hits,        &st->nee,
                      &st->shadow,      &st->sample_buf, &st->acc,         &st->params,      &st->adj_verts,
                      &st->adj_att,     &st->sorted_rays, &st->sorted_hits, &st->sort_keys, &st->sort_buckets,
-                     &st->occ_cache,   &st->walk};
+                     &st->occ_cache,   &st->walk,       &st->link[0],     &st->link[1]};
     for (void **b : bufs) {
         if (*b) cudaFree(*b);
         *b = nullptr;
@@ -104,6 +110,7 @@ inline void wf_free(WavefrontState *st)
     st->cap_paths = 0;
     st->acc_pixels = 0;
     st->sort_bucket_cap = 0;
+    st->link_cap = 0;
     st->nee_clean = false;
 }
 
@@ -161,6 +168,32 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
     return 0;
 }
 
+// Link queues of the pass-through chains (scenes with water or transparency
+// > 0.8): two buffers, each for half the shadow connections of the reserved
+// path slots; a chain that finds its queue full runs its remaining links in
+// place. Optional: when the allocation fails the chains run whole in
+// k_wf_shadow (same results).
+template <typename R> void wf_reserve_links(WavefrontState *st)
+{
+    if (st->link[0] && st->link[1]) return;
+    const size_t nshadow = st->cap_paths * (size_t)(st->light_count + 1);
+    size_t cap = nshadow / 2;
+    if (cap < 1) cap = 1;
+    if (cap > (size_t)INT_MAX) cap = (size_t)INT_MAX;
+    for (int k = 0; k < 2; ++k)
+        if (!st->link[k] && cudaMalloc(&st->link[k], cap * sizeof(WfLink<R>)) != cudaSuccess) st->link[k] = nullptr;
+    if (!st->link[0] || !st->link[1]) {
+        for (int k = 0; k < 2; ++k) {
+            if (st->link[k]) cudaFree(st->link[k]);
+            st->link[k] = nullptr;
+        }
+        cudaGetLastError();
+        st->link_cap = 0;
+        return;
+    }
+    st->link_cap = (int)cap;
+}
+
 // The adjoint replay's per-path buffers, sized to the reserved path slots.
 template <typename R> int wf_reserve_adj(WavefrontState *st)
 {
@@ -187,39 +220,62 @@ void launch_extend(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
         k_wf_extend<R, W><<<g, block, smem, s>>>(S, rays, C, which, hits);
 }
 
+// Link queues of the pass-through chains (k_wf_shadow_link): two buffers of
+// `cap` records, NULL when the state has none (the chain then runs whole in
+// k_wf_shadow).
+struct WfLinkQueues {
+    void *q[2];
+    int cap;
+};
+
+// Kernels of one shadow stage in a scene with pass-through materials and
+// link queues: the first link, then one launch per further link (five).
+static constexpr int kWfLinkLaunches = 5;
+
 template <typename R, bool ADJ, int W>
 void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
-                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk)
+                   const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk,
+                   const WfLinkQueues &lq)
 {
     if (S.has_passthrough) {
+        WfLink<R> *l0 = ADJ || !lq.cap ? nullptr : (WfLink<R> *)lq.q[0];
         if (!ADJ && occ && walk && S.pass_root != kNoPassTree) {
             // cached opaque blockers first (with the pass tree), then the
             // chain for the rest
             k_wf_shadow_pass_cache<R><<<g, block, smem, s>>>(S, sq, C, nee, occ, wh, b, walk);
-            k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
+            k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk, l0, lq.cap);
         } else {
-            k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
+            k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr, l0,
+                                                                lq.cap);
         }
+        if (l0)
+            for (int step = 1; step <= kWfLinkLaunches; ++step)
+                k_wf_shadow_link<R><<<g, block, smem, s>>>(S, sq, C, nee, b, step,
+                                                           (const WfLink<R> *)lq.q[(step - 1) & 1],
+                                                           (WfLink<R> *)lq.q[step & 1], lq.cap);
     } else if (dyn) {
         k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
     } else if (occ && walk) {
         // cached occluders first, then the tree walk for the misses
         k_wf_shadow_cache<R, ADJ><<<g, block, 0, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
-        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk);
+        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk, nullptr, 0);
     } else {
-        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr);
+        k_wf_shadow<R, ADJ, W, false><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr, nullptr, 0);
     }
 }
 
 template <typename R, bool ADJ>
 void launch_shadow_w(int W, bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
-                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk)
+                     const WfShadow<R> *sq, WfCounters *C, R *nee, R *att, int *occ, int wh, int b, int *walk,
+                     const WfLinkQueues &lq)
 {
     if constexpr (sizeof(R) == 4) {
-        if (W == 4) return launch_shadow<R, ADJ, 4>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
-        if (W == 8) return launch_shadow<R, ADJ, 8>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
+        if (W == 4)
+            return launch_shadow<R, ADJ, 4>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk, lq);
+        if (W == 8)
+            return launch_shadow<R, ADJ, 8>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk, lq);
     }
-    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk);
+    launch_shadow<R, ADJ, 2>(dyn, g, block, smem, s, S, sq, C, nee, att, occ, wh, b, walk, lq);
 }
 
 template <typename R>
@@ -303,6 +359,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         ev += 2;
     };
     int *occ = st->occ_cache_on && (!S.has_passthrough || st->pass_cache_on) ? (int *)st->occ_cache : nullptr;
+    const WfLinkQueues lq{{st->link[0], st->link[1]}, st->link[0] && st->link[1] ? st->link_cap : 0};
     const WfAdj<R> none{nullptr, nullptr, nullptr, P};
     const WfAdj<R> A{(AdjVertex<R> *)st->adj_verts, (R *)st->adj_att, sample_buf, P};
     // generate -> (extend, shade, shadow) x (depth + 1); the replay pass uses
@@ -321,7 +378,7 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             WF_CK(cudaMemsetAsync(&C->ray_count[which ^ 1], 0, sizeof(int), s), "memset(ray_count)");
             // shadow_count, shadow_fetch, ray_fetch (the next extend's), sorted
             // and walk_count
-            WF_CK(cudaMemsetAsync(&C->shadow_count, 0, 5 * sizeof(int), s), "memset(shadow_count)");
+            WF_CK(cudaMemsetAsync(&C->shadow_count, 0, kWfBounceCounters * sizeof(int), s), "memset(shadow_count)");
             const bool sort = sort_threshold > 0 && !replay && st->sorted_rays;
             if (sort) {
                 const int nb = sort_buckets(S.material_count + 1);
@@ -360,10 +417,10 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             tic();
             if (replay)
                 launch_shadow_w<R, true>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, A.att, occ, wh, b,
-                                         (int *)st->walk);
+                                         (int *)st->walk, lq);
             else
                 launch_shadow_w<R, false>(Ws, dyn, g, block, smem_s, s, S, sq, C, nee, nullptr, occ, wh, b,
-                                          (int *)st->walk);
+                                          (int *)st->walk, lq);
             toc(2);
             which ^= 1;
         }
@@ -405,6 +462,7 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     if (rc) return rc;
     const bool adjoint = adj != nullptr;
     if (adjoint && (rc = wf_reserve_adj<R>(st))) return rc;
+    if (S.has_passthrough) wf_reserve_links<R>(st);
     const int block = (opts && opts->block_size == 64) ? 64 : 128;
     const int sort_threshold = (!adjoint && opts && opts->sort_threshold > 0) ? opts->sort_threshold : 0;
     if (sort_threshold && (rc = wf_reserve_sort<R>(st, sort_buckets(S.material_count + 1)))) return rc;
@@ -455,7 +513,8 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
     const bool cache_on = st->occ_cache_on && st->occ_cache && st->walk;
     const int cache_pass = cache_on && !S.has_passthrough && !(opts && opts->traversal == MT_TRAVERSAL_DYNAMIC);
     const int pass_cache = cache_on && S.has_passthrough && st->pass_cache_on && S.pass_root != kNoPassTree;
-    const int cp = cache_pass + pass_cache;
+    const int links = S.has_passthrough && st->link[0] && st->link[1] && st->link_cap ? kWfLinkLaunches : 0;
+    const int cp = cache_pass + pass_cache + links;
     int kernels_per_window = adjoint ? n_batches * (((3 + cp) + (3 + cache_pass)) * (depth + 1) + 4)
                                      : n_batches * ((3 + cp + (sort_threshold ? 3 : 0)) * (depth + 1) + 3);
     cudaGraphExec_t &exec = adjoint ? st->adj_exec : st->exec;
@@ -468,10 +527,10 @@ int wavefront_render_impl(WavefrontState *&st, const DevScene<R> &S, const DevCa
         char key[256];
         // the scene travels by value in the captured kernel parameters, so
         // its identity, counters and parameter version are part of the key
-        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d:%d:%d:%d:%p:%d", (int)sizeof(R), w, h, batch_spp,
+        snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%p:%p:%d:%d:%d:%d:%d:%p:%d:%p", (int)sizeof(R), w, h, batch_spp,
                  n_batches, depth, (const void *)S.nodes, (const void *)S.counters, S.version, (int)dyn, block,
                  sort_threshold, S.bvh_width, (const void *)S.trace_rec,
-                 (int)st->occ_cache_on + 2 * (int)st->pass_cache_on);
+                 (int)st->occ_cache_on + 2 * (int)st->pass_cache_on, st->link[0]);
         if (!exec || exec_key != key) {
             if (exec) cudaGraphExecDestroy(exec);
             exec = nullptr;
