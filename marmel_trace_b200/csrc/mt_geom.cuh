@@ -732,12 +732,6 @@ MT_D void trav_leaf(const DevScene<R> &S, Trav<R> &tv, int node, Hit<R> *best, T
 // Descend the binary tree from `node` (nearer child in a register, farther
 // child pushed) to the next leaf; kEmpty when the walk is over or the stack
 // would overflow (error word set).
-#ifndef MT_PREFETCH
-#define MT_PREFETCH 0
-#endif
-// Ask L1 for the line at p (no register, no wait).
-MT_D void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
-
 template <typename R>
 MT_D int descend2(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp, int *stk, int stride, TravCount &c)
 {
@@ -749,18 +743,6 @@ MT_D int descend2(const DevScene<R> &S, const Trav<R> &tv, int node, int &sp, in
         bool hl, hr;
         R tl, tr;
         ++c.nvis;
-#if MT_PREFETCH
-        // both children's records (or, for a triangle leaf, its first
-        // triangle) start toward L1 while this node's boxes are tested
-        if (q3.x >= 0) prefetch_l1(S.nodes + 4 * (size_t)q3.x);
-#if MT_PREFETCH > 1
-        else if (sizeof(R) == 4 && ((~q3.x) >> 3 & 1)) prefetch_l1(S.tri4 + 3 * (size_t)((~q3.x) >> 4));
-#endif
-        if (q3.y >= 0) prefetch_l1(S.nodes + 4 * (size_t)q3.y);
-#if MT_PREFETCH > 1
-        else if (sizeof(R) == 4 && ((~q3.y) >> 3 & 1)) prefetch_l1(S.tri4 + 3 * (size_t)((~q3.y) >> 4));
-#endif
-#endif
         node_test(q0, q1, q2, tv.rp, tv.tmin, tv.closest, &hl, &hr, &tl, &tr);
         if (hl && hr) {
             bool lnear = tl <= tr;
