@@ -945,11 +945,13 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOC
 // Link `step` (1..5) of the pass-through chains queued by the previous link
 // (in[0 .. min(link_count[step - 1], cap))); chains that pass another
 // transparent hit go to `out` (link_count[step]), the others write their
-// connection's result.
+// connection's result. `last`: every chain runs to its end here (the few
+// long chains left would otherwise pay one launch per link).
 template <typename R>
 __global__ void __launch_bounds__(kWfMaxBlock, MT_PASS_MIN_BLOCKS) k_wf_shadow_link(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq,
                                                                    WfCounters *C, R *nee, int b, int step,
-                                                                   const WfLink<R> *in, WfLink<R> *out, int cap)
+                                                                   const WfLink<R> *in, WfLink<R> *out, int cap,
+                                                                   bool last)
 {
     const int c = C->link_count[step - 1];
     const int n = c < cap ? c : cap;
@@ -961,10 +963,8 @@ __global__ void __launch_bounds__(kWfMaxBlock, MT_PASS_MIN_BLOCKS) k_wf_shadow_l
         V3<R> atten = v3(L.att[0], L.att[1], L.att[2]);
         R tmin = R(1e-3), remaining = L.remaining;
         int r = chain_link(S, cur_o, d, tmin, remaining, atten, step);
-        if (r == 2) {
-            if (push_link(out, &C->link_count[step], cap, cur_o, remaining, atten, L.q)) continue;
-            for (int k = step + 1; r == 2; ++k) r = chain_link(S, cur_o, d, tmin, remaining, atten, k);
-        }
+        if (r == 2 && !last && push_link(out, &C->link_count[step], cap, cur_o, remaining, atten, L.q)) continue;
+        for (int k = step + 1; r == 2; ++k) r = chain_link(S, cur_o, d, tmin, remaining, atten, k);
         const bool occ = r == 1;
         const V3<R> o = v3(s.o[0], s.o[1], s.o[2]);
         // the sun through volumetric clouds (pt_nee_sun, src/pathtrace.c:545-546)

@@ -229,8 +229,13 @@ struct WfLinkQueues {
 };
 
 // Kernels of one shadow stage in a scene with pass-through materials and
-// link queues: the first link, then one launch per further link (five).
-static constexpr int kWfLinkLaunches = 5;
+// link queues: the first link, then one launch per further link up to
+// kWfLinkLaunches, the last of which runs the chains left to their end.
+#ifndef MT_LINK_LAUNCHES
+#define MT_LINK_LAUNCHES 3
+#endif
+static constexpr int kWfLinkLaunches = MT_LINK_LAUNCHES;
+static_assert(kWfLinkLaunches >= 1 && kWfLinkLaunches <= 5, "link launches");
 
 template <typename R, bool ADJ, int W>
 void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, const DevScene<R> &S,
@@ -252,7 +257,8 @@ void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
             for (int step = 1; step <= kWfLinkLaunches; ++step)
                 k_wf_shadow_link<R><<<g, block, smem, s>>>(S, sq, C, nee, b, step,
                                                            (const WfLink<R> *)lq.q[(step - 1) & 1],
-                                                           (WfLink<R> *)lq.q[step & 1], lq.cap);
+                                                           (WfLink<R> *)lq.q[step & 1], lq.cap,
+                                                           step == kWfLinkLaunches);
     } else if (dyn) {
         k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
     } else if (occ && walk) {
