@@ -965,6 +965,25 @@ def profile_case(w: int = 480, h: int = 270, spp: int = 16):
         torch.cuda.synchronize()
 
 
+def profile_case_glass(w: int = 512, h: int = 512, spp: int = 4):
+    """The capture case of the pass-through shadow chains: item 41 of the
+    batched workload (43k triangles, a third of the materials glass, seed 3)
+    at 512x512, 4 spp, library defaults, plain launches, two frames."""
+    import torch
+
+    import marmel_trace_b200 as mt
+    from marmel_trace_b200 import _capi, scenes
+
+    it = scenes.batch_workload(seed=3, n=64)[41]
+    cam = it["desc"].make_camera(w, h)
+    with mt.GpuScene(it["desc"], precision="fp32", integrator="wavefront", use_graph=0) as g:
+        acc = torch.zeros((h, w, 3), dtype=torch.float32, device="cuda")
+        for r in range(2):
+            _capi.check(g.lib.mt_render_accumulate_device(g.h, cam.ref, w, h, spp * r, spp * (r + 1), it["depth"], 0,
+                                                          acc.data_ptr(), 0, None), "mt_render_accumulate_device")
+        torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -983,13 +1002,14 @@ def main():
     ap.add_argument("--rmse-target", type=float, default=0.0,
                     help="only measure the time of both integrators to this RMSE against the exact image "
                          "(480x270, 262,144-spp converged reference, 1024-spp windows); prints its own JSON line")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="only render the small profiling case (480x270, 16 spp, depth 8, plain launches) twice, "
-                         "for ncu captures of the stage kernels; prints nothing")
+    ap.add_argument("--profile-case", nargs="?", const="torus", default=None, choices=["torus", "glass"],
+                    help="only render a small profiling case twice, plain launches, for ncu captures; prints "
+                         "nothing. torus: the benchmark scene at 480x270, 16 spp; glass: item 41 of the batched "
+                         "workload at 512x512, 4 spp (the pass-through shadow chains)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
-        profile_case()
+        profile_case() if args.profile_case == "torus" else profile_case_glass()
         return
     if args.rmse_target > 0:
         import torch
