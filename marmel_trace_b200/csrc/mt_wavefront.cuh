@@ -854,13 +854,19 @@ MT_D int chain_link(const DevScene<R> &S, V3<R> &cur_o, V3<R> d, R &tmin, R &rem
     return step < 5 ? 2 : 1;  // six links at most, then occluded
 }
 
-// Append chain state to the link queue `out` (capacity cap); false when it
-// is full (the caller then finishes the chain itself).
+// Append chain state to the link queue `out`. Its capacity `cap` is the
+// stage's shadow-connection capacity, and every launch appends at most one
+// record per connection it reads, so it cannot fill; if it ever did, the
+// error word says so (ERR_QUEUE) and the record is dropped.
 template <typename R>
-MT_D bool push_link(WfLink<R> *out, int *count, int cap, V3<R> o, R remaining, V3<R> atten, int q)
+MT_D void push_link(const DevScene<R> &S, WfLink<R> *out, int *count, int cap, V3<R> o, R remaining, V3<R> atten,
+                    int q)
 {
     const int at = warp_append(count, true);
-    if (at >= cap) return false;
+    if (at >= cap) {
+        atomicOr(S.err, ERR_QUEUE);
+        return;
+    }
     WfLink<R> L;
     L.o[0] = o.x;
     L.o[1] = o.y;
@@ -871,16 +877,15 @@ MT_D bool push_link(WfLink<R> *out, int *count, int cap, V3<R> o, R remaining, V
     L.att[2] = atten.z;
     L.q = q;
     out[at] = L;
-    return true;
 }
 
 // `walk` (may be NULL): the connections to process are sq[walk[0 .. C->walk_count)]
 // and their cached occluder has already missed; otherwise sq[0 .. C->shadow_count).
-template <typename R, bool ADJ, int W, bool PASS>
+template <typename R, bool ADJ, int W, bool PASS, bool LINKED = false>
 // (binary tree: at most 72 registers, so 7 blocks of 128 fit an SM; the
 // pass-through instantiation would otherwise take 80 and run 6)
 //
-// PASS with `link` (not the adjoint): only the chain's first link runs here;
+// PASS and LINKED (not the adjoint): only the chain's first link runs here;
 // chains that pass a transparent hit go to the link queue (link_count[0]) and
 // k_wf_shadow_link runs their next links, one launch per link, so that the
 // lanes of a warp do not wait for the longest chain among them.
@@ -919,9 +924,14 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOC
                     const int4 e = *reinterpret_cast<const int4 *>(entry);
                     if (e.x != leaf) *reinterpret_cast<int4 *>(entry) = make_int4(leaf, e.x, e.y, e.z);
                 }
-                if (r == 2 && link && push_link(link, &C->link_count[0], link_cap, cur_o, remaining, atten, qs))
-                    continue;
-                for (int step = 1; r == 2; ++step) r = chain_link(S, cur_o, d, tmin, remaining, atten, step);
+                if (LINKED) {
+                    if (r == 2) {
+                        push_link(S, link, &C->link_count[0], link_cap, cur_o, remaining, atten, qs);
+                        continue;
+                    }
+                } else {
+                    for (int step = 1; r == 2; ++step) r = chain_link(S, cur_o, d, tmin, remaining, atten, step);
+                }
                 occ = r == 1;
             }
         } else {
@@ -945,13 +955,12 @@ __global__ void __launch_bounds__(kWfMaxBlock, W == 2 ? (PASS ? MT_PASS_MIN_BLOC
 // Link `step` (1..5) of the pass-through chains queued by the previous link
 // (in[0 .. min(link_count[step - 1], cap))); chains that pass another
 // transparent hit go to `out` (link_count[step]), the others write their
-// connection's result. `last`: every chain runs to its end here (the few
+// connection's result. LAST: every chain runs to its end here (the few
 // long chains left would otherwise pay one launch per link).
-template <typename R>
+template <typename R, bool LAST>
 __global__ void __launch_bounds__(kWfMaxBlock, MT_PASS_MIN_BLOCKS) k_wf_shadow_link(const __grid_constant__ DevScene<R> S, const WfShadow<R> *sq,
                                                                    WfCounters *C, R *nee, int b, int step,
-                                                                   const WfLink<R> *in, WfLink<R> *out, int cap,
-                                                                   bool last)
+                                                                   const WfLink<R> *in, WfLink<R> *out, int cap)
 {
     const int c = C->link_count[step - 1];
     const int n = c < cap ? c : cap;
@@ -963,8 +972,12 @@ __global__ void __launch_bounds__(kWfMaxBlock, MT_PASS_MIN_BLOCKS) k_wf_shadow_l
         V3<R> atten = v3(L.att[0], L.att[1], L.att[2]);
         R tmin = R(1e-3), remaining = L.remaining;
         int r = chain_link(S, cur_o, d, tmin, remaining, atten, step);
-        if (r == 2 && !last && push_link(out, &C->link_count[step], cap, cur_o, remaining, atten, L.q)) continue;
-        for (int k = step + 1; r == 2; ++k) r = chain_link(S, cur_o, d, tmin, remaining, atten, k);
+        if constexpr (LAST) {
+            for (int k = step + 1; r == 2; ++k) r = chain_link(S, cur_o, d, tmin, remaining, atten, k);
+        } else if (r == 2) {
+            push_link(S, out, &C->link_count[step], cap, cur_o, remaining, atten, L.q);
+            continue;
+        }
         const bool occ = r == 1;
         const V3<R> o = v3(s.o[0], s.o[1], s.o[2]);
         // the sun through volumetric clouds (pt_nee_sun, src/pathtrace.c:545-546)

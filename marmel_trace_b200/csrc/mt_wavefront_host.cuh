@@ -169,15 +169,14 @@ template <typename R> int wf_reserve(WavefrontState *st, size_t n_paths, size_t 
 }
 
 // Link queues of the pass-through chains (scenes with water or transparency
-// > 0.8): two buffers, each for half the shadow connections of the reserved
-// path slots; a chain that finds its queue full runs its remaining links in
-// place. Optional: when the allocation fails the chains run whole in
-// k_wf_shadow (same results).
+// > 0.8): two buffers, each for every shadow connection of the reserved path
+// slots (a launch appends at most one record per connection). Optional: when
+// the allocation fails the chains run whole in k_wf_shadow (same results).
 template <typename R> void wf_reserve_links(WavefrontState *st)
 {
     if (st->link[0] && st->link[1]) return;
     const size_t nshadow = st->cap_paths * (size_t)(st->light_count + 1);
-    size_t cap = nshadow / 2;
+    size_t cap = nshadow;
     if (cap < 1) cap = 1;
     if (cap > (size_t)INT_MAX) cap = (size_t)INT_MAX;
     for (int k = 0; k < 2; ++k)
@@ -244,21 +243,27 @@ void launch_shadow(bool dyn, int g, int block, size_t smem, cudaStream_t s, cons
 {
     if (S.has_passthrough) {
         WfLink<R> *l0 = ADJ || !lq.cap ? nullptr : (WfLink<R> *)lq.q[0];
-        if (!ADJ && occ && walk && S.pass_root != kNoPassTree) {
-            // cached opaque blockers first (with the pass tree), then the
-            // chain for the rest
-            k_wf_shadow_pass_cache<R><<<g, block, smem, s>>>(S, sq, C, nee, occ, wh, b, walk);
-            k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, walk, l0, lq.cap);
-        } else {
-            k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, nullptr, l0,
-                                                                lq.cap);
+        const bool cached = !ADJ && occ && walk && S.pass_root != kNoPassTree;
+        // cached opaque blockers first (with the pass tree), then the chain
+        // for the rest
+        if (cached) k_wf_shadow_pass_cache<R><<<g, block, smem, s>>>(S, sq, C, nee, occ, wh, b, walk);
+        int *w = cached ? walk : nullptr;
+        if constexpr (!ADJ) {
+            if (l0) {
+                k_wf_shadow<R, false, 2, true, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, w, l0,
+                                                                            lq.cap);
+                for (int step = 1; step <= kWfLinkLaunches; ++step) {
+                    const WfLink<R> *in = (const WfLink<R> *)lq.q[(step - 1) & 1];
+                    WfLink<R> *out = (WfLink<R> *)lq.q[step & 1];
+                    if (step == kWfLinkLaunches)
+                        k_wf_shadow_link<R, true><<<g, block, smem, s>>>(S, sq, C, nee, b, step, in, out, lq.cap);
+                    else
+                        k_wf_shadow_link<R, false><<<g, block, smem, s>>>(S, sq, C, nee, b, step, in, out, lq.cap);
+                }
+                return;
+            }
         }
-        if (l0)
-            for (int step = 1; step <= kWfLinkLaunches; ++step)
-                k_wf_shadow_link<R><<<g, block, smem, s>>>(S, sq, C, nee, b, step,
-                                                           (const WfLink<R> *)lq.q[(step - 1) & 1],
-                                                           (WfLink<R> *)lq.q[step & 1], lq.cap,
-                                                           step == kWfLinkLaunches);
+        k_wf_shadow<R, ADJ, 2, true><<<g, block, smem, s>>>(S, sq, C, nee, att, occ, wh, b, w, nullptr, 0);
     } else if (dyn) {
         k_wf_shadow_dyn<R, ADJ, W><<<g, block, smem, s>>>(S, sq, C, nee, att);
     } else if (occ && walk) {
