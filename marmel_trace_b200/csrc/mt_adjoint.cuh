@@ -82,24 +82,52 @@ template <typename R> MT_D R dG_drough(R ndl, R ndv, R rough)
     return (dgl * gv + gl * dgv) * dk;
 }
 
-// Accumulate coeff . d shade(m, N, L, V, light) / d(material params).
+// The albedo rgb, roughness and metallic terms (offsets 0..4 within the
+// material's block) of one surface vertex, summed in registers over its NEE
+// connections and its BSDF weight and added to the block's accumulator once:
+// five shared-memory atomics per vertex instead of five per connection.
+// A non-finite term is dropped on its own, as gadd drops it.
+template <typename R> struct VertexSink {
+    R g[5] = {R(0), R(0), R(0), R(0), R(0)};
+    MT_D void add(int k, R v)
+    {
+        if (isfinite(v)) g[k] += v;
+    }
+    MT_D void flush(const AdjCtx &c, int mi, bool dmet) const
+    {
+        const int base = kParamsPerMaterial * mi;
+        for (int k = 0; k < 4; ++k) gadd(c, base + k, (float)g[k]);
+        if (dmet) gadd(c, base + 4, (float)g[4]);
+    }
+};
+
+// d metallic is taken only strictly inside (0, 1), where the clamp passes it
+template <typename R> MT_D bool metallic_differentiable(const DevMaterial<R> &m)
+{
+    return m.metallic > R(0) && m.metallic < R(1);
+}
+
+// Accumulate coeff . d shade(m, N, L, V, light) / d(material params) into
+// the vertex sink, and return shade(m, N, L, V, 1): the BSDF value both
+// terms share, from the same intermediates.
 // shade_local (src/material.c:157-188): only the albedo enters.
 // shade_pbr (src/material.c:234-290): albedo, metallic, roughness.
-template <typename R>
-MT_D void shade_grad(const DevMaterial<R> &m, int mi, V3<R> N, V3<R> L, V3<R> V, V3<R> light, V3<R> coeff,
-                     const AdjCtx &c)
+// PBR: every material of the scene is a PBR surface (the legacy branch
+// compiles out).
+template <typename R, bool PBR>
+MT_D V3<R> shade_grad(const DevMaterial<R> &m, V3<R> N, V3<R> L, V3<R> V, V3<R> light, V3<R> coeff,
+                      VertexSink<R> &sink)
 {
+    const V3<R> zero = v3(R(0), R(0), R(0));
     R ndl = dot(N, L);
-    if (ndl <= R(0)) return;
-    const int base = kParamsPerMaterial * mi;
-    if (!m.pbr) {
-        for (int ch = 0; ch < 3; ++ch) gadd(c, base + ch, (float)(comp3(coeff, ch) * comp3(light, ch) * ndl));
-        return;
+    if (ndl <= R(0)) return zero;
+    if (!PBR && !m.pbr) {
+        for (int ch = 0; ch < 3; ++ch) sink.add(ch, comp3(coeff, ch) * comp3(light, ch) * ndl);
+        return shade_local(m, N, L, V, v3(R(1), R(1), R(1)));
     }
     R ndv = dot(N, V);
-    if (ndv <= R(0)) return;
+    if (ndv <= R(0)) return zero;
     R met = mat_clamp01(m.metallic);
-    bool dmet = m.metallic > R(0) && m.metallic < R(1);
     R alpha = roughness_to_alpha(m.roughness);
     V3<R> h = add(L, V);
     R ndh = R(0), sin2 = R(1);
@@ -121,21 +149,25 @@ MT_D void shade_grad(const DevMaterial<R> &m, int mi, V3<R> N, V3<R> L, V3<R> V,
                                D * dG_drough(ndl, ndv, m.roughness)) / denom
                             : R(0);
     R d_rough = R(0), d_met = R(0);
+    R s1[3];
     for (int ch = 0; ch < 3; ++ch) {
         R A = comp3(coeff, ch) * comp3(light, ch) * ndl;
         R alb = m.albedo[ch];
         R f0 = R(0.04) + (alb - R(0.04)) * met;
         R F = f0 + (R(1) - f0) * k5;
         R kd = (R(1) - F) * (R(1) - met);
+        // shade_pbr's value for unit light: (kd albedo / pi + F D G / (4 ndl ndv)) ndl
+        s1[ch] = ((kd * alb) * (R(1) / Const<R>::pi) + F * specs) * ndl;
         R dF_dalb = (R(1) - k5) * met;
-        gadd(c, base + ch, (float)(A * ((-dF_dalb * (R(1) - met) * alb + kd) / Const<R>::pi + dF_dalb * specs)));
+        sink.add(ch, A * ((-dF_dalb * (R(1) - met) * alb + kd) / Const<R>::pi + dF_dalb * specs));
         R dF_dmet = (R(1) - k5) * (alb - R(0.04));
         R dkd_dmet = -dF_dmet * (R(1) - met) - (R(1) - F);
         d_met += A * (dkd_dmet * alb / Const<R>::pi + dF_dmet * specs);
         d_rough += A * F * dspecs;
     }
-    gadd(c, base + 3, (float)d_rough);
-    if (dmet) gadd(c, base + 4, (float)d_met);
+    sink.add(3, d_rough);
+    sink.add(4, d_met);
+    return v3(s1[0], s1[1], s1[2]);
 }
 
 // d sky_sample(dir) / d sun_color (diagonal): the sun glow and the lit clouds
@@ -181,12 +213,12 @@ template <typename R> struct LobeInfo {
     R lobe;         // legacy diffuse r_dif / p_dif
 };
 
-template <typename R>
+template <typename R, bool PBR>
 MT_D bool sample_with_info(const DevMaterial<R> &m, V3<R> N, V3<R> d, V3<R> V, int front_face, R u1, R u2, R u_lobe,
                            R u_glass, V3<R> *wi, V3<R> *w, int *refracted, int *specular, LobeInfo<R> *info)
 {
     info->kind = 0;
-    if (m.pbr) {
+    if (PBR || m.pbr) {
         *refracted = 0;
         bool ok = pt_sample_pbr(m, N, d, V, u1, u2, u_lobe, wi, w, specular);
         if (ok) {
@@ -225,19 +257,18 @@ MT_D bool sample_with_info(const DevMaterial<R> &m, V3<R> N, V3<R> d, V3<R> V, i
     return ok;
 }
 
-// Accumulate sum_c coeff_c d w_c / d theta for the sampled lobe (detached).
+// Accumulate sum_c coeff_c d w_c / d theta for the sampled lobe (detached)
+// into the vertex sink.
 template <typename R>
-MT_D void weight_grad(const DevMaterial<R> &m, int mi, const LobeInfo<R> &info, V3<R> N, V3<R> V, V3<R> wi,
-                      V3<R> coeff, const AdjCtx &c)
+MT_D void weight_grad(const DevMaterial<R> &m, const LobeInfo<R> &info, V3<R> N, V3<R> V, V3<R> wi, V3<R> coeff,
+                      VertexSink<R> &sink)
 {
-    const int base = kParamsPerMaterial * mi;
     if (info.kind == 3) {
-        for (int ch = 0; ch < 3; ++ch) gadd(c, base + ch, (float)(comp3(coeff, ch) * info.lobe));
+        for (int ch = 0; ch < 3; ++ch) sink.add(ch, comp3(coeff, ch) * info.lobe);
         return;
     }
     if (info.kind != 1 && info.kind != 2) return;
     R met = pt_clamp01(m.metallic);
-    bool dmet = m.metallic > R(0) && m.metallic < R(1);
     R ndv = dot(N, V);
     if (info.kind == 1) {
         V3<R> H = info.H;
@@ -263,12 +294,12 @@ MT_D void weight_grad(const DevMaterial<R> &m, int mi, const LobeInfo<R> &info, 
             R fc = mat_clamp01(f0);
             R F = fc + (R(1) - fc) * k5;
             R dF_df0 = f_in ? (R(1) - k5) : R(0);
-            gadd(c, base + ch, (float)(comp3(coeff, ch) * dF_df0 * met * S));
+            sink.add(ch, comp3(coeff, ch) * dF_df0 * met * S);
             d_met += comp3(coeff, ch) * dF_df0 * (alb - R(0.04)) * S;
             d_rough += comp3(coeff, ch) * F * dS;
         }
-        gadd(c, base + 3, (float)d_rough);
-        if (dmet) gadd(c, base + 4, (float)d_met);
+        sink.add(3, d_rough);
+        sink.add(4, d_met);
     } else {
         R cv = mat_clamp01(ndv);
         R mm = R(1) - cv;
@@ -284,10 +315,10 @@ MT_D void weight_grad(const DevMaterial<R> &m, int mi, const LobeInfo<R> &info, 
             R F = fc + (R(1) - fc) * k5;
             R dF_df0 = f_in ? (R(1) - k5) : R(0);
             R kd = (R(1) - F) * (R(1) - met);
-            gadd(c, base + ch, (float)(comp3(coeff, ch) * (-dF_df0 * met * (R(1) - met) * alb + kd) * inv));
+            sink.add(ch, comp3(coeff, ch) * (-dF_df0 * met * (R(1) - met) * alb + kd) * inv);
             d_met += comp3(coeff, ch) * (-dF_df0 * (alb - R(0.04)) * (R(1) - met) - (R(1) - F)) * alb * inv;
         }
-        if (dmet) gadd(c, base + 4, (float)d_met);
+        sink.add(4, d_met);
     }
 }
 
@@ -351,21 +382,30 @@ template <typename R> struct AdjVertex {
     R beta[3];     // throughput arriving at the vertex (the NEE weight)
     int mat;       // material index; -1: no vertex pending
     int b;         // bounce index
-    int flags;     // kVertFront | kVertSun
+    int flags;     // kVertFront | kVertSun | the connections made (vert_conn_bit)
     int pad;
 };
 static constexpr int kVertFront = 1;  // front-face hit (legacy glass sampling)
 static constexpr int kVertSun = 2;    // the vertex draws a sun NEE sample
+// Bit of AdjVertex::flags saying that NEE connection `li` (a light, or
+// kMaxLights: the sun) was queued, so that its transmittance record holds
+// this vertex's result. Records of connections not made are never read,
+// which spares clearing them between vertices.
+MT_HD constexpr int vert_conn_bit(int li) { return 1 << (2 + li); }
+static constexpr int kVertConnAll = ((1 << kNeeSlots) - 1) << 2;
 
 // Gradient terms of one vertex: NEE to every sphere light and to the sun,
-// given each connection's record att[kAttStride * slot] (transmittance zero
-// where it was not made, occluded or dark: such a connection adds nothing),
-// and the BSDF weight term against `remaining` = L - radiance through this
-// vertex.
+// given each made connection's record att[kAttStride * slot] (transmittance
+// zero where it was occluded or dark: such a connection adds nothing), and
+// the BSDF weight term against `remaining` = L - radiance through this
+// vertex. The vertex material's albedo / roughness / metallic terms are
+// summed in a VertexSink and added once.
 // Light sampling follows pt_nee_emissive / pt_nee_sun (src/pathtrace.c:534-606)
 // and the BSDF sample pt_sample_* (src/pathtrace.c:961-1000), from the same
 // random channels as the primal pass.
-template <typename R>
+// PBR: every material is a PBR surface without media or absorption
+// (DevScene::pbr_only); the legacy and absorption terms compile out.
+template <typename R, bool PBR = false>
 MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *att, uint32_t seed_key,
                          V3<R> remaining, V3<R> adj, const AdjCtx &ctx)
 {
@@ -376,8 +416,9 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
     const V3<R> V = v3(vx.v[0], vx.v[1], vx.v[2]);
     const V3<R> nee_w = mul(adj, v3(vx.beta[0], vx.beta[1], vx.beta[2]));
     const int b = vx.b;
-    const V3<R> one = v3(R(1), R(1), R(1));
+    VertexSink<R> sink;
     for (int li = 0; li < S.light_count; ++li) {
+        if (!(vx.flags & vert_conn_bit(li))) continue;
         const R *slot = att + kAttStride * li;
         const V3<R> a = v3(slot[0], slot[1], slot[2]);
         if (a.x == R(0) && a.y == R(0) && a.z == R(0)) continue;
@@ -393,15 +434,14 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
         R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
         V3<R> wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
         V3<R> coeff = scale(nee_w, Omega);
-        shade_grad(mm, mi, N, wi, V, mul(mat3(lt.emissive), a), coeff, ctx);
-        V3<R> s1 = shade(mm, N, wi, V, one);
+        const V3<R> s1 = shade_grad<R, PBR>(mm, N, wi, V, mul(mat3(lt.emissive), a), coeff, sink);
         int lmat = __ldg(S.prim_info + lt.prim).y;
         if (lmat >= 0 && lmat < S.material_count)
             for (int ch = 0; ch < 3; ++ch)
                 gadd(ctx, kParamsPerMaterial * lmat + 5 + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
-        nee_absorb_grad(ctx, slot, mul(mul(coeff, s1), mul(mat3(lt.emissive), a)));
+        if (!PBR) nee_absorb_grad(ctx, slot, mul(mul(coeff, s1), mul(mat3(lt.emissive), a)));
     }
-    if (vx.flags & kVertSun) {
+    if ((vx.flags & kVertSun) && (vx.flags & vert_conn_bit(kMaxLights))) {
         const R *as = att + kAttStride * kMaxLights;
         const V3<R> a = v3(as[0], as[1], as[2]);
         if (a.x != R(0) || a.y != R(0) || a.z != R(0)) {
@@ -411,11 +451,10 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
             R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
             R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
             V3<R> coeff = scale(nee_w, Omega);
-            shade_grad(mm, mi, N, Ls, V, mul(mat3(S.sky.sun_color), a), coeff, ctx);
-            V3<R> s1 = shade(mm, N, Ls, V, one);
+            const V3<R> s1 = shade_grad<R, PBR>(mm, N, Ls, V, mul(mat3(S.sky.sun_color), a), coeff, sink);
             for (int ch = 0; ch < 3; ++ch)
                 gadd(ctx, ctx.sun + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
-            nee_absorb_grad(ctx, as, mul(mul(coeff, s1), mul(mat3(S.sky.sun_color), a)));
+            if (!PBR) nee_absorb_grad(ctx, as, mul(mul(coeff, s1), mul(mat3(S.sky.sun_color), a)));
         }
     }
     uint32_t kb = hash3(seed_key ^ PT_KEY, (uint32_t)b, 0u);
@@ -426,9 +465,10 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
     V3<R> wi, w;
     int refracted = 0, sampled_specular = 0;
     LobeInfo<R> info;
-    if (sample_with_info(mm, N, neg(V), V, (vx.flags & kVertFront) ? 1 : 0, u1, u2, u_lobe, u_glass, &wi, &w,
-                         &refracted, &sampled_specular, &info))
-        weight_grad(mm, mi, info, N, V, wi, mul(adj, safe_div(remaining, w)), ctx);
+    if (sample_with_info<R, PBR>(mm, N, neg(V), V, (vx.flags & kVertFront) ? 1 : 0, u1, u2, u_lobe, u_glass, &wi,
+                                 &w, &refracted, &sampled_specular, &info))
+        weight_grad(mm, info, N, V, wi, mul(adj, safe_div(remaining, w)), sink);
+    sink.flush(ctx, mi, metallic_differentiable(mm));
 }
 
 // Replay of pathtrace_radiance (src/pathtrace.c:800-1028) that accumulates
@@ -499,8 +539,9 @@ MT_D void pathtrace_adjoint(const DevScene<R> &S, Ray3<R> primary, int max_depth
         vx.beta[0] = throughput.x; vx.beta[1] = throughput.y; vx.beta[2] = throughput.z;
         vx.mat = mi;
         vx.b = b;
+        // the local records below start cleared: every connection's record is valid
         vx.flags = (h.front_face ? kVertFront : 0) |
-                   ((b == 0 || (b == 1 && medium >= 0 && last_bounce_specular)) ? kVertSun : 0);
+                   ((b == 0 || (b == 1 && medium >= 0 && last_bounce_specular)) ? kVertSun : 0) | kVertConnAll;
         vx.pad = 0;
         R att[kNeeSlots * kAttStride];
         for (int k = 0; k < kNeeSlots * kAttStride; ++k) att[k] = R(0);

@@ -406,9 +406,14 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             tic();
             if (replay) {
                 // the adjoint rejects every scene extra
-                k_wf_shade<R, true, false><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b, depth,
-                                                                        paths, nee, rays[which ^ 1], sq, A, nullptr,
-                                                                        nullptr);
+                if (sizeof(R) == 4 && S.pbr_only)
+                    k_wf_shade<R, true, false, sizeof(R) == 4><<<g, block, smem_shade, s>>>(
+                        S, rays[which], hits, C, which, b, depth, paths, nee, rays[which ^ 1], sq, A, nullptr,
+                        nullptr);
+                else
+                    k_wf_shade<R, true, false><<<g, block, smem_shade, s>>>(S, rays[which], hits, C, which, b,
+                                                                            depth, paths, nee, rays[which ^ 1], sq, A,
+                                                                            nullptr, nullptr);
             } else {
                 const WfRay<R> *srays = sort ? (const WfRay<R> *)st->sorted_rays : nullptr;
                 if (S.has_extras)
@@ -451,7 +456,10 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
         if (adjoint) {
             if ((rc = bounces(batch, true))) return rc;
             tic();
-            k_wf_finalize_adj<R><<<g, block, 0, s>>>(S, n_paths, paths, nee, A);
+            if (sizeof(R) == 4 && S.pbr_only)
+                k_wf_finalize_adj<R, sizeof(R) == 4><<<g, block, 0, s>>>(S, n_paths, paths, nee, A);
+            else
+                k_wf_finalize_adj<R, false><<<g, block, 0, s>>>(S, n_paths, paths, nee, A);
             toc(3);
         }
     }
