@@ -21,7 +21,9 @@ roofline     : the dominant stage (shadow: the occluder-cache pass plus the
                walk on its own tree (instrumented, oracle/_ref, in the
                CPU-baseline leg) over the queries the GPU logs on a 480x270
                window, per path sample. `traffic` / `dram_gbs` / `l2_gbs` come
-               from the committed ncu capture of the current kernels.
+               from the committed ncu capture of the current kernels;
+               `l2_frac` puts `l2_gbs` against an L2-resident copy measured
+               in the same run (`l2_peak_gbs`).
 plain_gpu    : the same frames through the megakernel (one thread per pixel,
                the "plain GPU" form of the same estimator).
 time_to_rmse : 480x270 frames of the same scene and view: a 16,384-spp
@@ -35,7 +37,10 @@ c1           : the 64-sphere configuration (320x240, 8 spp, depth 5): path
                tracer (wavefront and megakernel) and fixed-spp Whitted.
 adjoint      : forward + path-replay backward of the inverse-rendering
                configuration (512x512, 32 spp, depth 6, 355 parameters).
-inverse      : 200 Adam steps of inverse rendering on that configuration.
+inverse      : 200 Adam steps of inverse rendering on that configuration;
+               beside them the loss floor (true parameters against the
+               target) and the image error of the start and final parameters
+               against the true ones on shared samples.
 batch        : the batched uneven workload (64 scenes) in one graph launch.
 large        : the 10M-triangle water / tree scene at 3840x2160, depth 12
                (cpu_reference_msamples_s: the reference on the same scene and
@@ -163,6 +168,30 @@ def peaks():
     if p.exists():
         return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def l2_peak_gbs(torch) -> float:
+    """Bandwidth of a device copy whose source and destination (16 MB each)
+    stay resident in the 126 MB L2: read + write bytes over CUDA-event time,
+    best of three runs of 200 copies. The denominator of the stages' L2
+    fractions, measured on the GPU the bench runs on."""
+    n = 16 * 1024 * 1024 // 4
+    a = torch.ones(n, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    st = torch.cuda.current_stream()
+    best = 0.0
+    for _ in range(3):
+        for _ in range(5):
+            b.copy_(a)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(200):
+            b.copy_(a)
+        e1.record(st)
+        e1.synchronize()
+        best = max(best, 200 * 2 * a.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del a, b
+    return best
 
 
 def cpu_model() -> str:
@@ -395,6 +424,8 @@ def run_ours(args):
         h0, h1 = res["history"][0], res["history"][-1]
         inverse = {"steps": res["steps"], "steps_per_s": round(res["steps_per_s"], 2), "params": res["params"],
                    "loss_first": round(h0["loss"], 6), "loss_last": round(h1["loss"], 6),
+                   "loss_at_truth": round(res["loss_at_truth"], 6),
+                   "image_rmse_crn": {k: round(v, 5) for k, v in res["image_rmse_crn"].items()},
                    "param_rmse_start": round(res["start_param_rmse"], 4), "param_rmse_last": round(h1["param_rmse"], 4),
                    "group_rmse_start": {k: round(v, 4) for k, v in res["start_groups"].items()},
                    "group_rmse_last": {k: round(v, 4) for k, v in h1["groups"].items()},
@@ -408,6 +439,7 @@ def run_ours(args):
 
     # roofline of the dominant stage
     peak, peak_kind = peaks()
+    l2_peak = l2_peak_gbs(torch)
     rays_per_sample = (cnt.extension_rays + cnt.shadow_rays) / n_counted
     bw = qopt.get("bvh_width", 2) or 2
     cpu = None
@@ -440,7 +472,8 @@ def run_ours(args):
                  "bytes_source": "GPU counters of a 4-spp pass (the walks' node visits and primitive tests)",
                  "traffic": round(tr * W * H * SPP / launches_k) if tr else None,
                  "dram_gbs": round(tr * W * H * SPP / t / 1e9, 1) if tr else None,
-                 "l2_gbs": round(l2 * W * H * SPP / t / 1e9, 1) if l2 else None}
+                 "l2_gbs": round(l2 * W * H * SPP / t / 1e9, 1) if l2 else None,
+                 "l2_frac": round(l2 * W * H * SPP / t / 1e9 / l2_peak, 4) if l2 else None}
             if cpu and cpu.get("canonical"):
                 can = cpu["canonical"][f"{k}_bytes_per_sample"] * W * H * SPP
                 r["canonical"] = {"bytes_per_launch": round(can / launches_k), "gbs": round(can / t / 1e9, 1),
@@ -457,7 +490,9 @@ def run_ours(args):
                     "kernel": r_dom["kernel"] + "; per-stage CUDA events over one frame",
                     "algorithmic_bytes_per_launch": r_dom["algorithmic_bytes_per_launch"],
                     "bytes_source": r_dom["bytes_source"], "canonical": r_dom.get("canonical"),
-                    "dram_gbs": r_dom["dram_gbs"], "l2_gbs": r_dom["l2_gbs"],
+                    "dram_gbs": r_dom["dram_gbs"], "l2_gbs": r_dom["l2_gbs"], "l2_frac": r_dom["l2_frac"],
+                    "l2_peak_gbs": round(l2_peak, 1),
+                    "l2_peak_source": "device copy of 16 MB held in L2, CUDA events (measured in this run)",
                     "traffic_source": TRAFFIC["source"], "second_kernel": r_oth}
 
     out = {
@@ -984,6 +1019,25 @@ def profile_case_glass(w: int = 512, h: int = 512, spp: int = 4):
         torch.cuda.synchronize()
 
 
+def profile_case_adjoint(w: int = 512, h: int = 512, spp: int = 8):
+    """The capture case of the adjoint: the inverse-rendering scene (128
+    spheres, 32 PBR materials, seed 4) at 512x512, 8 spp, depth 6 (2.1M
+    paths), plain launches. Two forward + backward pairs: the first allocates
+    the replay buffers, so captures skip its launches."""
+    import torch
+
+    from marmel_trace_b200 import scenes
+    from marmel_trace_b200.adjoint import DiffRenderer
+
+    r = DiffRenderer(scenes.adjoint_scene(), w, h, spp, 6, use_graph=0)
+    target = r.render(s0=1_000_000)
+    for k in range(2):
+        img = r.render(s0=spp * k)
+        r.backward(2.0 * (img - target), s0=spp * k)
+    torch.cuda.synchronize()
+    r.release()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1002,14 +1056,15 @@ def main():
     ap.add_argument("--rmse-target", type=float, default=0.0,
                     help="only measure the time of both integrators to this RMSE against the exact image "
                          "(480x270, 262,144-spp converged reference, 1024-spp windows); prints its own JSON line")
-    ap.add_argument("--profile-case", nargs="?", const="torus", default=None, choices=["torus", "glass"],
+    ap.add_argument("--profile-case", nargs="?", const="torus", default=None, choices=["torus", "glass", "adjoint"],
                     help="only render a small profiling case twice, plain launches, for ncu captures; prints "
                          "nothing. torus: the benchmark scene at 480x270, 16 spp; glass: item 41 of the batched "
-                         "workload at 512x512, 4 spp (the pass-through shadow chains)")
+                         "workload at 512x512, 4 spp (the pass-through shadow chains); adjoint: forward + backward "
+                         "of the inverse-rendering scene at 512x512, 8 spp")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
-        profile_case() if args.profile_case == "torus" else profile_case_glass()
+        {"torus": profile_case, "glass": profile_case_glass, "adjoint": profile_case_adjoint}[args.profile_case]()
         return
     if args.rmse_target > 0:
         import torch

@@ -20,6 +20,17 @@ them at the full rate.
 The parameter error is reported per group (albedo, roughness, metallic,
 emissive, sun; the absorption parameters do not act on this scene, which has
 no medium) over the materials some pixel of the target shows.
+
+Two image-space figures go with it. `loss_at_truth` is the L2 loss of the
+true parameters against the target, averaged over fresh windows: the floor
+that the Monte-Carlo noise of a `spp` render and of the target set, below
+which the loss cannot go. `image_rmse_crn` is the RMS difference between the
+image of the start (or final) parameters and the image of the true ones,
+both rendered at `target_spp` on the same sample window (common random
+numbers), so that most of the noise cancels: it measures how far the
+parameters are from reproducing the target, which one view pins down better
+than the parameters themselves (the sun radiance and the albedos trade
+against each other, and so do metallic and albedo on rough surfaces).
 """
 from __future__ import annotations
 
@@ -107,8 +118,21 @@ def run(steps: int = 200, width: int = 512, height: int = 512, spp: int = 32, de
                          "groups": group_errors(cur, truth, n_mat, seen)})
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    final = params.detach().cpu().numpy()
+    # the loss floor: the true parameters against the target on fresh windows
+    r.set_params(truth)
+    floor = [float(((r.render(s0=spp * (2 * steps + 2 * j)) - target) ** 2).mean()) for j in range(4)]
     r.release()
+    # start / final images against the true image on one shared sample window
+    ev = DiffRenderer(d, width, height, target_spp, depth, device=device)
+    imgs = {}
+    for name, p in (("truth", truth), ("start", start), ("last", final)):
+        ev.set_params(p)
+        imgs[name] = ev.render(s0=20_000_000)
+    ev.release()
+    crn = {k: float(torch.sqrt(((imgs[k] - imgs["truth"]) ** 2).mean())) for k in ("start", "last")}
     return {"steps": steps, "seconds": dt, "steps_per_s": steps / dt, "history": hist,
+            "loss_at_truth": float(np.mean(floor)), "image_rmse_crn": crn,
             "start_param_rmse": float(np.sqrt(np.mean((start - truth) ** 2))),
             "start_groups": group_errors(start, truth, n_mat, seen), "params": len(truth),
             "materials_seen": int(seen.sum()),
