@@ -417,45 +417,50 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
     const V3<R> nee_w = mul(adj, v3(vx.beta[0], vx.beta[1], vx.beta[2]));
     const int b = vx.b;
     VertexSink<R> sink;
-    for (int li = 0; li < S.light_count; ++li) {
+    // the lights in order, then the sun (slot kMaxLights) as one more pass of
+    // the same loop, so the gradient code is emitted once: the replay kernels
+    // are bound by instruction fetch
+    const int n_conn = S.light_count + ((vx.flags & kVertSun) ? 1 : 0);
+    for (int k = 0; k < n_conn; ++k) {
+        const bool sun = k == S.light_count;
+        const int li = sun ? kMaxLights : k;
         if (!(vx.flags & vert_conn_bit(li))) continue;
         const R *slot = att + kAttStride * li;
         const V3<R> a = v3(slot[0], slot[1], slot[2]);
         if (a.x == R(0) && a.y == R(0) && a.z == R(0)) continue;
-        const DevLight<R> &lt = S.lights[li];
-        V3<R> to_c = sub(mat3(lt.center), P);
-        R dc2 = length_sq(to_c);
-        R dc = msqrt(dc2);
-        R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
-        const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
-        R Omega = R(2) * R(3.14159265358979323846) * omc;
-        V3<R> w = scale(to_c, R(1) / dc);
-        R u1 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
-        R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
-        V3<R> wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
-        V3<R> coeff = scale(nee_w, Omega);
-        const V3<R> s1 = shade_grad<R, PBR>(mm, N, wi, V, mul(mat3(lt.emissive), a), coeff, sink);
-        int lmat = __ldg(S.prim_info + lt.prim).y;
-        if (lmat >= 0 && lmat < S.material_count)
-            for (int ch = 0; ch < 3; ++ch)
-                gadd(ctx, kParamsPerMaterial * lmat + 5 + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
-        if (!PBR) nee_absorb_grad(ctx, slot, mul(mul(coeff, s1), mul(mat3(lt.emissive), a)));
-    }
-    if ((vx.flags & kVertSun) && (vx.flags & vert_conn_bit(kMaxLights))) {
-        const R *as = att + kAttStride * kMaxLights;
-        const V3<R> a = v3(as[0], as[1], as[2]);
-        if (a.x != R(0) || a.y != R(0) || a.z != R(0)) {
+        V3<R> wi, emit;
+        R Omega;
+        int pidx;  // first parameter of the emitter's radiance: its material's emissive rgb, or the sun's
+        if (!sun) {
+            const DevLight<R> &lt = S.lights[li];
+            V3<R> to_c = sub(mat3(lt.center), P);
+            R dc2 = length_sq(to_c);
+            R dc = msqrt(dc2);
+            R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
+            const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
+            Omega = R(2) * R(3.14159265358979323846) * omc;
+            V3<R> w = scale(to_c, R(1) / dc);
+            R u1 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
+            R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
+            wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
+            emit = mat3(lt.emissive);
+            const int lmat = __ldg(S.prim_info + lt.prim).y;
+            pidx = (lmat >= 0 && lmat < S.material_count) ? kParamsPerMaterial * lmat + 5 : -1;
+        } else {
             R r1 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_A);
             R r2 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_B);
-            V3<R> Ls = sun_disk_dir(mat3(S.sky.sun_dir), S.sky.sun_radius, r1, r2);
+            wi = sun_disk_dir(mat3(S.sky.sun_dir), S.sky.sun_radius, r1, r2);
             R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
-            R Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
-            V3<R> coeff = scale(nee_w, Omega);
-            const V3<R> s1 = shade_grad<R, PBR>(mm, N, Ls, V, mul(mat3(S.sky.sun_color), a), coeff, sink);
-            for (int ch = 0; ch < 3; ++ch)
-                gadd(ctx, ctx.sun + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
-            if (!PBR) nee_absorb_grad(ctx, as, mul(mul(coeff, s1), mul(mat3(S.sky.sun_color), a)));
+            Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
+            emit = mat3(S.sky.sun_color);
+            pidx = ctx.sun;
         }
+        const V3<R> coeff = scale(nee_w, Omega);
+        const V3<R> s1 = shade_grad<R, PBR>(mm, N, wi, V, mul(emit, a), coeff, sink);
+        if (pidx >= 0)
+            for (int ch = 0; ch < 3; ++ch)
+                gadd(ctx, pidx + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
+        if (!PBR) nee_absorb_grad(ctx, slot, mul(mul(coeff, s1), mul(emit, a)));
     }
     uint32_t kb = hash3(seed_key ^ PT_KEY, (uint32_t)b, 0u);
     R u1 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_A);
