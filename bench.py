@@ -22,8 +22,8 @@ roofline     : the dominant stage (shadow: the occluder-cache pass plus the
                CPU-baseline leg) over the queries the GPU logs on a 480x270
                window, per path sample. `traffic` / `dram_gbs` / `l2_gbs` come
                from the committed ncu capture of the current kernels;
-               `l2_frac` puts `l2_gbs` against an L2-resident copy measured
-               in the same run (`l2_peak_gbs`).
+               `l2_frac` puts `l2_gbs` against the L2 read bandwidth
+               measured in the same run (`l2_peak_gbs`).
 plain_gpu    : the same frames through the megakernel (one thread per pixel,
                the "plain GPU" form of the same estimator).
 time_to_rmse : 480x270 frames of the same scene and view: a 16,384-spp
@@ -170,28 +170,19 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def l2_peak_gbs(torch) -> float:
-    """Bandwidth of a device copy whose source and destination (16 MB each)
-    stay resident in the 126 MB L2: read + write bytes over CUDA-event time,
-    best of three runs of 200 copies. The denominator of the stages' L2
-    fractions, measured on the GPU the bench runs on."""
-    n = 16 * 1024 * 1024 // 4
-    a = torch.ones(n, dtype=torch.float32, device="cuda")
-    b = torch.empty_like(a)
-    st = torch.cuda.current_stream()
-    best = 0.0
-    for _ in range(3):
-        for _ in range(5):
-            b.copy_(a)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        for _ in range(200):
-            b.copy_(a)
-        e1.record(st)
-        e1.synchronize()
-        best = max(best, 200 * 2 * a.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9)
-    del a, b
-    return best
+def l2_peak_gbs(device: int) -> float:
+    """L2 read bandwidth measured on the GPU the bench runs on
+    (mt_measure_l2_read_gbs: one launch reads a 32 MB buffer 64 times with
+    L2-only 16-byte loads; best of three launches). The denominator of the
+    stages' L2 fractions."""
+    import ctypes as C
+
+    from marmel_trace_b200 import _capi
+
+    lib = _capi.load()
+    out = C.c_double(0.0)
+    _capi.check(lib.mt_measure_l2_read_gbs(device, 32 << 20, 64, C.byref(out)), "mt_measure_l2_read_gbs")
+    return out.value
 
 
 def cpu_model() -> str:
@@ -439,7 +430,7 @@ def run_ours(args):
 
     # roofline of the dominant stage
     peak, peak_kind = peaks()
-    l2_peak = l2_peak_gbs(torch)
+    l2_peak = l2_peak_gbs(local)
     rays_per_sample = (cnt.extension_rays + cnt.shadow_rays) / n_counted
     bw = qopt.get("bvh_width", 2) or 2
     cpu = None
@@ -492,7 +483,8 @@ def run_ours(args):
                     "bytes_source": r_dom["bytes_source"], "canonical": r_dom.get("canonical"),
                     "dram_gbs": r_dom["dram_gbs"], "l2_gbs": r_dom["l2_gbs"], "l2_frac": r_dom["l2_frac"],
                     "l2_peak_gbs": round(l2_peak, 1),
-                    "l2_peak_source": "device copy of 16 MB held in L2, CUDA events (measured in this run)",
+                    "l2_peak_source": "mt_measure_l2_read_gbs: 32 MB held in L2 read 64 times in one launch, "
+                                      "L2-only loads (measured in this run)",
                     "traffic_source": TRAFFIC["source"], "second_kernel": r_oth}
 
     out = {

@@ -586,6 +586,16 @@ int mt_adjoint_backward_device(mt_scene *scene, const mt_camera *cam, int width,
                                int spp_end, int max_depth, const float *dL_dimage_dev, double *grad_dev,
                                int accumulate, void *stream);
 
+/*
+ * Measured L2 read bandwidth of `device` in GB/s: one launch reads a buffer of
+ * `bytes` (a multiple of 16 in [1 MiB, 96 MiB], so that it stays in the 126 MB
+ * L2) `reps` times with L2-only 16-byte loads from a grid of 2048 threads per
+ * SM; best of three launches after a warm-up one. It is the denominator of
+ * the traversal kernels' L2 fractions in the benchmark. Allocates and frees
+ * its buffer; synchronous. No counterpart in the reference (a CPU renderer).
+ */
+int mt_measure_l2_read_gbs(int device, size_t bytes, int reps, double *gbs);
+
 /* Library version and last error text (thread-local, never NULL). */
 const char *mt_version(void);
 const char *mt_last_error(void);

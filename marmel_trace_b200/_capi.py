@@ -266,6 +266,7 @@ SIGNATURES = {
     "mt_scene_set_material_params": (I, [P, P, I]),
     "mt_adjoint_backward": (I, [P, P, I, I, I, I, P, P, I]),
     "mt_adjoint_backward_device": (I, [P, P, I, I, I, I, I, P, P, I, P]),
+    "mt_measure_l2_read_gbs": (I, [I, C.c_size_t, I, P]),
     "mt_version": (C.c_char_p, []),
     "mt_last_error": (C.c_char_p, []),
 }

@@ -40,6 +40,7 @@ UNITS = [
     ("mt_adjoint_f64.cu", ["--fmad=false"]),
     ("mt_bvh.cpp", []),
     ("mt_bvh_gpu.cu", ["--fmad=false"]),
+    ("mt_probe.cu", []),
 ]
 
 

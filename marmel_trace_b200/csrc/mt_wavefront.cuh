@@ -286,9 +286,11 @@ MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> 
 //
 // ADJ: the replay pass of the adjoint. The path's previous vertex (held in
 // A.verts) gets its gradient terms once its NEE results are gathered, with
-// the remaining radiance L - radiance; emission and sky terms are taken
-// where they occur. The radiance bookkeeping is the primal pass's, so the
-// replay reproduces it exactly.
+// the remaining radiance L - radiance: from bounce 1 on k_wf_vertex_adj does
+// both for the queue before this kernel runs, so the gradient code of a
+// vertex is not part of this kernel. Emission and sky terms are taken where
+// they occur. The radiance bookkeeping is the primal pass's, so the replay
+// reproduces it exactly.
 //
 // When the bounce's extend results were sorted by material (C->sorted), the
 // kernel reads the sorted copies instead.
@@ -351,16 +353,14 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !ADJ && !EXTRA
             st = paths[slot];
             throughput = v3(st.throughput[0], st.throughput[1], st.throughput[2]);
             radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
-            if (b > 0) gather_nee(S, nee + (size_t)slot * kNeeSlots * 3, &radiance);
+            // ADJ: k_wf_vertex_adj has gathered this path's NEE results into
+            // its radiance and taken its previous vertex's gradient
+            if (!ADJ && b > 0) gather_nee(S, nee + (size_t)slot * kNeeSlots * 3, &radiance);
             V3<R> adj = zero, Lp = zero;
             if constexpr (ADJ) {
                 adj = adj_of_path(A.P, slot);
                 const R *Lq = A.L + 3 * (size_t)slot;
                 Lp = v3(Lq[0], Lq[1], Lq[2]);
-                const AdjVertex<R> pv = A.verts[slot];
-                if (pv.mat >= 0)
-                    vertex_adjoint<R, PBR>(S, pv, A.att + (size_t)slot * kNeeSlots * kAttStride, st.seed_key,
-                                           sub(Lp, radiance), adj, ctx);
             }
             const V3<R> ro = v3(r.o[0], r.o[1], r.o[2]);
             const V3<R> d = v3(r.d[0], r.d[1], r.d[2]);
@@ -1213,23 +1213,77 @@ __global__ void k_wf_finalize(const __grid_constant__ DevScene<R> S, int n_paths
     }
 }
 
-// Adjoint replay: the vertex each path still holds (its last) takes its
-// gradient terms against the radiance the path ends with. PBR as in k_wf_shade.
+// Adjoint replay, before the shade of bounce b >= 1: every path of the
+// bounce's ray queue gathers its NEE results into its radiance (written back;
+// the shade kernel then skips the gather) and its previous vertex takes its
+// gradient terms against L - radiance. Kept out of k_wf_shade: with the
+// gradient code inside, the replay shade was bound by instruction fetch.
+// PBR as in k_wf_shade.
 template <typename R, bool PBR>
-__global__ void k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
+__global__ void k_wf_vertex_adj(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfCounters *C,
+                                int which, WfPath<R> *paths, R *nee, WfAdj<R> A)
 {
     __shared__ float adj_g[kAdjMaxParams];
     const AdjCtx ctx = make_adj_ctx(adj_g, S.material_count);
     adj_block_begin(adj_g, A.P);
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_paths; q += gridDim.x * blockDim.x) {
-        const AdjVertex<R> pv = A.verts[q];
+    const int n = C->ray_count[which];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int slot = rays_in[q].slot;
+        WfPath<R> *sp = paths + slot;
+        V3<R> radiance = v3(sp->radiance[0], sp->radiance[1], sp->radiance[2]);
+        gather_nee(S, nee + (size_t)slot * kNeeSlots * 3, &radiance);
+        sp->radiance[0] = radiance.x;
+        sp->radiance[1] = radiance.y;
+        sp->radiance[2] = radiance.z;
+        const AdjVertex<R> pv = A.verts[slot];
         if (pv.mat < 0) continue;
-        const WfPath<R> st = paths[q];
-        V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
-        gather_nee(S, nee + (size_t)q * kNeeSlots * 3, &radiance);
-        const R *Lq = A.L + 3 * (size_t)q;
-        vertex_adjoint<R, PBR>(S, pv, A.att + (size_t)q * kNeeSlots * kAttStride, st.seed_key,
-                       sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj_of_path(A.P, q), ctx);
+        const R *Lq = A.L + 3 * (size_t)slot;
+        vertex_adjoint<R, PBR>(S, pv, A.att + (size_t)slot * kNeeSlots * kAttStride, sp->seed_key,
+                               sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj_of_path(A.P, slot), ctx);
+    }
+    adj_block_end(adj_g, A.P);
+}
+
+// Adjoint replay: the vertex each path still holds (its last) takes its
+// gradient terms against the radiance the path ends with. PBR as in k_wf_shade.
+// Paths whose last vertex is pending are gathered first, chunk by chunk of
+// 8 x blockDim paths, into a list in shared memory (warp-aggregated appends),
+// so the gradient code runs on full warps instead of on the scattered lanes
+// of a grid-stride loop over every path (paths that escaped hold none).
+static constexpr int kFinalizeChunkPerThread = 8;
+template <typename R, bool PBR>
+__global__ void k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
+{
+    __shared__ float adj_g[kAdjMaxParams];
+    __shared__ int pending[kFinalizeChunkPerThread * kWfMaxBlock];
+    __shared__ int n_pending;
+    const AdjCtx ctx = make_adj_ctx(adj_g, S.material_count);
+    adj_block_begin(adj_g, A.P);
+    const int chunk = kFinalizeChunkPerThread * (int)blockDim.x;
+    for (long long base = (long long)blockIdx.x * chunk; base < n_paths; base += (long long)gridDim.x * chunk) {
+        if (threadIdx.x == 0) n_pending = 0;
+        __syncthreads();
+        // every lane runs the same iterations (chunk is a multiple of the
+        // block, the block of the warp), so each append sees the whole warp
+        for (int i = threadIdx.x; i < chunk; i += blockDim.x) {
+            const long long q = base + i;
+            const bool want = q < n_paths && A.verts[q].mat >= 0;
+            const int at = warp_append(&n_pending, want);
+            if (want) pending[at] = (int)q;
+        }
+        __syncthreads();
+        const int np = n_pending;
+        for (int i = threadIdx.x; i < np; i += blockDim.x) {
+            const int q = pending[i];
+            const AdjVertex<R> pv = A.verts[q];
+            const WfPath<R> st = paths[q];
+            V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
+            gather_nee(S, nee + (size_t)q * kNeeSlots * 3, &radiance);
+            const R *Lq = A.L + 3 * (size_t)q;
+            vertex_adjoint<R, PBR>(S, pv, A.att + (size_t)q * kNeeSlots * kAttStride, st.seed_key,
+                                   sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj_of_path(A.P, q), ctx);
+        }
+        __syncthreads();  // the list is rebuilt for the next chunk
     }
     adj_block_end(adj_g, A.P);
 }

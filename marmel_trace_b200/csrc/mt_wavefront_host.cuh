@@ -406,6 +406,13 @@ int wf_enqueue(WavefrontState *st, const DevScene<R> &S, int w, int h, int batch
             tic();
             if (replay) {
                 // the adjoint rejects every scene extra
+                if (b > 0) {
+                    if (sizeof(R) == 4 && S.pbr_only)
+                        k_wf_vertex_adj<R, sizeof(R) == 4><<<g, block, 0, s>>>(S, rays[which], C, which, paths, nee,
+                                                                               A);
+                    else
+                        k_wf_vertex_adj<R, false><<<g, block, 0, s>>>(S, rays[which], C, which, paths, nee, A);
+                }
                 if (sizeof(R) == 4 && S.pbr_only)
                     k_wf_shade<R, true, false, sizeof(R) == 4><<<g, block, smem_shade, s>>>(
                         S, rays[which], hits, C, which, b, depth, paths, nee, rays[which ^ 1], sq, A, nullptr,
