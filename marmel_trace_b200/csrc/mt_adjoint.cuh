@@ -405,11 +405,18 @@ static constexpr int kVertConnAll = ((1 << kNeeSlots) - 1) << 2;
 // random channels as the primal pass.
 // PBR: every material is a PBR surface without media or absorption
 // (DevScene::pbr_only); the legacy and absorption terms compile out.
-template <typename R, bool PBR = false>
+// WARP: the caller runs all 32 lanes of the warp through this call together
+// (`active` false where a lane has no vertex). A connection's emitter terms
+// then go to the same three parameters for every lane of the warp (one light
+// per iteration), so they are summed across the warp with shuffles and added
+// by one lane: the vertex kernels were bound by these shared-memory atomics.
+// Without WARP (the one-thread-per-pixel replay, whose lanes diverge) each
+// lane adds its own.
+template <typename R, bool PBR = false, bool WARP = false>
 MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *att, uint32_t seed_key,
-                         V3<R> remaining, V3<R> adj, const AdjCtx &ctx)
+                         V3<R> remaining, V3<R> adj, const AdjCtx &ctx, bool active = true)
 {
-    const int mi = vx.mat;
+    const int mi = active ? vx.mat : 0;
     const DevMaterial<R> &mm = S.materials[mi];
     const V3<R> P = v3(vx.p[0], vx.p[1], vx.p[2]);
     const V3<R> N = v3(vx.n[0], vx.n[1], vx.n[2]);
@@ -419,49 +426,71 @@ MT_D void vertex_adjoint(const DevScene<R> &S, const AdjVertex<R> &vx, const R *
     VertexSink<R> sink;
     // the lights in order, then the sun (slot kMaxLights) as one more pass of
     // the same loop, so the gradient code is emitted once: the replay kernels
-    // are bound by instruction fetch
-    const int n_conn = S.light_count + ((vx.flags & kVertSun) ? 1 : 0);
+    // are bound by instruction fetch. Under WARP every lane takes every pass.
+    const bool sun_wanted = active && (vx.flags & kVertSun);
+    const int n_conn = S.light_count + ((WARP || sun_wanted) ? 1 : 0);
     for (int k = 0; k < n_conn; ++k) {
         const bool sun = k == S.light_count;
         const int li = sun ? kMaxLights : k;
-        if (!(vx.flags & vert_conn_bit(li))) continue;
-        const R *slot = att + kAttStride * li;
-        const V3<R> a = v3(slot[0], slot[1], slot[2]);
-        if (a.x == R(0) && a.y == R(0) && a.z == R(0)) continue;
-        V3<R> wi, emit;
-        R Omega;
+        V3<R> e = v3(R(0), R(0), R(0));  // the emitter's radiance term of this lane
         int pidx;  // first parameter of the emitter's radiance: its material's emissive rgb, or the sun's
         if (!sun) {
-            const DevLight<R> &lt = S.lights[li];
-            V3<R> to_c = sub(mat3(lt.center), P);
-            R dc2 = length_sq(to_c);
-            R dc = msqrt(dc2);
-            R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
-            const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
-            Omega = R(2) * R(3.14159265358979323846) * omc;
-            V3<R> w = scale(to_c, R(1) / dc);
-            R u1 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
-            R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
-            wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
-            emit = mat3(lt.emissive);
-            const int lmat = __ldg(S.prim_info + lt.prim).y;
+            const int lmat = __ldg(S.prim_info + S.lights[li].prim).y;
             pidx = (lmat >= 0 && lmat < S.material_count) ? kParamsPerMaterial * lmat + 5 : -1;
         } else {
-            R r1 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_A);
-            R r2 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_B);
-            wi = sun_disk_dir(mat3(S.sky.sun_dir), S.sky.sun_radius, r1, r2);
-            R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
-            Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
-            emit = mat3(S.sky.sun_color);
             pidx = ctx.sun;
         }
-        const V3<R> coeff = scale(nee_w, Omega);
-        const V3<R> s1 = shade_grad<R, PBR>(mm, N, wi, V, mul(emit, a), coeff, sink);
-        if (pidx >= 0)
-            for (int ch = 0; ch < 3; ++ch)
-                gadd(ctx, pidx + ch, (float)(comp3(coeff, ch) * comp3(a, ch) * comp3(s1, ch)));
-        if (!PBR) nee_absorb_grad(ctx, slot, mul(mul(coeff, s1), mul(emit, a)));
+        const bool made = active && (!sun || sun_wanted) && (vx.flags & vert_conn_bit(li));
+        const R *slot = att + kAttStride * li;
+        const V3<R> a = made ? v3(slot[0], slot[1], slot[2]) : v3(R(0), R(0), R(0));
+        if (a.x != R(0) || a.y != R(0) || a.z != R(0)) {
+            V3<R> wi, emit;
+            R Omega;
+            if (!sun) {
+                const DevLight<R> &lt = S.lights[li];
+                V3<R> to_c = sub(mat3(lt.center), P);
+                R dc2 = length_sq(to_c);
+                R dc = msqrt(dc2);
+                R cos_mx = msqrt(R(1) - (lt.radius * lt.radius) / dc2);
+                const R omc = cone_one_minus_cos((lt.radius * lt.radius) / dc2, cos_mx);
+                Omega = R(2) * R(3.14159265358979323846) * omc;
+                V3<R> w = scale(to_c, R(1) / dc);
+                R u1 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_A);
+                R u2 = rand01<R>(seed_key ^ (uint32_t)li, (uint32_t)b, PT_CH_NEE_EMIT_B);
+                wi = light_sphere_sample_dir(w, cos_mx, omc, u1, u2);
+                emit = mat3(lt.emissive);
+            } else {
+                R r1 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_A);
+                R r2 = rand01<R>(seed_key, (uint32_t)b, PT_CH_NEE_SUN_B);
+                wi = sun_disk_dir(mat3(S.sky.sun_dir), S.sky.sun_radius, r1, r2);
+                R rad = S.sky.sun_radius * R(3.14159265358979323846) / R(180);
+                Omega = (S.sky.sun_radius > R(0)) ? R(2) * R(3.14159265358979323846) * (R(1) - mcos(rad)) : R(1);
+                emit = mat3(S.sky.sun_color);
+            }
+            const V3<R> coeff = scale(nee_w, Omega);
+            const V3<R> s1 = shade_grad<R, PBR>(mm, N, wi, V, mul(emit, a), coeff, sink);
+            e = mul(mul(coeff, a), s1);
+            if (!PBR) nee_absorb_grad(ctx, slot, mul(mul(coeff, s1), mul(emit, a)));
+        }
+        if constexpr (WARP) {
+            // a non-finite term is dropped before the sum, as gadd drops it
+            float ev[3] = {(float)e.x, (float)e.y, (float)e.z};
+            bool any = false;
+            for (int ch = 0; ch < 3; ++ch) {
+                if (!isfinite(ev[ch])) ev[ch] = 0.0f;
+                any |= ev[ch] != 0.0f;
+            }
+            if (__any_sync(0xffffffffu, any) && pidx >= 0) {
+                for (int ch = 0; ch < 3; ++ch)
+                    for (int o = 16; o > 0; o >>= 1) ev[ch] += __shfl_xor_sync(0xffffffffu, ev[ch], o);
+                if ((threadIdx.x & 31) == 0)
+                    for (int ch = 0; ch < 3; ++ch) gadd(ctx, pidx + ch, ev[ch]);
+            }
+        } else if (pidx >= 0) {
+            for (int ch = 0; ch < 3; ++ch) gadd(ctx, pidx + ch, (float)comp3(e, ch));
+        }
     }
+    if (!active) return;
     uint32_t kb = hash3(seed_key ^ PT_KEY, (uint32_t)b, 0u);
     R u1 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_A);
     R u2 = rand01<R>(kb, (uint32_t)b, PT_CH_BSDF_B);

@@ -1227,19 +1227,33 @@ __global__ void k_wf_vertex_adj(const __grid_constant__ DevScene<R> S, const WfR
     const AdjCtx ctx = make_adj_ctx(adj_g, S.material_count);
     adj_block_begin(adj_g, A.P);
     const int n = C->ray_count[which];
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const int slot = rays_in[q].slot;
-        WfPath<R> *sp = paths + slot;
-        V3<R> radiance = v3(sp->radiance[0], sp->radiance[1], sp->radiance[2]);
-        gather_nee(S, nee + (size_t)slot * kNeeSlots * 3, &radiance);
-        sp->radiance[0] = radiance.x;
-        sp->radiance[1] = radiance.y;
-        sp->radiance[2] = radiance.z;
-        const AdjVertex<R> pv = A.verts[slot];
-        if (pv.mat < 0) continue;
-        const R *Lq = A.L + 3 * (size_t)slot;
-        vertex_adjoint<R, PBR>(S, pv, A.att + (size_t)slot * kNeeSlots * kAttStride, sp->seed_key,
-                               sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj_of_path(A.P, slot), ctx);
+    const int stride = gridDim.x * blockDim.x;
+    // every lane of a warp takes the same iterations: vertex_adjoint sums
+    // across the warp
+    const int n_round = (n + stride - 1) / stride * stride;
+    const V3<R> zero = v3(R(0), R(0), R(0));
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_round; q += stride) {
+        AdjVertex<R> pv = {};
+        pv.mat = -1;
+        int slot = 0;
+        uint32_t seed_key = 0;
+        V3<R> remaining = zero, adj = zero;
+        if (q < n) {
+            slot = rays_in[q].slot;
+            WfPath<R> *sp = paths + slot;
+            V3<R> radiance = v3(sp->radiance[0], sp->radiance[1], sp->radiance[2]);
+            gather_nee(S, nee + (size_t)slot * kNeeSlots * 3, &radiance);
+            sp->radiance[0] = radiance.x;
+            sp->radiance[1] = radiance.y;
+            sp->radiance[2] = radiance.z;
+            pv = A.verts[slot];
+            seed_key = sp->seed_key;
+            const R *Lq = A.L + 3 * (size_t)slot;
+            remaining = sub(v3(Lq[0], Lq[1], Lq[2]), radiance);
+            adj = adj_of_path(A.P, slot);
+        }
+        vertex_adjoint<R, PBR, true>(S, pv, A.att + (size_t)slot * kNeeSlots * kAttStride, seed_key, remaining, adj,
+                                     ctx, pv.mat >= 0);
     }
     adj_block_end(adj_g, A.P);
 }
@@ -1273,15 +1287,29 @@ __global__ void k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_p
         }
         __syncthreads();
         const int np = n_pending;
-        for (int i = threadIdx.x; i < np; i += blockDim.x) {
-            const int q = pending[i];
-            const AdjVertex<R> pv = A.verts[q];
-            const WfPath<R> st = paths[q];
-            V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
-            gather_nee(S, nee + (size_t)q * kNeeSlots * 3, &radiance);
-            const R *Lq = A.L + 3 * (size_t)q;
-            vertex_adjoint<R, PBR>(S, pv, A.att + (size_t)q * kNeeSlots * kAttStride, st.seed_key,
-                                   sub(v3(Lq[0], Lq[1], Lq[2]), radiance), adj_of_path(A.P, q), ctx);
+        // every lane of the block takes the same iterations (vertex_adjoint
+        // sums across the warp); lanes past the list take part inactive
+        const int np_round = (np + (int)blockDim.x - 1) / (int)blockDim.x * (int)blockDim.x;
+        const V3<R> zero = v3(R(0), R(0), R(0));
+        for (int i = threadIdx.x; i < np_round; i += blockDim.x) {
+            AdjVertex<R> pv = {};
+            pv.mat = -1;
+            int q = 0;
+            uint32_t seed_key = 0;
+            V3<R> remaining = zero, adj = zero;
+            if (i < np) {
+                q = pending[i];
+                pv = A.verts[q];
+                const WfPath<R> st = paths[q];
+                V3<R> radiance = v3(st.radiance[0], st.radiance[1], st.radiance[2]);
+                gather_nee(S, nee + (size_t)q * kNeeSlots * 3, &radiance);
+                seed_key = st.seed_key;
+                const R *Lq = A.L + 3 * (size_t)q;
+                remaining = sub(v3(Lq[0], Lq[1], Lq[2]), radiance);
+                adj = adj_of_path(A.P, q);
+            }
+            vertex_adjoint<R, PBR, true>(S, pv, A.att + (size_t)q * kNeeSlots * kAttStride, seed_key, remaining,
+                                         adj, ctx, i < np);
         }
         __syncthreads();  // the list is rebuilt for the next chunk
     }
