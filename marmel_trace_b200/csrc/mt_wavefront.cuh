@@ -1269,9 +1269,10 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && PBR) ? 7 : 0) 
 // 8 x blockDim paths, into a list in shared memory (warp-aggregated appends),
 // so the gradient code runs on full warps instead of on the scattered lanes
 // of a grid-stride loop over every path (paths that escaped hold none).
+// Held to 7 blocks per SM like k_wf_vertex_adj (backward 46.8 -> 46.5 ms).
 static constexpr int kFinalizeChunkPerThread = 8;
 template <typename R, bool PBR>
-__global__ void k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
+__global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && PBR) ? 7 : 0) k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
 {
     __shared__ float adj_g[kAdjMaxParams];
     __shared__ int pending[kFinalizeChunkPerThread * kWfMaxBlock];
