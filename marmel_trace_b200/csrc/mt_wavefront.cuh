@@ -312,11 +312,13 @@ MT_D void push_shadow(WfShadow<R> *sq, WfCounters *C, bool want, V3<R> o, V3<R> 
 // so no transmittance record is cleared between vertices. With both, the
 // backward of the 512x512, 32-spp adjoint configuration measured 70.1 ms
 // against 100.7 ms, gradients equal to 2e-6 relative (float sum order).
-// The FP32 PBR replay kernel is held to 7 blocks of 128 per SM as well
-// (72 registers, 16 bytes of spills): backward 49.3 ms against 52.7 at 91
-// registers and 5 blocks, 53.4 at 6 blocks.
+// The FP32 replay kernels are held to 7 blocks of 128 per SM as well: for
+// the PBR scene (72 registers, 16 bytes of spills) backward 49.3 ms against
+// 52.7 at 91 registers and 5 blocks, 53.4 at 6 blocks; with the vertex
+// kernels bounded the same way, the water scene's backward (legacy and
+// medium terms) took 53.1 ms against 61.2.
 template <typename R, bool ADJ, bool EXTRAS, bool PBR = false>
-__global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !EXTRAS && (!ADJ || PBR)) ? 7 : 0) k_wf_shade(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
+__global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && !EXTRAS) ? 7 : 0) k_wf_shade(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfHit<R> *hits,
                                                   WfCounters *C, int which, int b, int max_depth, WfPath<R> *paths,
                                                   R *nee, WfRay<R> *rays_out, WfShadow<R> *sq, WfAdj<R> A,
                                                   const WfRay<R> *sorted_rays, const WfHit<R> *sorted_hits)
@@ -1221,11 +1223,11 @@ __global__ void k_wf_finalize(const __grid_constant__ DevScene<R> S, int n_paths
 // the shade kernel then skips the gather) and its previous vertex takes its
 // gradient terms against L - radiance. Kept out of k_wf_shade: with the
 // gradient code inside, the replay shade was bound by instruction fetch.
-// PBR as in k_wf_shade. The FP32 PBR kernel is held to 7 blocks of 128 per
-// SM (72 registers, 88 bytes of spills): backward 46.9 ms against 49.2 at 91
-// registers and 5 blocks; 6 blocks measured no change.
+// PBR as in k_wf_shade. The FP32 kernels are held to 7 blocks of 128 per SM
+// (72 registers, 88 bytes of spills for PBR): backward 46.9 ms against 49.2
+// at 91 registers and 5 blocks; 6 blocks measured no change.
 template <typename R, bool PBR>
-__global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && PBR) ? 7 : 0) k_wf_vertex_adj(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfCounters *C,
+__global__ void __launch_bounds__(kWfMaxBlock, sizeof(R) == 4 ? 7 : 0) k_wf_vertex_adj(const __grid_constant__ DevScene<R> S, const WfRay<R> *rays_in, const WfCounters *C,
                                 int which, WfPath<R> *paths, R *nee, WfAdj<R> A)
 {
     __shared__ float adj_g[kAdjMaxParams];
@@ -1272,7 +1274,7 @@ __global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && PBR) ? 7 : 0) 
 // Held to 7 blocks per SM like k_wf_vertex_adj (backward 46.8 -> 46.5 ms).
 static constexpr int kFinalizeChunkPerThread = 8;
 template <typename R, bool PBR>
-__global__ void __launch_bounds__(kWfMaxBlock, (sizeof(R) == 4 && PBR) ? 7 : 0) k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
+__global__ void __launch_bounds__(kWfMaxBlock, sizeof(R) == 4 ? 7 : 0) k_wf_finalize_adj(const __grid_constant__ DevScene<R> S, int n_paths, const WfPath<R> *paths, R *nee, WfAdj<R> A)
 {
     __shared__ float adj_g[kAdjMaxParams];
     __shared__ int pending[kFinalizeChunkPerThread * kWfMaxBlock];
